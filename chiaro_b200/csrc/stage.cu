@@ -1,0 +1,990 @@
+// stage.cu — host side of the B200 depth stage and its C ABI.
+//
+// Orchestrates refine_multiview_depth (crates/chiaro-fusion/src/depth.rs:312-580)
+// on one CUDA stream: cost volume -> eight-path SGM -> winner-take-all ->
+// optional completion -> direct measurement -> consistency filters -> report
+// statistics -> per-target decisions -> output warps and depth map. Every
+// stage is a kernel; the host only validates, uploads, launches and reads
+// the results back. There is no CPU fallback: a CUDA failure is reported as
+// CHIARO_ERR_CUDA.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "cost.cuh"
+#include "decisions.cuh"
+#include "direct.cuh"
+#include "filters.cuh"
+#include "select.cuh"
+#include "sgm.cuh"
+
+using namespace chiaro;
+
+struct chiaro_depth_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    struct Buffer {
+        void *ptr = nullptr;
+        size_t bytes = 0;
+    };
+    std::map<std::string, Buffer> buffers;
+    cudaEvent_t events[8] = {};
+    float timings[7] = {};
+    int launches = 0;  // this library's kernel launches in the last stage call
+};
+
+namespace {
+
+struct CudaError {
+    cudaError_t code;
+    const char *what;
+};
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) throw CudaError{e_, #call};         \
+    } while (0)
+
+// Grow-only named device buffer of at least `count` elements.
+template <class T>
+T *dbuf(chiaro_depth_ctx *ctx, const std::string &name, size_t count) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    auto &b = ctx->buffers[name];
+    if (b.bytes < bytes) {
+        if (b.ptr) CK(cudaFree(b.ptr));
+        b.ptr = nullptr;
+        CK(cudaMalloc(&b.ptr, bytes));
+        b.bytes = bytes;
+    }
+    return static_cast<T *>(b.ptr);
+}
+
+int fail(chiaro_depth_ctx *ctx, const CudaError &e) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s failed: %s", e.what, cudaGetErrorString(e.code));
+    ctx->error = buf;
+    cudaGetLastError();
+    return CHIARO_ERR_CUDA;
+}
+
+size_t div_ceil(size_t a, size_t b) { return (a + b - 1) / b; }
+
+bool options_valid(const chiaro_depth_options &o) {  // depth.rs:1879-1891
+    return o.enabled && o.grid_step > 0 && std::isfinite(o.near_depth) && std::isfinite(o.far_depth) &&
+           o.near_depth > 0.0 && o.far_depth > o.near_depth && o.planes >= 3 && o.patch_radius > 0 &&
+           o.minimum_support > 0 && o.best_view_count >= o.minimum_support && o.minimum_neighbour_support > 0;
+}
+
+// inverse_depth_samples (depth.rs:1834-1843)
+std::vector<double> inverse_depth_samples(double near_d, double far_d, size_t count) {
+    double near_inverse = 1.0 / near_d, far_inverse = 1.0 / far_d;
+    std::vector<double> out(count);
+    for (size_t i = 0; i < count; ++i) {
+        double weight = (double)i / (double)(count - 1);
+        out[i] = 1.0 / (near_inverse * (1.0 - weight) + far_inverse * weight);
+    }
+    return out;
+}
+
+// Spatial weights exp(-d^2 / (2 sigma^2)), sigma = max(0.75 r, 1), in f32 with
+// the platform expf exactly as warped_patch_zncc computes them (depth.rs:1777, 1805-1806).
+std::vector<float> spatial_weights(int radius) {
+    float sigma = std::fmax((float)radius * 0.75f, 1.0f);
+    std::vector<float> w;
+    for (int dy = -radius; dy <= radius; ++dy)
+        for (int dx = -radius; dx <= radius; ++dx) {
+            float distance_sq = (float)(dx * dx + dy * dy);
+            w.push_back(std::exp(-distance_sq / (2.0f * sigma * sigma)));
+        }
+    return w;
+}
+
+unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)div_ceil(n, threads); }
+
+struct Grids {
+    size_t coarse_step, coarse_columns, coarse_rows;
+    size_t step, columns, rows;
+};
+
+Grids grids_for(size_t width, size_t height, const chiaro_depth_options &o) {
+    Grids g;
+    g.coarse_step = std::max<size_t>(o.grid_step, 4);
+    g.coarse_columns = div_ceil(width, g.coarse_step) + 1;
+    g.coarse_rows = div_ceil(height, g.coarse_step) + 1;
+    g.step = std::max<size_t>(g.coarse_step / 2, 4);
+    g.columns = div_ceil(width, g.step) + 1;
+    g.rows = div_ceil(height, g.step) + 1;
+    return g;
+}
+
+template <class T>
+void upload(chiaro_depth_ctx *ctx, T *dst, const T *src, size_t count) {
+    CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+}
+template <class T>
+void download(chiaro_depth_ctx *ctx, T *dst, const T *src, size_t count) {
+    if (!dst) return;
+    CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+}
+
+void set_smem_limits() {
+    static bool done = false;
+    if (done) return;
+    CK(cudaFuncSetAttribute(cost_volume_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(direct_depth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(target_decision_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    done = true;
+}
+
+// ---- SGM ---------------------------------------------------------------------------
+void launch_sgm(chiaro_depth_ctx *ctx, const float *data, const float *guidance, float *out, int columns, int rows,
+                int labels) {
+    const int K = (labels + 31) / 32;
+    const int threads = 256;
+    const int order[4] = {SGM_ROWS, SGM_COLUMNS, SGM_DOWN_RIGHT, SGM_DOWN_LEFT};
+    bool first = true;
+    for (int f : order) {
+        int paths = sgm_path_count(f, columns, rows);
+        unsigned blocks = blocks_for((size_t)paths * 32, threads);
+        for (int reverse = 0; reverse < 2; ++reverse) {
+            int acc = first ? 0 : 1;
+            switch (K) {
+#define SGM_CASE(k)                                                                                        \
+    case k:                                                                                                \
+        sgm_direction_kernel<k><<<blocks, threads, 0, ctx->stream>>>(data, guidance, out, columns, rows, labels, \
+                                                                     f, reverse, acc);                     \
+        break;
+                SGM_CASE(1) SGM_CASE(2) SGM_CASE(3) SGM_CASE(4) SGM_CASE(5) SGM_CASE(6) SGM_CASE(7) SGM_CASE(8)
+#undef SGM_CASE
+                default: throw CudaError{cudaErrorInvalidValue, "labels exceed 256"};
+            }
+            CK(cudaGetLastError());
+            first = false;
+        }
+    }
+}
+
+// ---- the stage ------------------------------------------------------------------------
+struct StageOutputs {  // device pointers
+    double *depth;
+    float *confidence;
+    uint8_t *provenance;
+    float2 *points[MAX_VIEWS];
+    float *warp_confidence[MAX_VIEWS];
+};
+
+struct Results {  // read back once at the end
+    unsigned long long tested, measured, regularized;
+    unsigned long long target_counts[MAX_VIEWS][3];
+    double median_depth;
+    float median_improvement;
+    int has_median_depth, has_median_improvement;
+};
+
+__global__ void field_stats_kernel(const uint8_t *__restrict__ tested, Field f, int n, Results *res, double *depth_keys,
+                                   float *improvement_keys) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int t = 0, m = 0, r = 0;
+    if (i < n) {
+        t = tested[i];
+        bool has = f.has[i];
+        m = has && !f.regularized[i];
+        r = has && f.regularized[i];
+        depth_keys[i] = has ? f.depth[i] : INFINITY;
+        improvement_keys[i] = m ? f.improvement[i] : INFINITY;
+    }
+    unsigned full = 0xffffffffu;
+    int ct = __popc(__ballot_sync(full, t)), cm = __popc(__ballot_sync(full, m)), cr = __popc(__ballot_sync(full, r));
+    if ((threadIdx.x & 31) == 0) {
+        if (ct) atomicAdd(&res->tested, (unsigned long long)ct);
+        if (cm) atomicAdd(&res->measured, (unsigned long long)cm);
+        if (cr) atomicAdd(&res->regularized, (unsigned long long)cr);
+    }
+}
+
+__global__ void medians_kernel(const double *sorted_depth, const float *sorted_improvement, Results *res) {
+    unsigned long long nd = res->measured + res->regularized, ni = res->measured;
+    res->has_median_depth = nd > 0;
+    res->median_depth = nd > 0 ? sorted_depth[nd / 2] : 0.0;
+    res->has_median_improvement = ni > 0;
+    res->median_improvement = ni > 0 ? sorted_improvement[ni / 2] : 0.0f;
+}
+
+__global__ void depth_map_kernel(Field f, const uint8_t *__restrict__ tested, double *depth, float *confidence,
+                                 uint8_t *provenance, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (f.has[i]) {
+        depth[i] = f.depth[i];
+        confidence[i] = f.confidence[i];
+        provenance[i] = f.regularized[i] ? CHIARO_REGULARIZED : CHIARO_MEASURED;
+    } else {
+        depth[i] = NAN;
+        confidence[i] = tested[i] ? 1.0f : 0.0f;
+        provenance[i] = tested[i] ? CHIARO_GLOBAL : CHIARO_UNSUPPORTED;
+    }
+}
+
+Field field_bufs(chiaro_depth_ctx *ctx, const std::string &name, size_t n) {
+    Field f;
+    f.has = dbuf<uint8_t>(ctx, name + ".has", n);
+    f.depth = dbuf<double>(ctx, name + ".depth", n);
+    f.confidence = dbuf<float>(ctx, name + ".confidence", n);
+    f.improvement = dbuf<float>(ctx, name + ".improvement", n);
+    f.regularized = dbuf<uint8_t>(ctx, name + ".regularized", n);
+    return f;
+}
+
+void copy_field(chiaro_depth_ctx *ctx, const Field &dst, const Field &src, size_t n) {
+    CK(cudaMemcpyAsync(dst.has, src.has, n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.depth, src.depth, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.confidence, src.confidence, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.improvement, src.improvement, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.regularized, src.regularized, n, cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+Decisions decision_bufs(chiaro_depth_ctx *ctx, const std::string &name, size_t n) {
+    Decisions d;
+    d.kind = dbuf<uint8_t>(ctx, name + ".kind", n);
+    d.global = dbuf<float2>(ctx, name + ".global", n);
+    d.point = dbuf<float2>(ctx, name + ".point", n);
+    d.confidence = dbuf<float>(ctx, name + ".confidence", n);
+    d.measured = dbuf<uint8_t>(ctx, name + ".measured", n);
+    return d;
+}
+
+void copy_decisions(chiaro_depth_ctx *ctx, const Decisions &dst, const Decisions &src, size_t n) {
+    CK(cudaMemcpyAsync(dst.kind, src.kind, n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.global, src.global, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.point, src.point, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.confidence, src.confidence, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dst.measured, src.measured, n, cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+void download_field(chiaro_depth_ctx *ctx, const Field &f, size_t n, uint8_t *has, double *depth, float *confidence,
+                    float *improvement, uint8_t *regularized) {
+    download(ctx, has, f.has, n);
+    download(ctx, depth, f.depth, n);
+    download(ctx, confidence, f.confidence, n);
+    download(ctx, improvement, f.improvement, n);
+    download(ctx, regularized, f.regularized, n);
+}
+
+// Run the whole stage on device-resident views. h_views: the DevView array
+// (device pointers inside), d_views: its device copy.
+void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const DevView *d_views, int reference,
+               const chiaro_depth_options &o, const Grids &g, const StageOutputs &out, Results *d_results,
+               Results &h_results, const chiaro_depth_debug *debug, std::vector<int> &rewritten) {
+    cudaStream_t s = ctx->stream;
+    set_smem_limits();
+    const int n_views = (int)h_views.size();
+    std::vector<int> targets;
+    for (int i = 0; i < n_views; ++i)
+        if (i != reference && h_views[i].accepted && h_views[i].has_camera) targets.push_back(i);
+    const int V = (int)targets.size();
+    const int D = (int)o.planes + 1;
+    const int radius = (int)o.patch_radius;
+    const int direct_radius = std::max(radius, 3), wide_radius = std::max(2 * radius, 8);
+    const size_t N = g.coarse_columns * g.coarse_rows, M = g.columns * g.rows;
+    const double inverse_step = (1.0 / o.near_depth - 1.0 / o.far_depth) / (double)(o.planes - 1);
+
+    // constant tables
+    auto finite_depths = inverse_depth_samples(o.near_depth, o.far_depth, o.planes);
+    std::vector<double> labels(D);
+    labels[0] = NAN;
+    for (int l = 1; l < D; ++l) labels[l] = finite_depths[o.planes - l];
+    auto unseeded = inverse_depth_samples(o.near_depth, o.far_depth, 32);
+    std::reverse(unseeded.begin(), unseeded.end());
+    auto sp = spatial_weights(radius), sp_direct = spatial_weights(direct_radius),
+         sp_wide = spatial_weights(wide_radius);
+    std::vector<double> spatial25(25);
+    for (int dy = -2; dy <= 2; ++dy)
+        for (int dx = -2; dx <= 2; ++dx) spatial25[(dy + 2) * 5 + dx + 2] = std::exp((double)(-(dx * dx + dy * dy)) / 6.0);
+    double *d_labels = dbuf<double>(ctx, "labels", D);
+    double *d_unseeded = dbuf<double>(ctx, "unseeded", 32);
+    float *d_sp = dbuf<float>(ctx, "spatial", sp.size());
+    float *d_sp_direct = dbuf<float>(ctx, "spatial_direct", sp_direct.size());
+    float *d_sp_wide = dbuf<float>(ctx, "spatial_wide", sp_wide.size());
+    double *d_sp25 = dbuf<double>(ctx, "spatial25", 25);
+    upload(ctx, d_labels, labels.data(), D);
+    upload(ctx, d_unseeded, unseeded.data(), 32);
+    upload(ctx, d_sp, sp.data(), sp.size());
+    upload(ctx, d_sp_direct, sp_direct.data(), sp_direct.size());
+    upload(ctx, d_sp_wide, sp_wide.data(), sp_wide.size());
+    upload(ctx, d_sp25, spatial25.data(), 25);
+    CK(cudaMemsetAsync(d_results, 0, sizeof(Results), s));
+
+    CK(cudaEventRecord(ctx->events[0], s));
+    // ---- cost volume
+    float *scores = dbuf<float>(ctx, "scores", N * D);
+    float *costs = dbuf<float>(ctx, "costs", N * D);
+    float *guidance = dbuf<float>(ctx, "guidance", N);
+    uint8_t *tested = dbuf<uint8_t>(ctx, "tested", N);
+    {
+        CostParams p{};
+        p.views = d_views;
+        p.reference = reference;
+        p.n_targets = V;
+        for (int v = 0; v < V; ++v) p.targets[v] = targets[v];
+        p.columns = (int)g.coarse_columns;
+        p.rows = (int)g.coarse_rows;
+        p.step = (int)g.coarse_step;
+        p.labels = D;
+        p.label_depth = d_labels;
+        p.spatial = d_sp;
+        p.radius = radius;
+        p.minimum_support = (int)o.minimum_support;
+        p.best_view_count = (int)std::min<uint64_t>(o.best_view_count, MAX_VIEWS);
+        p.scores = scores;
+        p.costs = costs;
+        p.guidance = guidance;
+        p.tested = tested;
+        int taps = (2 * radius + 1) * (2 * radius + 1);
+        unsigned threads = (unsigned)std::min(256, (D + 31) / 32 * 32);
+        cost_volume_kernel<<<(unsigned)N, threads, node_smem_bytes(V, taps), s>>>(p);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(ctx->events[1], s));
+    // ---- SGM
+    float *regularised = dbuf<float>(ctx, "regularised", N * D);
+    launch_sgm(ctx, costs, guidance, regularised, (int)g.coarse_columns, (int)g.coarse_rows, D);
+    CK(cudaEventRecord(ctx->events[2], s));
+    // ---- select (+ completion)
+    Field coarse = field_bufs(ctx, "coarse", N);
+    uint8_t *fillable = dbuf<uint8_t>(ctx, "fillable", N);
+    {
+        SelectParams p{};
+        p.scores = scores;
+        p.regularised = regularised;
+        p.tested = tested;
+        p.label_depth = d_labels;
+        p.nodes = (int)N;
+        p.labels = D;
+        p.minimum_score = o.minimum_score;
+        p.minimum_margin = o.minimum_margin;
+        p.minimum_improvement = o.minimum_improvement;
+        p.field = coarse;
+        p.fillable = fillable;
+        select_depths_kernel<<<blocks_for(N * 32, 256), 256, 0, s>>>(p);
+        CK(cudaGetLastError());
+    }
+    if (o.completion_iterations > 0) {
+        Field other = field_bufs(ctx, "coarse2", N);
+        Field src = coarse, dst = other;
+        for (uint64_t it = 0; it < o.completion_iterations; ++it) {
+            copy_field(ctx, dst, src, N);
+            CompleteParams p{src, dst, guidance, fillable, (int)g.coarse_columns, (int)g.coarse_rows,
+                             (int)o.minimum_neighbour_support};
+            complete_depth_kernel<<<blocks_for(N, 256), 256, 0, s>>>(p);
+            CK(cudaGetLastError());
+            std::swap(src, dst);
+        }
+        if (src.has != coarse.has) copy_field(ctx, coarse, src, N);
+    }
+    if (debug) {
+        download(ctx, debug->coarse_scores, scores, N * D);
+        download(ctx, debug->coarse_costs, costs, N * D);
+        download(ctx, debug->coarse_guidance, guidance, N);
+        download(ctx, debug->coarse_tested, tested, N);
+        download(ctx, debug->regularised, regularised, N * D);
+        download_field(ctx, coarse, N, debug->coarse_has, debug->coarse_depth, debug->coarse_confidence,
+                       debug->coarse_improvement, debug->coarse_regularized);
+        download(ctx, debug->coarse_fillable, fillable, N);
+    }
+    CK(cudaEventRecord(ctx->events[3], s));
+    // ---- direct measurement
+    Field direct = field_bufs(ctx, "direct", M);
+    float *fguidance = dbuf<float>(ctx, "fine_guidance", M);
+    uint8_t *ftested = dbuf<uint8_t>(ctx, "fine_tested", M);
+    {
+        DirectParams p{};
+        p.views = d_views;
+        p.reference = reference;
+        p.n_targets = V;
+        for (int v = 0; v < V; ++v) p.targets[v] = targets[v];
+        p.columns = (int)g.columns;
+        p.rows = (int)g.rows;
+        p.step = (int)g.step;
+        p.coarse = coarse;
+        p.coarse_columns = (int)g.coarse_columns;
+        p.coarse_rows = (int)g.coarse_rows;
+        p.coarse_step = (int)g.coarse_step;
+        p.inverse_step = inverse_step;
+        p.near_depth = o.near_depth;
+        p.far_depth = o.far_depth;
+        p.unseeded = d_unseeded;
+        p.radius = direct_radius;
+        p.wide_radius = wide_radius;
+        p.spatial = d_sp_direct;
+        p.spatial_wide = d_sp_wide;
+        p.minimum_score = o.minimum_score;
+        p.minimum_margin = o.minimum_margin;
+        p.minimum_improvement = o.minimum_improvement;
+        p.minimum_support = (int)o.minimum_support;
+        p.best_view_count = (int)std::min<uint64_t>(o.best_view_count, MAX_VIEWS);
+        p.out = direct;
+        p.guidance = fguidance;
+        p.tested = ftested;
+        int taps_max = std::max((2 * wide_radius + 1) * (2 * wide_radius + 1), (2 * direct_radius + 1) * (2 * direct_radius + 1));
+        direct_depth_kernel<<<(unsigned)M, 128, node_smem_bytes(V, taps_max), s>>>(p);
+        CK(cudaGetLastError());
+    }
+    if (debug) {
+        download_field(ctx, direct, M, debug->direct_has, debug->direct_depth, debug->direct_confidence,
+                       debug->direct_improvement, debug->direct_regularized);
+        download(ctx, debug->direct_guidance, fguidance, M);
+        download(ctx, debug->direct_tested, ftested, M);
+    }
+    CK(cudaEventRecord(ctx->events[4], s));
+    // ---- consistency filters (depth.rs:383-392)
+    uint8_t *has_a = dbuf<uint8_t>(ctx, "has_isolated", M);
+    reject_isolated_kernel<<<blocks_for(M, 256), 256, 0, s>>>(direct.has, direct.depth, direct.confidence, fguidance,
+                                                             has_a, (int)g.columns, (int)g.rows, inverse_step * 2.5);
+    CK(cudaGetLastError());
+    if (debug) download(ctx, debug->isolated_has, has_a, M);
+    int *parent = dbuf<int>(ctx, "uf_parent", M);
+    int *csize = dbuf<int>(ctx, "uf_size", M);
+    components_init_kernel<<<blocks_for(M, 256), 256, 0, s>>>(parent, (int)M);
+    CK(cudaMemsetAsync(csize, 0, M * sizeof(int), s));
+    components_union_kernel<<<blocks_for(M, 256), 256, 0, s>>>(has_a, direct.depth, fguidance, parent, (int)g.columns,
+                                                               (int)g.rows, inverse_step * 2.5);
+    components_size_kernel<<<blocks_for(M, 256), 256, 0, s>>>(has_a, parent, csize, (int)M);
+    Field fin = field_bufs(ctx, "final", M);
+    components_mark_kernel<<<blocks_for(M, 256), 256, 0, s>>>(has_a, parent, csize, fin.has, (int)M,
+                                                              MINIMUM_DIRECT_COMPONENT_NODES);
+    CK(cudaGetLastError());
+    if (debug) download(ctx, debug->component_has, fin.has, M);
+    fit_local_planes_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin.has, direct.depth, direct.confidence, fguidance,
+                                                               d_sp25, fin.depth, (int)g.columns, (int)g.rows,
+                                                               inverse_step * 4.0);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(fin.confidence, direct.confidence, M * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(fin.improvement, direct.improvement, M * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(fin.regularized, direct.regularized, M, cudaMemcpyDeviceToDevice, s));
+    // depth of removed nodes: NaN (None)
+    if (debug && debug->fitted_depth) {
+        std::vector<uint8_t> h(M);
+        download(ctx, h.data(), fin.has, M);
+        download(ctx, debug->fitted_depth, fin.depth, M);
+        CK(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < M; ++i)
+            if (!h[i]) debug->fitted_depth[i] = NAN;
+    }
+    // report statistics and medians
+    double *depth_keys = dbuf<double>(ctx, "depth_keys", M);
+    double *depth_sorted = dbuf<double>(ctx, "depth_sorted", M);
+    float *imp_keys = dbuf<float>(ctx, "imp_keys", M);
+    float *imp_sorted = dbuf<float>(ctx, "imp_sorted", M);
+    field_stats_kernel<<<blocks_for(M, 256), 256, 0, s>>>(ftested, fin, (int)M, d_results, depth_keys, imp_keys);
+    CK(cudaGetLastError());
+    {
+        size_t t1 = 0, t2 = 0;
+        CK(cub::DeviceRadixSort::SortKeys(nullptr, t1, depth_keys, depth_sorted, (int)M, 0, 64, s));
+        CK(cub::DeviceRadixSort::SortKeys(nullptr, t2, imp_keys, imp_sorted, (int)M, 0, 32, s));
+        void *tmp = dbuf<unsigned char>(ctx, "cub_tmp", std::max(t1, t2));
+        CK(cub::DeviceRadixSort::SortKeys(tmp, t1, depth_keys, depth_sorted, (int)M, 0, 64, s));
+        CK(cub::DeviceRadixSort::SortKeys(tmp, t2, imp_keys, imp_sorted, (int)M, 0, 32, s));
+    }
+    medians_kernel<<<1, 1, 0, s>>>(depth_sorted, imp_sorted, d_results);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->events[5], s));
+    // ---- per-target decisions (depth.rs:420-547)
+    Decisions dec = decision_bufs(ctx, "dec", M), dec2 = decision_bufs(ctx, "dec2", M),
+              dec3 = decision_bufs(ctx, "dec3", M);
+    rewritten.clear();
+    for (int t : targets) {
+        DecisionParams p{};
+        p.views = d_views;
+        p.reference = reference;
+        p.target = t;
+        p.columns = (int)g.columns;
+        p.rows = (int)g.rows;
+        p.step = (int)g.step;
+        p.field = fin;
+        p.inverse_step = inverse_step;
+        p.near_depth = o.near_depth;
+        p.far_depth = o.far_depth;
+        p.radius = radius;
+        p.spatial = d_sp;
+        p.minimum_score = o.minimum_score;
+        p.out = dec;
+        int taps = (2 * radius + 1) * (2 * radius + 1);
+        target_decision_kernel<<<(unsigned)M, 32, node_smem_bytes(1, taps), s>>>(p);
+        CK(cudaGetLastError());
+        copy_decisions(ctx, dec2, dec, M);
+        warp_consensus_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec, dec2, (int)g.columns, (int)g.rows);
+        copy_decisions(ctx, dec3, dec2, M);
+        warp_boundary_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec2, dec3, fguidance, (int)g.columns, (int)g.rows);
+        warp_output_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec3, out.points[t], out.warp_confidence[t],
+                                                              d_results->target_counts[t], (int)M);
+        CK(cudaGetLastError());
+        if (debug && debug->decision_kind) download(ctx, debug->decision_kind + (size_t)t * M, dec3.kind, M);
+        rewritten.push_back(t);
+    }
+    depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->events[6], s));
+    // cost 1, SGM 8, select 1, completion, direct 1, filters 6, stats 2, 4 per target, map 1
+    ctx->launches = 1 + 8 + 1 + (int)o.completion_iterations + 1 + 6 + 2 + 4 * V + 1;
+    CK(cudaMemcpyAsync(&h_results, d_results, sizeof(Results), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ctx->timings[i], ctx->events[i], ctx->events[i + 1]));
+    CK(cudaEventElapsedTime(&ctx->timings[6], ctx->events[0], ctx->events[6]));
+}
+
+float fraction(unsigned long long count, unsigned long long total) {
+    return total == 0 ? 0.0f : (float)count / (float)total;
+}
+
+void fill_reports(const Results &r, const std::vector<int> &rewritten, size_t n_views, chiaro_depth_report *reports) {
+    if (!reports) return;
+    for (size_t i = 0; i < n_views; ++i) reports[i].present = 0;
+    unsigned long long fallback =
+        r.tested >= r.measured + r.regularized ? r.tested - (r.measured + r.regularized) : 0;
+    for (int t : rewritten) {
+        chiaro_depth_report &rep = reports[t];
+        rep.present = 1;
+        rep.tested_nodes = r.tested;
+        rep.measured_nodes = r.measured;
+        rep.regularized_nodes = r.regularized;
+        rep.fallback_nodes = fallback;
+        rep.refined_nodes = r.target_counts[t][0];
+        rep.occluded_nodes = r.target_counts[t][1];
+        rep.boundary_nodes = r.target_counts[t][2];
+        rep.reconstructed_fraction = fraction(r.measured + r.regularized, r.tested);
+        rep.refined_fraction = fraction(r.target_counts[t][0], r.tested);
+        rep.occluded_fraction = fraction(r.target_counts[t][1], r.tested);
+        rep.has_median_depth = r.has_median_depth;
+        rep.median_depth = r.has_median_depth ? r.median_depth : 0.0;
+        rep.has_median_score_improvement = r.has_median_improvement;
+        rep.median_score_improvement = r.has_median_improvement ? r.median_improvement : 0.0f;
+    }
+}
+
+int validate(const chiaro_view *views, size_t n_views, size_t reference_index, const chiaro_depth_options *options) {
+    if (!views || !options) return CHIARO_ERR_ARGUMENT;
+    if (!options_valid(*options) || reference_index >= n_views || !views[reference_index].has_camera)
+        return CHIARO_INVALID;
+    if (n_views > (size_t)MAX_VIEWS || options->planes + 1 > (uint64_t)MAX_LABELS ||
+        options->patch_radius > (uint64_t)MAX_RADIUS)
+        return CHIARO_ERR_ARGUMENT;
+    for (size_t i = 0; i < n_views; ++i) {
+        const chiaro_view &v = views[i];
+        if (!v.luminance || v.luma_width < 1 || v.luma_height < 1 || !v.warp.points || v.warp.step < 1 ||
+            v.warp.columns < 1 || v.warp.rows < 1)
+            return CHIARO_ERR_ARGUMENT;
+    }
+    return CHIARO_OK;
+}
+
+DevView dev_view(const chiaro_view &v, const float *luma, const float2 *points) {
+    DevView d{};
+    d.luma.data = luma;
+    d.luma.width = (int)v.luma_width;
+    d.luma.height = (int)v.luma_height;
+    d.warp.points = points;
+    d.warp.step = (int)v.warp.step;
+    d.warp.columns = (int)v.warp.columns;
+    d.warp.rows = (int)v.warp.rows;
+    d.width = (int)v.width;
+    d.height = (int)v.height;
+    d.has_camera = v.has_camera != 0;
+    d.accepted = v.accepted != 0;
+    if (v.has_camera) camera_from_abi(v.camera, d.cam);
+    return d;
+}
+
+int refine(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views, size_t reference_index,
+           const chiaro_depth_options *options, chiaro_warp *refined, chiaro_depth_report *reports,
+           chiaro_depth_map *out_map, const chiaro_depth_debug *debug, bool device_pointers) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    int st = validate(views, n_views, reference_index, options);
+    if (st != CHIARO_OK) {
+        if (reports && st == CHIARO_INVALID)
+            for (size_t i = 0; i < n_views; ++i) reports[i].present = 0;
+        return st;
+    }
+    const chiaro_depth_options &o = *options;
+    Grids g = grids_for(views[reference_index].width, views[reference_index].height, o);
+    const size_t M = g.columns * g.rows;
+    if (!out_map || out_map->capacity < M || !out_map->depth || !out_map->confidence || !out_map->provenance)
+        return CHIARO_ERR_CAPACITY;
+    for (size_t t = 0; t < n_views; ++t) {
+        bool target = t != reference_index && views[t].accepted && views[t].has_camera;
+        if (target && (!refined || refined[t].capacity < M || !refined[t].points || !refined[t].confidence))
+            return CHIARO_ERR_CAPACITY;
+    }
+    try {
+        CK(cudaSetDevice(ctx->device));
+        std::vector<DevView> h_views(n_views);
+        for (size_t i = 0; i < n_views; ++i) {
+            const chiaro_view &v = views[i];
+            size_t luma_n = v.luma_width * v.luma_height, warp_n = v.warp.columns * v.warp.rows;
+            const float *luma = v.luminance;
+            const float2 *pts = reinterpret_cast<const float2 *>(v.warp.points);
+            if (!device_pointers) {
+                float *dl = dbuf<float>(ctx, "luma" + std::to_string(i), luma_n);
+                float2 *dp = dbuf<float2>(ctx, "warp" + std::to_string(i), warp_n);
+                upload(ctx, dl, v.luminance, luma_n);
+                upload(ctx, dp, reinterpret_cast<const float2 *>(v.warp.points), warp_n);
+                luma = dl;
+                pts = dp;
+            }
+            h_views[i] = dev_view(v, luma, pts);
+        }
+        DevView *d_views = dbuf<DevView>(ctx, "views", n_views);
+        upload(ctx, d_views, h_views.data(), n_views);
+        StageOutputs out{};
+        if (device_pointers) {
+            out.depth = out_map->depth;
+            out.confidence = out_map->confidence;
+            out.provenance = out_map->provenance;
+            for (size_t t = 0; t < n_views; ++t)
+                if (refined && refined[t].points) {
+                    out.points[t] = reinterpret_cast<float2 *>(refined[t].points);
+                    out.warp_confidence[t] = refined[t].confidence;
+                }
+        } else {
+            out.depth = dbuf<double>(ctx, "out.depth", M);
+            out.confidence = dbuf<float>(ctx, "out.confidence", M);
+            out.provenance = dbuf<uint8_t>(ctx, "out.provenance", M);
+            for (size_t t = 0; t < n_views; ++t) {
+                out.points[t] = dbuf<float2>(ctx, "out.points" + std::to_string(t), M);
+                out.warp_confidence[t] = dbuf<float>(ctx, "out.wconf" + std::to_string(t), M);
+            }
+        }
+        Results *d_results = dbuf<Results>(ctx, "results", 1);
+        Results h_results{};
+        std::vector<int> rewritten;
+        run_stage(ctx, h_views, d_views, (int)reference_index, o, g, out, d_results, h_results, debug, rewritten);
+        if (!device_pointers) {
+            download(ctx, out_map->depth, out.depth, M);
+            download(ctx, out_map->confidence, out.confidence, M);
+            download(ctx, out_map->provenance, out.provenance, M);
+            for (int t : rewritten) {
+                download(ctx, reinterpret_cast<float2 *>(refined[t].points), out.points[t], M);
+                download(ctx, refined[t].confidence, out.warp_confidence[t], M);
+            }
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        out_map->columns = g.columns;
+        out_map->rows = g.rows;
+        out_map->step = g.step;
+        out_map->near_depth = o.near_depth;
+        out_map->far_depth = o.far_depth;
+        for (int t : rewritten) {
+            refined[t].step = g.step;
+            refined[t].columns = g.columns;
+            refined[t].rows = g.rows;
+        }
+        fill_reports(h_results, rewritten, n_views, reports);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------
+extern "C" {
+
+int chiaro_depth_abi_version(void) { return CHIARO_DEPTH_ABI_VERSION; }
+
+int chiaro_depth_ctx_create(int device, chiaro_depth_ctx **out) {
+    if (!out) return CHIARO_ERR_ARGUMENT;
+    *out = nullptr;
+    auto *ctx = new chiaro_depth_ctx();
+    ctx->device = device;
+    try {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        for (auto &e : ctx->events) CK(cudaEventCreate(&e));
+    } catch (const CudaError &e) {
+        delete ctx;
+        return CHIARO_ERR_CUDA;
+    }
+    *out = ctx;
+    return CHIARO_OK;
+}
+
+void chiaro_depth_ctx_destroy(chiaro_depth_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &kv : ctx->buffers)
+        if (kv.second.ptr) cudaFree(kv.second.ptr);
+    for (auto &e : ctx->events)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *chiaro_depth_last_error(const chiaro_depth_ctx *ctx) { return ctx ? ctx->error.c_str() : "no context"; }
+
+void chiaro_depth_options_default(chiaro_depth_options *o) {  // depth.rs:69-91
+    if (!o) return;
+    *o = chiaro_depth_options{};
+    o->enabled = 1;
+    o->grid_step = 8;
+    o->near_depth = 500.0;
+    o->far_depth = 10000000.0;
+    o->planes = 96;
+    o->patch_radius = 4;
+    o->minimum_support = 2;
+    o->best_view_count = 3;
+    o->minimum_score = 0.45f;
+    o->minimum_margin = 0.01f;
+    o->minimum_improvement = 0.01f;
+    o->minimum_neighbour_support = 2;
+    o->completion_iterations = 0;
+}
+
+int chiaro_depth_options_valid(const chiaro_depth_options *o) { return o && options_valid(*o) ? 1 : 0; }
+
+int chiaro_depth_output_shape(uint64_t width, uint64_t height, const chiaro_depth_options *o, uint64_t *columns,
+                              uint64_t *rows, uint64_t *step, uint64_t *coarse_columns, uint64_t *coarse_rows,
+                              uint64_t *coarse_step) {
+    if (!o) return CHIARO_ERR_ARGUMENT;
+    Grids g = grids_for(width, height, *o);
+    if (columns) *columns = g.columns;
+    if (rows) *rows = g.rows;
+    if (step) *step = g.step;
+    if (coarse_columns) *coarse_columns = g.coarse_columns;
+    if (coarse_rows) *coarse_rows = g.coarse_rows;
+    if (coarse_step) *coarse_step = g.coarse_step;
+    return CHIARO_OK;
+}
+
+int chiaro_refine_multiview_depth(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views,
+                                  size_t reference_index, const chiaro_depth_options *options, chiaro_warp *refined,
+                                  chiaro_depth_report *reports, chiaro_depth_map *out_map,
+                                  const chiaro_depth_debug *debug) {
+    return refine(ctx, views, n_views, reference_index, options, refined, reports, out_map, debug, false);
+}
+
+int chiaro_refine_multiview_depth_device(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views,
+                                         size_t reference_index, const chiaro_depth_options *options,
+                                         chiaro_warp *refined, chiaro_depth_report *reports,
+                                         chiaro_depth_map *out_map) {
+    return refine(ctx, views, n_views, reference_index, options, refined, reports, out_map, nullptr, true);
+}
+
+int chiaro_depth_last_timings(const chiaro_depth_ctx *ctx, float *ms, int capacity) {
+    if (!ctx || !ms) return 0;
+    int n = std::min(capacity, 7);
+    for (int i = 0; i < n; ++i) ms[i] = ctx->timings[i];
+    return n;
+}
+
+int chiaro_depth_last_launches(const chiaro_depth_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+void *chiaro_depth_ctx_stream(const chiaro_depth_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int chiaro_sgm_aggregate_device(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, uint64_t columns,
+                                uint64_t rows, uint64_t labels, float *out) {
+    if (!ctx || !costs || !guidance || !out || columns < 1 || rows < 1 || labels < 1 || labels > MAX_LABELS)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        launch_sgm(ctx, costs, guidance, out, (int)columns, (int)rows, (int)labels);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_sgm_aggregate(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, uint64_t columns,
+                         uint64_t rows, uint64_t labels, float *out) {
+    if (!ctx || !costs || !guidance || !out || columns < 1 || rows < 1 || labels < 1 || labels > MAX_LABELS)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        size_t n = columns * rows, nl = n * labels;
+        float *dc = dbuf<float>(ctx, "op.costs", nl), *dg = dbuf<float>(ctx, "op.guidance", n),
+              *dout = dbuf<float>(ctx, "op.out", nl);
+        upload(ctx, dc, costs, nl);
+        upload(ctx, dg, guidance, n);
+        launch_sgm(ctx, dc, dg, dout, (int)columns, (int)rows, (int)labels);
+        download(ctx, out, dout, nl);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_select_depths(chiaro_depth_ctx *ctx, const double *labels, uint64_t n_labels, const float *scores,
+                         const float *regularised, const uint8_t *tested, uint64_t n_nodes,
+                         const chiaro_depth_options *options, uint8_t *has, double *depth, float *confidence,
+                         float *improvement, uint8_t *regularized, uint8_t *fillable) {
+    if (!ctx || !labels || !scores || !regularised || !tested || !options || n_labels < 2 || n_labels > MAX_LABELS)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        size_t nl = n_nodes * n_labels;
+        double *dl = dbuf<double>(ctx, "op.labels", n_labels);
+        float *ds = dbuf<float>(ctx, "op.scores", nl), *dr = dbuf<float>(ctx, "op.reg", nl);
+        uint8_t *dt = dbuf<uint8_t>(ctx, "op.tested", n_nodes);
+        Field f = field_bufs(ctx, "op.field", n_nodes);
+        uint8_t *dfill = dbuf<uint8_t>(ctx, "op.fillable", n_nodes);
+        upload(ctx, dl, labels, n_labels);
+        upload(ctx, ds, scores, nl);
+        upload(ctx, dr, regularised, nl);
+        upload(ctx, dt, tested, n_nodes);
+        SelectParams p{};
+        p.scores = ds;
+        p.regularised = dr;
+        p.tested = dt;
+        p.label_depth = dl;
+        p.nodes = (int)n_nodes;
+        p.labels = (int)n_labels;
+        p.minimum_score = options->minimum_score;
+        p.minimum_margin = options->minimum_margin;
+        p.minimum_improvement = options->minimum_improvement;
+        p.field = f;
+        p.fillable = dfill;
+        select_depths_kernel<<<blocks_for(n_nodes * 32, 256), 256, 0, ctx->stream>>>(p);
+        CK(cudaGetLastError());
+        download_field(ctx, f, n_nodes, has, depth, confidence, improvement, regularized);
+        download(ctx, fillable, dfill, n_nodes);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_reject_isolated(chiaro_depth_ctx *ctx, uint8_t *has, const double *depth, const float *confidence,
+                           const float *guidance, uint64_t columns, uint64_t rows, double inverse_tolerance) {
+    if (!ctx || !has || !depth || !confidence || !guidance) return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        size_t n = columns * rows;
+        uint8_t *dh = dbuf<uint8_t>(ctx, "op.has", n), *dh2 = dbuf<uint8_t>(ctx, "op.has2", n);
+        double *dd = dbuf<double>(ctx, "op.depth", n);
+        float *dc = dbuf<float>(ctx, "op.conf", n), *dg = dbuf<float>(ctx, "op.guid", n);
+        upload(ctx, dh, has, n);
+        upload(ctx, dd, depth, n);
+        upload(ctx, dc, confidence, n);
+        upload(ctx, dg, guidance, n);
+        reject_isolated_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(dh, dd, dc, dg, dh2, (int)columns,
+                                                                           (int)rows, inverse_tolerance);
+        CK(cudaGetLastError());
+        download(ctx, has, dh2, n);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_reject_small_components(chiaro_depth_ctx *ctx, uint8_t *has, const double *depth, const float *guidance,
+                                   uint64_t columns, uint64_t rows, double inverse_tolerance, uint64_t minimum_nodes) {
+    if (!ctx || !has || !depth || !guidance) return CHIARO_ERR_ARGUMENT;
+    if (minimum_nodes <= 1) return CHIARO_OK;  // depth.rs:941-943
+    try {
+        CK(cudaSetDevice(ctx->device));
+        size_t n = columns * rows;
+        cudaStream_t s = ctx->stream;
+        uint8_t *dh = dbuf<uint8_t>(ctx, "op.has", n), *dh2 = dbuf<uint8_t>(ctx, "op.has2", n);
+        double *dd = dbuf<double>(ctx, "op.depth", n);
+        float *dg = dbuf<float>(ctx, "op.guid", n);
+        int *parent = dbuf<int>(ctx, "op.parent", n), *size = dbuf<int>(ctx, "op.size", n);
+        upload(ctx, dh, has, n);
+        upload(ctx, dd, depth, n);
+        upload(ctx, dg, guidance, n);
+        components_init_kernel<<<blocks_for(n, 256), 256, 0, s>>>(parent, (int)n);
+        CK(cudaMemsetAsync(size, 0, n * sizeof(int), s));
+        components_union_kernel<<<blocks_for(n, 256), 256, 0, s>>>(dh, dd, dg, parent, (int)columns, (int)rows,
+                                                                   inverse_tolerance);
+        components_size_kernel<<<blocks_for(n, 256), 256, 0, s>>>(dh, parent, size, (int)n);
+        components_mark_kernel<<<blocks_for(n, 256), 256, 0, s>>>(dh, parent, size, dh2, (int)n, (int)minimum_nodes);
+        CK(cudaGetLastError());
+        download(ctx, has, dh2, n);
+        CK(cudaStreamSynchronize(s));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_fit_local_planes(chiaro_depth_ctx *ctx, const uint8_t *has, double *depth, const float *confidence,
+                            const float *guidance, uint64_t columns, uint64_t rows, double inverse_tolerance) {
+    if (!ctx || !has || !depth || !confidence || !guidance) return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        size_t n = columns * rows;
+        uint8_t *dh = dbuf<uint8_t>(ctx, "op.has", n);
+        double *dd = dbuf<double>(ctx, "op.depth", n), *dd2 = dbuf<double>(ctx, "op.depth2", n);
+        float *dc = dbuf<float>(ctx, "op.conf", n), *dg = dbuf<float>(ctx, "op.guid", n);
+        std::vector<double> spatial25(25);
+        for (int dy = -2; dy <= 2; ++dy)
+            for (int dx = -2; dx <= 2; ++dx)
+                spatial25[(dy + 2) * 5 + dx + 2] = std::exp((double)(-(dx * dx + dy * dy)) / 6.0);
+        double *d25 = dbuf<double>(ctx, "op.sp25", 25);
+        upload(ctx, d25, spatial25.data(), 25);
+        upload(ctx, dh, has, n);
+        upload(ctx, dd, depth, n);
+        upload(ctx, dc, confidence, n);
+        upload(ctx, dg, guidance, n);
+        fit_local_planes_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(dh, dd, dc, dg, d25, dd2, (int)columns,
+                                                                            (int)rows, inverse_tolerance);
+        CK(cudaGetLastError());
+        download(ctx, depth, dd2, n);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *global, float *point,
+                                 const uint8_t *measured, const float *guidance, uint64_t columns, uint64_t rows,
+                                 int consensus, int boundaries) {
+    if (!ctx || !kind || !global || !point || !measured || !guidance) return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        size_t n = columns * rows;
+        cudaStream_t s = ctx->stream;
+        Decisions a = decision_bufs(ctx, "op.dec", n), b = decision_bufs(ctx, "op.dec2", n);
+        float *dg = dbuf<float>(ctx, "op.guid", n);
+        upload(ctx, a.kind, kind, n);
+        upload(ctx, a.global, reinterpret_cast<const float2 *>(global), n);
+        upload(ctx, a.point, reinterpret_cast<const float2 *>(point), n);
+        upload(ctx, a.measured, measured, n);
+        CK(cudaMemsetAsync(a.confidence, 0, n * 4, s));
+        upload(ctx, dg, guidance, n);
+        if (consensus) {
+            copy_decisions(ctx, b, a, n);
+            warp_consensus_kernel<<<blocks_for(n, 256), 256, 0, s>>>(a, b, (int)columns, (int)rows);
+            std::swap(a, b);
+        }
+        if (boundaries) {
+            copy_decisions(ctx, b, a, n);
+            warp_boundary_kernel<<<blocks_for(n, 256), 256, 0, s>>>(a, b, dg, (int)columns, (int)rows);
+            std::swap(a, b);
+        }
+        CK(cudaGetLastError());
+        download(ctx, kind, a.kind, n);
+        download(ctx, reinterpret_cast<float2 *>(global), a.global, n);
+        download(ctx, reinterpret_cast<float2 *>(point), a.point, n);
+        CK(cudaStreamSynchronize(s));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+}  // extern "C"

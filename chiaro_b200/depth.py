@@ -1,0 +1,331 @@
+"""Host API of the depth stage: the Python form of ``chiaro_fusion::depth``.
+
+``refine_multiview_depth(inputs, reference_index, alignments, options)``
+keeps the signature and the semantics of the Rust function
+(crates/chiaro-fusion/src/depth.rs:312-580): it returns ``None`` where the
+reference returns ``None``, replaces ``alignments[t].warp`` and sets
+``alignments[t].report.depth`` for every accepted calibrated target, and
+returns the ``DenseDepthMap``. All of the work runs in the CUDA library
+``libchiaro_depth.so`` through its C ABI; there is no CPU fallback, and the
+call raises if the library cannot be loaded.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import struct
+import zlib
+from dataclasses import dataclass, field
+from enum import IntEnum
+from pathlib import Path
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .abi import DepthMapC, DepthOptionsC, DepthReportC, ViewC, WarpC, dptr, fptr, u8ptr
+
+
+@dataclass
+class DepthOptions:
+    """DepthOptions with the reference defaults (depth.rs:39-91)."""
+
+    enabled: bool = True
+    grid_step: int = 8
+    near_depth: float = 500.0
+    far_depth: float = 10_000_000.0
+    planes: int = 96
+    patch_radius: int = 4
+    minimum_support: int = 2
+    best_view_count: int = 3
+    minimum_score: float = 0.45
+    minimum_margin: float = 0.01
+    minimum_improvement: float = 0.01
+    minimum_neighbour_support: int = 2
+    completion_iterations: int = 0
+
+    def to_c(self) -> DepthOptionsC:
+        o = DepthOptionsC()
+        o.enabled = 1 if self.enabled else 0
+        o.grid_step = int(self.grid_step)
+        o.near_depth = float(self.near_depth)
+        o.far_depth = float(self.far_depth)
+        o.planes = int(self.planes)
+        o.patch_radius = int(self.patch_radius)
+        o.minimum_support = int(self.minimum_support)
+        o.best_view_count = int(self.best_view_count)
+        o.minimum_score = float(self.minimum_score)
+        o.minimum_margin = float(self.minimum_margin)
+        o.minimum_improvement = float(self.minimum_improvement)
+        o.minimum_neighbour_support = int(self.minimum_neighbour_support)
+        o.completion_iterations = int(self.completion_iterations)
+        return o
+
+    def is_valid(self) -> bool:
+        """valid_options (depth.rs:1879-1891)."""
+        return (self.enabled and self.grid_step > 0 and np.isfinite(self.near_depth)
+                and np.isfinite(self.far_depth) and self.near_depth > 0.0
+                and self.far_depth > self.near_depth and self.planes >= 3 and self.patch_radius > 0
+                and self.minimum_support > 0 and self.best_view_count >= self.minimum_support
+                and self.minimum_neighbour_support > 0)
+
+
+class DepthProvenance(IntEnum):
+    """depth.rs:115-121."""
+
+    Unsupported = abi.UNSUPPORTED
+    Global = abi.GLOBAL
+    Measured = abi.MEASURED
+    Regularized = abi.REGULARIZED
+
+
+@dataclass
+class DenseDepthNode:
+    """depth.rs:123-128."""
+
+    depth: Optional[float]
+    confidence: float
+    provenance: DepthProvenance
+
+
+@dataclass
+class DepthAlignmentReport:
+    """depth.rs:93-113."""
+
+    tested_nodes: int = 0
+    measured_nodes: int = 0
+    regularized_nodes: int = 0
+    fallback_nodes: int = 0
+    refined_nodes: int = 0
+    occluded_nodes: int = 0
+    boundary_nodes: int = 0
+    reconstructed_fraction: float = 0.0
+    refined_fraction: float = 0.0
+    occluded_fraction: float = 0.0
+    median_depth: Optional[float] = None
+    median_score_improvement: Optional[float] = None
+
+    @staticmethod
+    def from_c(r: DepthReportC) -> "DepthAlignmentReport":
+        return DepthAlignmentReport(
+            tested_nodes=r.tested_nodes, measured_nodes=r.measured_nodes,
+            regularized_nodes=r.regularized_nodes, fallback_nodes=r.fallback_nodes,
+            refined_nodes=r.refined_nodes, occluded_nodes=r.occluded_nodes,
+            boundary_nodes=r.boundary_nodes,
+            reconstructed_fraction=float(np.float32(r.reconstructed_fraction)),
+            refined_fraction=float(np.float32(r.refined_fraction)),
+            occluded_fraction=float(np.float32(r.occluded_fraction)),
+            median_depth=float(r.median_depth) if r.has_median_depth else None,
+            median_score_improvement=(float(np.float32(r.median_score_improvement))
+                                      if r.has_median_score_improvement else None))
+
+
+@dataclass
+class DenseDepthMap:
+    """depth.rs:133-141, stored as arrays: ``depth`` (NaN = None),
+    ``confidence`` and ``provenance`` of ``columns * rows`` nodes."""
+
+    columns: int
+    rows: int
+    step: int
+    near_depth: float
+    far_depth: float
+    depth: np.ndarray
+    confidence: np.ndarray
+    provenance: np.ndarray
+
+    @property
+    def nodes(self) -> List[DenseDepthNode]:
+        return [self._node(i) for i in range(self.columns * self.rows)]
+
+    def _node(self, i: int) -> DenseDepthNode:
+        d = float(self.depth[i])
+        return DenseDepthNode(None if np.isnan(d) else d, float(self.confidence[i]),
+                              DepthProvenance(int(self.provenance[i])))
+
+    def node(self, column: int, row: int) -> Optional[DenseDepthNode]:
+        """depth.rs:144-146."""
+        if column < self.columns and row < self.rows:
+            return self._node(row * self.columns + column)
+        return None
+
+    def sample_nearest(self, x: float, y: float) -> Optional[DenseDepthNode]:
+        """depth.rs:152-159: nearest node, no interpolation."""
+        if x < 0.0 or y < 0.0 or self.step == 0:
+            return None
+        column = int(_round_half_away(np.float32(x) / np.float32(self.step)))
+        row = int(_round_half_away(np.float32(y) / np.float32(self.step)))
+        return self.node(column, row)
+
+    def diagnostic_samples(self):
+        """depth.rs:200-222: (inverse-depth u16[n], provenance u16[3n])."""
+        near_inverse = 1.0 / self.near_depth
+        far_inverse = 1.0 / self.far_depth
+        rng = max(near_inverse - far_inverse, np.finfo(np.float64).tiny)
+        has = np.isin(self.provenance, (abi.MEASURED, abi.REGULARIZED))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            normalized = np.clip((1.0 / self.depth - far_inverse) / rng, 0.0, 1.0)
+        encoded = np.where(has, 1 + _round_u16(normalized * 65534.0).astype(np.int64), 0).astype(np.uint16)
+        conf = np.clip(self.confidence.astype(np.float32), np.float32(0), np.float32(1))
+        scale = (np.float32(0.35) + np.float32(0.65) * conf).astype(np.float64)
+        color = np.zeros((len(self.provenance), 3), dtype=np.uint16)
+        color[self.provenance == abi.GLOBAL] = (0, 0, 32768)
+        m = self.provenance == abi.MEASURED
+        color[m, 1] = _round_u16(65535.0 * scale[m])
+        r = self.provenance == abi.REGULARIZED
+        color[r, 0] = _round_u16(65535.0 * scale[r])
+        color[r, 1] = _round_u16(32768.0 * scale[r])
+        return encoded, color.reshape(-1)
+
+    def visualization_samples(self) -> np.ndarray:
+        """depth.rs:224-245: logarithmic depth colouring, u16[3n]."""
+        log_range = np.log(self.far_depth / self.near_depth)
+        has = np.isin(self.provenance, (abi.MEASURED, abi.REGULARIZED))
+        out = np.zeros((len(self.provenance), 3), dtype=np.uint16)
+        if has.any():
+            d = self.depth[has]
+            normalized = np.clip((np.log(self.far_depth) - np.log(d)) / log_range, 0.0, 1.0)
+            conf = 0.45 + 0.55 * np.clip(self.confidence[has].astype(np.float32), np.float32(0),
+                                         np.float32(1)).astype(np.float64)
+            base = _depth_color(normalized)
+            out[has] = _round_u16(base.astype(np.float64) * conf[:, None])
+        out[(~has) & (self.provenance == abi.GLOBAL)] = (0, 0, 12000)
+        return out.reshape(-1)
+
+    def write_diagnostics(self, inverse_depth_path, provenance_path) -> None:
+        """depth.rs:166-184: 16-bit gray inverse depth + 16-bit RGB provenance PNGs."""
+        depth, prov = self.diagnostic_samples()
+        _write_png16(Path(inverse_depth_path), self.columns, self.rows, depth, 1)
+        _write_png16(Path(provenance_path), self.columns, self.rows, prov, 3)
+
+    def write_visualization(self, path) -> None:
+        """depth.rs:191-198."""
+        _write_png16(Path(path), self.columns, self.rows, self.visualization_samples(), 3)
+
+
+def _round_half_away(v):
+    """Rust `round()`: half away from zero (v - trunc(v) is exact)."""
+    v = np.asarray(v)
+    t = np.trunc(v)
+    return np.where(np.abs(v - t) >= 0.5, t + np.sign(v), t)
+
+
+def _round_u16(v):
+    r = _round_half_away(np.asarray(v, dtype=np.float64))
+    return np.clip(np.nan_to_num(r, nan=0.0), 0, 65535).astype(np.uint16)
+
+
+def _depth_color(normalized: np.ndarray) -> np.ndarray:
+    """depth.rs:1861-1877."""
+    stops = np.array([[0.0, 0.1, 0.7], [0.0, 0.9, 1.0], [0.0, 1.0, 0.2], [1.0, 0.9, 0.0], [1.0, 0.0, 0.0]])
+    position = np.clip(normalized, 0.0, 1.0) * 4.0
+    lower = np.minimum(np.floor(position).astype(np.int64), 4)
+    upper = np.minimum(lower + 1, 4)
+    frac = (position - lower)[:, None]
+    return _round_u16((stops[lower] * (1.0 - frac) + stops[upper] * frac) * 65535.0)
+
+
+def _write_png16(path: Path, width: int, height: int, samples: np.ndarray, channels: int) -> None:
+    """Minimal 16-bit PNG writer (gray or RGB), written atomically."""
+    data = np.asarray(samples, dtype=">u2").reshape(height, width * channels)
+    raw = b"".join(b"\x00" + row.tobytes() for row in data)
+
+    def chunk(tag: bytes, payload: bytes) -> bytes:
+        return (struct.pack(">I", len(payload)) + tag + payload
+                + struct.pack(">I", zlib.crc32(tag + payload) & 0xFFFFFFFF))
+
+    color_type = 0 if channels == 1 else 2
+    png = (b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", width, height, 16, color_type, 0, 0, 0))
+           + chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b""))
+    tmp = path.with_name(path.name + ".tmp")
+    tmp.write_bytes(png)
+    tmp.replace(path)
+
+
+def output_shape(width: int, height: int, options: DepthOptions):
+    """Grids of the stage: ((columns, rows, step), (coarse_columns, coarse_rows, coarse_step))
+    (depth.rs:326-328 and depth.rs:726-728)."""
+    coarse_step = max(options.grid_step, 4)
+    step = max(coarse_step // 2, 4)
+    return ((-(-width // step) + 1, -(-height // step) + 1, step),
+            (-(-width // coarse_step) + 1, -(-height // coarse_step) + 1, coarse_step))
+
+
+def pack_views(inputs: Sequence, alignments: Sequence):
+    """Fill the C view array; returns (views, keepalive)."""
+    n = len(inputs)
+    views = (ViewC * n)()
+    keep = []
+    for i, (inp, al) in enumerate(zip(inputs, alignments)):
+        luma = np.ascontiguousarray(inp.luminance.data, dtype=np.float32)
+        pts = np.ascontiguousarray(al.warp.points, dtype=np.float32)
+        conf = np.ascontiguousarray(al.warp.confidence, dtype=np.float32)
+        keep += [luma, pts, conf]
+        v = views[i]
+        v.luminance = fptr(luma)
+        v.luma_width = inp.luminance.width
+        v.luma_height = inp.luminance.height
+        v.width = inp.width
+        v.height = inp.height
+        v.has_camera = 1 if inp.camera is not None else 0
+        v.accepted = 1 if al.report.accepted else 0
+        if inp.camera is not None:
+            v.camera = inp.camera.to_c()
+        v.warp.step = al.warp.step
+        v.warp.columns = al.warp.columns
+        v.warp.rows = al.warp.rows
+        v.warp.points = fptr(pts)
+        v.warp.confidence = fptr(conf)
+        v.warp.capacity = al.warp.columns * al.warp.rows
+    return views, keep
+
+
+def refine_multiview_depth(inputs: Sequence, reference_index: int, alignments: Sequence,
+                           options: DepthOptions, context=None, debug=None) -> Optional[DenseDepthMap]:
+    """depth.rs:312-580 on the GPU. See the module docstring for semantics.
+
+    ``debug`` may be a dict of numpy arrays named like the fields of
+    ``chiaro_depth_debug``; the library fills them with stage results.
+    """
+    from .runtime import default_context
+
+    if len(inputs) != len(alignments):
+        return None
+    if reference_index >= len(inputs) or inputs[reference_index].camera is None or not options.is_valid():
+        return None
+    ctx = context if context is not None else default_context()
+    ref = inputs[reference_index]
+    (columns, rows, step), _ = output_shape(ref.width, ref.height, options)
+    m = columns * rows
+    n = len(inputs)
+    views, keep = pack_views(inputs, alignments)
+    refined = (WarpC * n)()
+    out_points = [np.empty(2 * m, dtype=np.float32) for _ in range(n)]
+    out_conf = [np.empty(m, dtype=np.float32) for _ in range(n)]
+    for i in range(n):
+        refined[i].points = fptr(out_points[i])
+        refined[i].confidence = fptr(out_conf[i])
+        refined[i].capacity = m
+    reports = (DepthReportC * n)()
+    depth = np.empty(m, dtype=np.float64)
+    confidence = np.empty(m, dtype=np.float32)
+    provenance = np.empty(m, dtype=np.uint8)
+    dmap = DepthMapC()
+    dmap.capacity = m
+    dmap.depth = dptr(depth)
+    dmap.confidence = fptr(confidence)
+    dmap.provenance = u8ptr(provenance)
+    dbg = ctx.make_debug(debug) if debug else None
+    opt = options.to_c()
+    status = ctx.lib.chiaro_refine_multiview_depth(ctx.handle, views, n, reference_index, C.byref(opt), refined,
+                                                   reports, C.byref(dmap), C.byref(dbg) if dbg is not None else None)
+    if status == abi.INVALID:
+        return None
+    ctx.check(status)
+    for t in range(n):
+        if reports[t].present:
+            w = refined[t]
+            alignments[t].warp = type(alignments[t].warp)(int(w.step), int(w.columns), int(w.rows),
+                                                          out_points[t].reshape(m, 2), out_conf[t])
+            alignments[t].report.depth = DepthAlignmentReport.from_c(reports[t])
+    return DenseDepthMap(int(dmap.columns), int(dmap.rows), int(dmap.step), float(dmap.near_depth),
+                         float(dmap.far_depth), depth, confidence, provenance)

@@ -1,0 +1,165 @@
+"""Loading of the CUDA library and the per-thread device context.
+
+The library is ``chiaro_b200/_build/libchiaro_depth.so`` (built in-tree by
+``chiaro_b200.build``). Loading fails loudly when it is missing: the depth
+stage has no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .abi import (DepthDebugC, DepthMapC, DepthOptionsC, DepthReportC, ViewC, WarpC)
+from .build import HOSTCHECK, LIB
+
+P = C.POINTER
+
+# name -> (restype, argtypes); mirrors include/chiaro_depth.h
+SIGNATURES = {
+    "chiaro_depth_abi_version": (C.c_int, []),
+    "chiaro_depth_ctx_create": (C.c_int, [C.c_int, P(C.c_void_p)]),
+    "chiaro_depth_ctx_destroy": (None, [C.c_void_p]),
+    "chiaro_depth_last_error": (C.c_char_p, [C.c_void_p]),
+    "chiaro_depth_options_default": (None, [P(DepthOptionsC)]),
+    "chiaro_depth_options_valid": (C.c_int, [P(DepthOptionsC)]),
+    "chiaro_depth_output_shape": (C.c_int, [C.c_uint64, C.c_uint64, P(DepthOptionsC), P(C.c_uint64),
+                                            P(C.c_uint64), P(C.c_uint64), P(C.c_uint64), P(C.c_uint64),
+                                            P(C.c_uint64)]),
+    "chiaro_refine_multiview_depth": (C.c_int, [C.c_void_p, P(ViewC), C.c_size_t, C.c_size_t, P(DepthOptionsC),
+                                                P(WarpC), P(DepthReportC), P(DepthMapC), P(DepthDebugC)]),
+    "chiaro_refine_multiview_depth_device": (C.c_int, [C.c_void_p, P(ViewC), C.c_size_t, C.c_size_t,
+                                                       P(DepthOptionsC), P(WarpC), P(DepthReportC), P(DepthMapC)]),
+    "chiaro_depth_last_timings": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int]),
+    "chiaro_depth_last_launches": (C.c_int, [C.c_void_p]),
+    "chiaro_depth_ctx_stream": (C.c_void_p, [C.c_void_p]),
+    "chiaro_sgm_aggregate": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_uint64, C.c_uint64, C.c_uint64,
+                                       P(C.c_float)]),
+    "chiaro_sgm_aggregate_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
+                                              C.c_uint64, C.c_void_p]),
+    "chiaro_select_depths": (C.c_int, [C.c_void_p, P(C.c_double), C.c_uint64, P(C.c_float), P(C.c_float),
+                                       P(C.c_uint8), C.c_uint64, P(DepthOptionsC), P(C.c_uint8), P(C.c_double),
+                                       P(C.c_float), P(C.c_float), P(C.c_uint8), P(C.c_uint8)]),
+    "chiaro_reject_isolated": (C.c_int, [C.c_void_p, P(C.c_uint8), P(C.c_double), P(C.c_float), P(C.c_float),
+                                         C.c_uint64, C.c_uint64, C.c_double]),
+    "chiaro_reject_small_components": (C.c_int, [C.c_void_p, P(C.c_uint8), P(C.c_double), P(C.c_float),
+                                                 C.c_uint64, C.c_uint64, C.c_double, C.c_uint64]),
+    "chiaro_fit_local_planes": (C.c_int, [C.c_void_p, P(C.c_uint8), P(C.c_double), P(C.c_float), P(C.c_float),
+                                          C.c_uint64, C.c_uint64, C.c_double]),
+    "chiaro_warp_decisions_filter": (C.c_int, [C.c_void_p, P(C.c_uint8), P(C.c_float), P(C.c_float),
+                                               P(C.c_uint8), P(C.c_float), C.c_uint64, C.c_uint64, C.c_int,
+                                               C.c_int]),
+}
+
+HOSTCHECK_SIGNATURES = {
+    "chiaro_hc_exp_f32": (C.c_float, [C.c_float]),
+    "chiaro_hc_exp_f64": (C.c_double, [C.c_double]),
+    "chiaro_hc_expf_mismatches": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_int, P(C.c_uint32)]),
+    "chiaro_hc_exp_mismatches": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_double, P(C.c_uint32)]),
+    "chiaro_hc_plane_sample": (C.c_float, [P(C.c_float), C.c_int, C.c_int, C.c_float, C.c_float, P(C.c_int)]),
+    "chiaro_hc_warp_map": (C.c_int, [P(C.c_float), C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                     P(C.c_float)]),
+    "chiaro_hc_map_from": (C.c_int, [P(abi.CameraC), P(abi.CameraC), P(C.c_double), C.c_double, P(C.c_double)]),
+}
+
+_lib = None
+_hostcheck = None
+_lock = threading.Lock()
+_local = threading.local()
+
+
+def _bind(lib, table):
+    for name, (res, args) in table.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def library_path() -> Path:
+    return LIB
+
+
+def load_library():
+    """Load libchiaro_depth.so (raising if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB.exists():
+                raise RuntimeError(f"{LIB} is missing: build it with `python -m chiaro_b200.build` "
+                                   "(the depth stage has no CPU fallback)")
+            _lib = _bind(C.CDLL(str(LIB)), SIGNATURES)
+            if _lib.chiaro_depth_abi_version() != abi.ABI_VERSION:
+                raise RuntimeError("libchiaro_depth.so ABI version mismatch")
+    return _lib
+
+
+def load_hostcheck():
+    global _hostcheck
+    with _lock:
+        if _hostcheck is None:
+            if not HOSTCHECK.exists():
+                raise RuntimeError(f"{HOSTCHECK} is missing: run `python -m chiaro_b200.build`")
+            _hostcheck = _bind(C.CDLL(str(HOSTCHECK)), HOSTCHECK_SIGNATURES)
+    return _hostcheck
+
+
+class DepthContext:
+    """One CUDA device context of the library (own stream and buffers)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        status = self.lib.chiaro_depth_ctx_create(device, C.byref(h))
+        if status != abi.OK:
+            raise RuntimeError(f"chiaro_depth_ctx_create(device={device}) failed: {abi.STATUS_NAMES.get(status)}")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self.lib.chiaro_depth_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, status: int):
+        if status != abi.OK:
+            msg = self.lib.chiaro_depth_last_error(self.handle) or b""
+            raise RuntimeError(f"depth library error {status} ({abi.STATUS_NAMES.get(status, '?')}): "
+                               f"{msg.decode(errors='replace')}")
+
+    def timings(self) -> dict:
+        ms = (C.c_float * 7)()
+        n = self.lib.chiaro_depth_last_timings(self.handle, ms, 7)
+        names = ["cost_volume", "sgm", "select", "direct", "filters", "decisions", "total"]
+        return {names[i]: float(ms[i]) for i in range(n)}
+
+    def launches(self) -> int:
+        return int(self.lib.chiaro_depth_last_launches(self.handle))
+
+    def stream_handle(self) -> int:
+        return int(self.lib.chiaro_depth_ctx_stream(self.handle) or 0)
+
+    def make_debug(self, arrays: dict) -> DepthDebugC:
+        dbg = DepthDebugC()
+        for name, arr in arrays.items():
+            setattr(dbg, name, arr.ctypes.data_as(C.POINTER(abi.DEBUG_FIELD_TYPES[name])))
+        return dbg
+
+
+def default_context(device: Optional[int] = None) -> DepthContext:
+    """The calling thread's context (one per host thread, as the library requires)."""
+    ctx = getattr(_local, "ctx", None)
+    if ctx is None or (device is not None and ctx.device != device):
+        ctx = DepthContext(0 if device is None else device)
+        _local.ctx = ctx
+    return ctx

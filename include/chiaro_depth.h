@@ -1,0 +1,311 @@
+/*
+ * chiaro_depth.h — C ABI of the B200 multi-view depth stage.
+ *
+ * This library is a drop-in for chiaro-fusion's calibrated multi-view depth
+ * stage, `refine_multiview_depth` (crates/chiaro-fusion/src/depth.rs:312-580).
+ * Every entry point takes plain pointers and sizes; no C++ or torch types cross
+ * the boundary. A Rust `-sys` crate, a ctypes module or a C caller binds these
+ * declarations directly.
+ *
+ * Units and conventions (identical to the reference):
+ *   - depths are calibration distance units (millimetres on the L16);
+ *   - pixel coordinates are calibration-raster pixels, x right, y down;
+ *   - luminance planes are the half-resolution f32 log-luminance planes of
+ *     `Mosaic::luminance_half` (crates/chiaro-fusion/src/image.rs:401-428);
+ *     plane pixel (i, j) is centred at raster (2i + 0.5, 2j + 0.5);
+ *   - warps map reference-raster pixels to target-raster pixels on a regular
+ *     grid, NaN marking undefined nodes (crates/chiaro-fusion/src/align.rs:34-45).
+ *
+ * Status codes: every function returns one of CHIARO_OK .. CHIARO_ERR_*.
+ * CHIARO_INVALID is the C form of the reference's `None` return.
+ */
+#ifndef CHIARO_DEPTH_H
+#define CHIARO_DEPTH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHIARO_DEPTH_ABI_VERSION 1
+
+enum chiaro_status {
+    CHIARO_OK = 0,
+    CHIARO_INVALID = 1,       /* reference returns None (depth.rs:318-324)      */
+    CHIARO_ERR_CUDA = 2,      /* a CUDA runtime call failed                      */
+    CHIARO_ERR_TIMEOUT = 3,   /* a bounded device wait gave up                   */
+    CHIARO_ERR_CAPACITY = 4,  /* a caller buffer is smaller than the result     */
+    CHIARO_ERR_ARGUMENT = 5   /* NULL pointer or inconsistent sizes             */
+};
+
+/* DepthOptions (depth.rs:39-91). usize fields are 64-bit like Rust's usize. */
+typedef struct chiaro_depth_options {
+    int32_t enabled;
+    int32_t _pad0;
+    uint64_t grid_step;
+    double near_depth;
+    double far_depth;
+    uint64_t planes;
+    uint64_t patch_radius;
+    uint64_t minimum_support;
+    uint64_t best_view_count;
+    float minimum_score;
+    float minimum_margin;
+    float minimum_improvement;
+    int32_t _pad1;
+    uint64_t minimum_neighbour_support;
+    uint64_t completion_iterations;
+} chiaro_depth_options;
+
+/* Resolved camera (geometry.rs:31-62). Matrices are row-major m[row*3+col].
+ * flip: 0 = no mirror flip, 1 = flip_img_around_x == true, 2 == false
+ * (geometry.rs:129-136). pose_kind: 0 = Canonical, 1 = Mirror
+ * (geometry.rs:50-62). Missing distortion coefficients are zero
+ * (geometry.rs:310-312). */
+typedef struct chiaro_camera {
+    uint64_t width;
+    uint64_t height;
+    double k[9];
+    double k_inverse[9];
+    int32_t has_distortion;
+    int32_t flip;
+    double distortion_center[2];
+    double distortion_normalization[2];
+    double distortion_coeffs[5];
+    int32_t pose_kind;
+    int32_t _pad0;
+    double rotation_wc[9];
+    double rotation_cw[9];
+    double translation_wc[3];
+    double center[3];
+    double real_cw[9];
+    double reflect[9];
+    double virtual_center[3];
+    double orientation_correction[9];
+} chiaro_camera;
+
+/* One module's input (AlignInput, align.rs:246-257) plus its global alignment
+ * (ModuleAlignment.warp / report.accepted, align.rs:148-157). */
+typedef struct chiaro_warp {
+    uint64_t step;
+    uint64_t columns;
+    uint64_t rows;
+    float *points;       /* 2 * columns * rows, (x, y) interleaved; NaN = undefined */
+    float *confidence;   /* columns * rows (may be NULL on input)                    */
+    uint64_t capacity;   /* node capacity of points/confidence when used as output  */
+} chiaro_warp;
+
+typedef struct chiaro_view {
+    const float *luminance;   /* luma_width * luma_height, row-major */
+    uint64_t luma_width;
+    uint64_t luma_height;
+    uint64_t width;           /* raster width  (AlignInput.width)  */
+    uint64_t height;          /* raster height (AlignInput.height) */
+    int32_t has_camera;       /* AlignInput.camera.is_some()        */
+    int32_t accepted;         /* ModuleAlignment.report.accepted    */
+    chiaro_camera camera;
+    chiaro_warp warp;         /* ModuleAlignment.warp (input)       */
+} chiaro_view;
+
+/* DepthProvenance (depth.rs:115-121). */
+enum chiaro_provenance {
+    CHIARO_UNSUPPORTED = 0,
+    CHIARO_GLOBAL = 1,
+    CHIARO_MEASURED = 2,
+    CHIARO_REGULARIZED = 3
+};
+
+/* DenseDepthMap (depth.rs:133-141); caller-owned arrays of `capacity` nodes.
+ * depth is NaN where the reference holds None. */
+typedef struct chiaro_depth_map {
+    uint64_t columns;
+    uint64_t rows;
+    uint64_t step;
+    double near_depth;
+    double far_depth;
+    uint64_t capacity;
+    double *depth;
+    float *confidence;
+    uint8_t *provenance;
+} chiaro_depth_map;
+
+/* DepthAlignmentReport (depth.rs:93-113); `present` mirrors report.depth.is_some(). */
+typedef struct chiaro_depth_report {
+    int32_t present;
+    int32_t has_median_depth;
+    uint64_t tested_nodes;
+    uint64_t measured_nodes;
+    uint64_t regularized_nodes;
+    uint64_t fallback_nodes;
+    uint64_t refined_nodes;
+    uint64_t occluded_nodes;
+    uint64_t boundary_nodes;
+    float reconstructed_fraction;
+    float refined_fraction;
+    float occluded_fraction;
+    int32_t has_median_score_improvement;
+    double median_depth;
+    float median_score_improvement;
+    int32_t _pad0;
+} chiaro_depth_report;
+
+/* Optional host buffers receiving intermediate stage results (any may be NULL).
+ * Sizes: coarse N = coarse_columns*coarse_rows, D = planes + 1, fine M =
+ * columns*rows of the output grid. Per-target arrays are [n_views][M]. */
+typedef struct chiaro_depth_debug {
+    float *coarse_scores;          /* N*D  CostVolume.scores     (depth.rs:1233) */
+    float *coarse_costs;           /* N*D  CostVolume.costs      (depth.rs:1236) */
+    float *coarse_guidance;        /* N                                         */
+    uint8_t *coarse_tested;        /* N                                         */
+    float *regularised;            /* N*D  semi_global_costs     (depth.rs:1279) */
+    uint8_t *coarse_has;           /* N    select_depths field   (depth.rs:1385) */
+    double *coarse_depth;          /* N                                         */
+    float *coarse_confidence;      /* N                                         */
+    float *coarse_improvement;     /* N                                         */
+    uint8_t *coarse_regularized;   /* N                                         */
+    uint8_t *coarse_fillable;      /* N                                         */
+    uint8_t *direct_has;           /* M    measure_direct_depths (depth.rs:715)  */
+    double *direct_depth;          /* M                                         */
+    float *direct_confidence;      /* M                                         */
+    float *direct_improvement;     /* M                                         */
+    uint8_t *direct_regularized;   /* M                                         */
+    float *direct_guidance;        /* M                                         */
+    uint8_t *direct_tested;        /* M                                         */
+    uint8_t *isolated_has;         /* M    after reject_isolated (depth.rs:881)  */
+    uint8_t *component_has;        /* M    after components      (depth.rs:933)  */
+    double *fitted_depth;          /* M    after plane fit       (depth.rs:995)  */
+    uint8_t *decision_kind;        /* n_views*M NodeWarp kind after boundaries   */
+} chiaro_depth_debug;
+
+/* NodeWarp kinds (depth.rs:256-271). */
+enum chiaro_node_warp {
+    CHIARO_NW_UNDEFINED = 0,
+    CHIARO_NW_GLOBAL = 1,
+    CHIARO_NW_REFINED = 2,
+    CHIARO_NW_OCCLUDED = 3,
+    CHIARO_NW_BOUNDARY = 4
+};
+
+typedef struct chiaro_depth_ctx chiaro_depth_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Create a context bound to CUDA device `device` with its own stream. One
+ * context per host thread; calls on one context are synchronous. */
+int chiaro_depth_ctx_create(int device, chiaro_depth_ctx **out);
+void chiaro_depth_ctx_destroy(chiaro_depth_ctx *ctx);
+const char *chiaro_depth_last_error(const chiaro_depth_ctx *ctx);
+int chiaro_depth_abi_version(void);
+
+/* DepthOptions::default() (depth.rs:69-91). */
+void chiaro_depth_options_default(chiaro_depth_options *out);
+/* valid_options (depth.rs:1879-1891): 1 when valid. */
+int chiaro_depth_options_valid(const chiaro_depth_options *options);
+
+/* Output grid of the stage for a reference raster: the direct-pass grid
+ * (depth.rs:326-328, depth.rs:726-728). Also reports the coarse grid. */
+int chiaro_depth_output_shape(uint64_t width, uint64_t height,
+                              const chiaro_depth_options *options,
+                              uint64_t *columns, uint64_t *rows, uint64_t *step,
+                              uint64_t *coarse_columns, uint64_t *coarse_rows,
+                              uint64_t *coarse_step);
+
+/* ---- the stage ---------------------------------------------------------- */
+
+/* refine_multiview_depth (depth.rs:312-580).
+ * views[n_views]: every module's input and global warp (host memory).
+ * refined[n_views]: caller-owned output warps. For every target that the
+ * reference would rewrite (accepted, has a camera, not the reference;
+ * depth.rs:420-426) the library writes step/columns/rows, points and
+ * confidence, and sets reports[t].present = 1; other entries are untouched
+ * except reports[t].present = 0.
+ * out_map: the DenseDepthMap. debug may be NULL.
+ * Returns CHIARO_INVALID where the reference returns None. */
+int chiaro_refine_multiview_depth(chiaro_depth_ctx *ctx,
+                                  const chiaro_view *views, size_t n_views,
+                                  size_t reference_index,
+                                  const chiaro_depth_options *options,
+                                  chiaro_warp *refined,
+                                  chiaro_depth_report *reports,
+                                  chiaro_depth_map *out_map,
+                                  const chiaro_depth_debug *debug);
+
+/* Same stage with every array pointer in `views` (luminance, warp points and
+ * confidence), in `refined` and in `out_map` referring to device memory of the
+ * context's device; nothing is copied across PCIe. Used when inputs are
+ * already resident in HBM. Reports are host structs. */
+int chiaro_refine_multiview_depth_device(chiaro_depth_ctx *ctx,
+                                         const chiaro_view *views, size_t n_views,
+                                         size_t reference_index,
+                                         const chiaro_depth_options *options,
+                                         chiaro_warp *refined,
+                                         chiaro_depth_report *reports,
+                                         chiaro_depth_map *out_map);
+
+/* Device time in milliseconds of each stage of the last call on this context:
+ * [0] cost volume, [1] SGM, [2] select, [3] direct pass, [4] filters,
+ * [5] per-target decisions, [6] whole stage. Returns the count written. */
+int chiaro_depth_last_timings(const chiaro_depth_ctx *ctx, float *ms, int capacity);
+
+/* Number of this library's kernel launches in the last stage call. */
+int chiaro_depth_last_launches(const chiaro_depth_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events with the library's. */
+void *chiaro_depth_ctx_stream(const chiaro_depth_ctx *ctx);
+
+/* ---- individual operators (host buffers) -------------------------------- */
+
+/* semi_global_costs (depth.rs:1279-1311): eight-path SGM over a label-minor
+ * [columns*rows][labels] f32 cost volume with per-node guidance. Output order
+ * of summation is the reference's, so results are bit-identical. */
+int chiaro_sgm_aggregate(chiaro_depth_ctx *ctx, const float *costs,
+                         const float *guidance, uint64_t columns, uint64_t rows,
+                         uint64_t labels, float *out);
+
+/* Same operator on device pointers (stream of the context). */
+int chiaro_sgm_aggregate_device(chiaro_depth_ctx *ctx, const float *costs,
+                                const float *guidance, uint64_t columns,
+                                uint64_t rows, uint64_t labels, float *out);
+
+/* select_depths (depth.rs:1385-1467) with sublabel_depth (depth.rs:1469-1488).
+ * labels[n_labels]: label depths, NaN for label 0 (the global warp). */
+int chiaro_select_depths(chiaro_depth_ctx *ctx, const double *labels,
+                         uint64_t n_labels, const float *scores,
+                         const float *regularised, const uint8_t *tested,
+                         uint64_t n_nodes, const chiaro_depth_options *options,
+                         uint8_t *has, double *depth, float *confidence,
+                         float *improvement, uint8_t *regularized,
+                         uint8_t *fillable);
+
+/* reject_isolated_direct_depths (depth.rs:881-924), in place on has[]. */
+int chiaro_reject_isolated(chiaro_depth_ctx *ctx, uint8_t *has, const double *depth,
+                           const float *confidence, const float *guidance,
+                           uint64_t columns, uint64_t rows, double inverse_tolerance);
+
+/* reject_small_direct_components (depth.rs:933-989), in place on has[]. */
+int chiaro_reject_small_components(chiaro_depth_ctx *ctx, uint8_t *has,
+                                   const double *depth, const float *guidance,
+                                   uint64_t columns, uint64_t rows,
+                                   double inverse_tolerance, uint64_t minimum_nodes);
+
+/* fit_local_depth_planes (depth.rs:995-1060), in place on depth[]. */
+int chiaro_fit_local_planes(chiaro_depth_ctx *ctx, const uint8_t *has, double *depth,
+                            const float *confidence, const float *guidance,
+                            uint64_t columns, uint64_t rows, double inverse_tolerance);
+
+/* enforce_warp_consensus (depth.rs:582-618) then, when `boundaries` is set,
+ * suppress_warp_boundaries (depth.rs:620-672), in place. kind[] uses
+ * chiaro_node_warp; global/point are 2 floats per node. */
+int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *global,
+                                 float *point, const uint8_t *measured,
+                                 const float *guidance, uint64_t columns,
+                                 uint64_t rows, int consensus, int boundaries);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHIARO_DEPTH_H */

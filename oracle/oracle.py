@@ -1,0 +1,185 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Loads ``oracle/_build/libchiaro_oracle.so`` (built by ``make -C oracle``) and
+exposes the restated reference functions to the tests, the smoke check and the
+benchmark's CPU-baseline leg. Nothing in the ``chiaro_b200`` package imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from chiaro_b200 import abi
+from chiaro_b200.abi import (CameraC, DepthDebugC, DepthMapC, DepthOptionsC, DepthReportC, ViewC, WarpC,
+                             dptr, fptr, sizeptr, u8ptr, u16ptr)
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libchiaro_oracle.so"
+
+
+def build(force: bool = False) -> Path:
+    src = [HERE / "chiaro_oracle.cpp", HERE.parent / "include" / "chiaro_depth.h"]
+    if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in src):
+        subprocess.run(["make", "-C", str(HERE), "-s"], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        P = C.POINTER
+        sig = {
+            "oracle_options_default": (None, [P(DepthOptionsC)]),
+            "oracle_options_valid": (C.c_int, [P(DepthOptionsC)]),
+            "oracle_refine_multiview_depth": (C.c_int, [P(ViewC), C.c_size_t, C.c_size_t, P(DepthOptionsC),
+                                                        P(WarpC), P(DepthReportC), P(DepthMapC), P(DepthDebugC),
+                                                        C.c_int]),
+            "oracle_inverse_depth_samples": (None, [C.c_double, C.c_double, C.c_size_t, P(C.c_double)]),
+            "oracle_sublabel_depth": (C.c_double, [P(C.c_double), C.c_size_t, P(C.c_float), C.c_size_t]),
+            "oracle_aggregate": (C.c_int, [P(C.c_float), C.c_size_t, P(DepthOptionsC), P(C.c_float)]),
+            "oracle_semi_global_costs": (None, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, C.c_size_t,
+                                                P(C.c_float)]),
+            "oracle_diagonal_paths": (C.c_size_t, [C.c_size_t, C.c_size_t, C.c_int, P(C.c_size_t),
+                                                   P(C.c_size_t)]),
+            "oracle_select_depths": (None, [P(C.c_double), C.c_size_t, P(C.c_float), P(C.c_float), P(C.c_uint8),
+                                            C.c_size_t, P(DepthOptionsC), P(C.c_uint8), P(C.c_double),
+                                            P(C.c_float), P(C.c_float), P(C.c_uint8), P(C.c_uint8)]),
+            "oracle_complete_depth_field": (None, [P(C.c_uint8), P(C.c_double), P(C.c_float), P(C.c_float),
+                                                   P(C.c_uint8), P(C.c_float), P(C.c_uint8), C.c_size_t,
+                                                   C.c_size_t, P(DepthOptionsC)]),
+            "oracle_reject_isolated": (None, [P(C.c_uint8), P(C.c_double), P(C.c_float), P(C.c_float),
+                                              C.c_size_t, C.c_size_t, C.c_double]),
+            "oracle_reject_small_components": (None, [P(C.c_uint8), P(C.c_double), P(C.c_float), C.c_size_t,
+                                                      C.c_size_t, C.c_double, C.c_size_t]),
+            "oracle_fit_local_planes": (None, [P(C.c_uint8), P(C.c_double), P(C.c_float), P(C.c_float),
+                                               C.c_size_t, C.c_size_t, C.c_double]),
+            "oracle_select_direct_depth": (C.c_int, [P(C.c_double), P(C.c_float), C.c_size_t, C.c_int, C.c_float,
+                                                     C.c_int, P(DepthOptionsC), P(C.c_double), P(C.c_float),
+                                                     P(C.c_float)]),
+            "oracle_best_depth_candidate": (C.c_long, [P(C.c_double), P(C.c_float), C.c_size_t,
+                                                       P(DepthOptionsC)]),
+            "oracle_warp_decisions_agree": (C.c_int, [C.c_int, C.c_int, P(C.c_float), P(C.c_float), C.c_int,
+                                                      P(C.c_float), P(C.c_float)]),
+            "oracle_warp_decisions_filter": (None, [P(C.c_uint8), P(C.c_float), P(C.c_float), P(C.c_uint8),
+                                                    P(C.c_float), C.c_size_t, C.c_size_t, C.c_int, C.c_int]),
+            "oracle_diagnostic_samples": (None, [P(DepthMapC), P(C.c_uint16), P(C.c_uint16)]),
+            "oracle_visualization_samples": (None, [P(DepthMapC), P(C.c_uint16)]),
+            "oracle_distort": (None, [P(CameraC), P(C.c_double), P(C.c_double)]),
+            "oracle_undistort": (None, [P(CameraC), P(C.c_double), P(C.c_double)]),
+            "oracle_pixel_to_ray": (None, [P(CameraC), P(C.c_double), P(C.c_double), P(C.c_double)]),
+            "oracle_project": (C.c_int, [P(CameraC), P(C.c_double), P(C.c_double)]),
+            "oracle_map_from": (C.c_int, [P(CameraC), P(CameraC), P(C.c_double), C.c_double, P(C.c_double)]),
+            "oracle_warp_map": (C.c_int, [P(WarpC), C.c_float, C.c_float, P(C.c_float)]),
+            "oracle_warp_magnification": (C.c_int, [P(WarpC), C.c_float, C.c_float, P(C.c_float)]),
+            "oracle_plane_sample": (C.c_float, [P(C.c_float), C.c_size_t, C.c_size_t, C.c_float, C.c_float,
+                                                P(C.c_int)]),
+            "oracle_score_one_view": (C.c_int, [P(ViewC), C.c_size_t, C.c_size_t, C.c_size_t, C.c_double,
+                                                C.c_double, C.c_double, C.c_size_t, P(C.c_float)]),
+            "oracle_build_cost_volume": (C.c_int, [P(ViewC), C.c_size_t, C.c_size_t, P(DepthOptionsC), C.c_size_t,
+                                                   C.c_size_t, P(C.c_float), P(C.c_float), P(C.c_float),
+                                                   P(C.c_uint8), C.c_int]),
+            "oracle_measure_direct_depths": (C.c_int, [P(ViewC), C.c_size_t, C.c_size_t, P(DepthOptionsC),
+                                                       P(C.c_uint8), P(C.c_double), P(C.c_float), P(C.c_float),
+                                                       P(C.c_uint8), C.c_size_t, C.c_size_t, P(C.c_uint8),
+                                                       P(C.c_double), P(C.c_float), P(C.c_float), P(C.c_float),
+                                                       P(C.c_uint8), C.c_int]),
+            "oracle_target_decisions": (C.c_int, [P(ViewC), C.c_size_t, C.c_size_t, C.c_size_t, P(DepthOptionsC),
+                                                  P(C.c_uint8), P(C.c_double), P(C.c_float), P(C.c_uint8),
+                                                  P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_uint8)]),
+            "oracle_luminance_half": (None, [P(C.c_uint16), C.c_size_t, C.c_size_t, C.c_float, C.c_float,
+                                             P(C.c_float)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def default_options() -> DepthOptionsC:
+    o = DepthOptionsC()
+    lib().oracle_options_default(C.byref(o))
+    return o
+
+
+def refine_multiview_depth(inputs, reference_index, alignments, options, threads: int = 0, debug=None):
+    """Run the oracle's whole stage; returns a dict of numpy outputs or None."""
+    from chiaro_b200.depth import output_shape, pack_views
+
+    n = len(inputs)
+    ref = inputs[reference_index]
+    (columns, rows, step), (cc, cr, cs) = output_shape(ref.width, ref.height, options)
+    m = columns * rows
+    views, keep = pack_views(inputs, alignments)
+    refined = (WarpC * n)()
+    pts = [np.full(2 * m, np.nan, dtype=np.float32) for _ in range(n)]
+    conf = [np.full(m, np.nan, dtype=np.float32) for _ in range(n)]
+    for i in range(n):
+        refined[i].points = fptr(pts[i])
+        refined[i].confidence = fptr(conf[i])
+        refined[i].capacity = m
+    reports = (DepthReportC * n)()
+    depth = np.empty(m, dtype=np.float64)
+    confidence = np.empty(m, dtype=np.float32)
+    provenance = np.empty(m, dtype=np.uint8)
+    dmap = DepthMapC()
+    dmap.capacity = m
+    dmap.depth = dptr(depth)
+    dmap.confidence = fptr(confidence)
+    dmap.provenance = u8ptr(provenance)
+    dbg = None
+    if debug is not None:
+        dbg = make_debug(debug)
+    opt = options.to_c()
+    status = lib().oracle_refine_multiview_depth(views, n, reference_index, C.byref(opt), refined, reports,
+                                                 C.byref(dmap), C.byref(dbg) if dbg is not None else None, threads)
+    if status == abi.INVALID:
+        return None
+    assert status == abi.OK, status
+    return dict(columns=int(dmap.columns), rows=int(dmap.rows), step=int(dmap.step), depth=depth,
+                confidence=confidence, provenance=provenance, points=pts, warp_confidence=conf,
+                reports=[reports[i] for i in range(n)], refined=[refined[i] for i in range(n)])
+
+
+def make_debug(arrays: dict) -> DepthDebugC:
+    dbg = DepthDebugC()
+    for name, arr in arrays.items():
+        ctype = abi.DEBUG_FIELD_TYPES[name]
+        setattr(dbg, name, arr.ctypes.data_as(C.POINTER(ctype)))
+    return dbg
+
+
+def debug_buffers(n_views: int, coarse_nodes: int, labels: int, fine_nodes: int) -> dict:
+    """Allocate every debug field with its documented size."""
+    N, D, M = coarse_nodes, labels, fine_nodes
+    f32, f64, u8 = np.float32, np.float64, np.uint8
+    spec = dict(coarse_scores=(N * D, f32), coarse_costs=(N * D, f32), coarse_guidance=(N, f32),
+                coarse_tested=(N, u8), regularised=(N * D, f32), coarse_has=(N, u8), coarse_depth=(N, f64),
+                coarse_confidence=(N, f32), coarse_improvement=(N, f32), coarse_regularized=(N, u8),
+                coarse_fillable=(N, u8), direct_has=(M, u8), direct_depth=(M, f64), direct_confidence=(M, f32),
+                direct_improvement=(M, f32), direct_regularized=(M, u8), direct_guidance=(M, f32),
+                direct_tested=(M, u8), isolated_has=(M, u8), component_has=(M, u8), fitted_depth=(M, f64),
+                decision_kind=(n_views * M, u8))
+    return {k: np.zeros(n, dtype=t) for k, (n, t) in spec.items()}
+
+
+def semi_global_costs(costs: np.ndarray, guidance: np.ndarray, columns: int, rows: int, labels: int) -> np.ndarray:
+    out = np.empty(columns * rows * labels, dtype=np.float32)
+    costs = np.ascontiguousarray(costs, dtype=np.float32)
+    guidance = np.ascontiguousarray(guidance, dtype=np.float32)
+    lib().oracle_semi_global_costs(fptr(costs), fptr(guidance), columns, rows, labels, fptr(out))
+    return out
+
+
+def threads_default() -> int:
+    return os.cpu_count() or 1
