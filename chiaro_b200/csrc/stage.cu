@@ -988,3 +988,4 @@ int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *gl
 }
 
 }  // extern "C"
+
