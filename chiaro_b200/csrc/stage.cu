@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -989,3 +990,74 @@ int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *gl
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------------
+// Allocation-free form of the connected-components filter.
+//
+// Some callers cannot allocate device memory: a host that hands this library a
+// fixed memory budget (an embedded or real-time pipeline), a plugin running
+// inside a framework that owns the allocator, or code building a CUDA graph
+// around its own buffers. This entry point takes the caller's device buffers
+// for inputs and output and keeps the union-find scratch (parent and component
+// size per node) in a file-scope device array, so it calls no cudaMalloc,
+// cudaFree or allocating library routine.
+//
+// The array holds NOALLOC_MAX_NODES nodes (2 x 4 MiB); every GPU that loads
+// the library keeps it until the process exits. All calls share it, so calls
+// that overlap on the GPU (different streams, or host threads) race; the
+// scratch keeps the previous call's contents and is reinitialised on every call.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t NOALLOC_MAX_NODES = 1u << 20;
+
+static __device__ __align__(256) int g_component_scratch[2 * NOALLOC_MAX_NODES];  // [parent | size]
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_scratch_mutex;
+int *g_scratch_address[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_component_scratch on the current device, looked up once
+// per device with that device current (the host-side symbol is only a stand-in).
+cudaError_t component_scratch(int **out) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_address[device]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_component_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_address[device] = static_cast<int *>(p);
+    }
+    *out = g_scratch_address[device];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int chiaro_reject_small_components_noalloc(void *stream, const uint8_t *has, const double *depth,
+                                                      const float *guidance, uint64_t columns, uint64_t rows,
+                                                      double inverse_tolerance, uint64_t minimum_nodes,
+                                                      uint8_t *has_out) {
+    if (!has || !depth || !guidance || !has_out || columns < 1 || rows < 1) return CHIARO_ERR_ARGUMENT;
+    const uint64_t n = columns * rows;
+    if (n > NOALLOC_MAX_NODES) return CHIARO_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (minimum_nodes <= 1) {  // depth.rs:941-943: nothing is removed
+        return cudaMemcpyAsync(has_out, has, n, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? CHIARO_OK
+                                                                                              : CHIARO_ERR_CUDA;
+    }
+    int *scratch = nullptr;
+    if (component_scratch(&scratch) != cudaSuccess) return CHIARO_ERR_CUDA;
+    int *parent = scratch, *size = scratch + NOALLOC_MAX_NODES;
+    const unsigned blocks = blocks_for(n, 256);
+    components_init_kernel<<<blocks, 256, 0, s>>>(parent, (int)n);
+    if (cudaMemsetAsync(size, 0, n * sizeof(int), s) != cudaSuccess) return CHIARO_ERR_CUDA;
+    components_union_kernel<<<blocks, 256, 0, s>>>(has, depth, guidance, parent, (int)columns, (int)rows,
+                                                   inverse_tolerance);
+    components_size_kernel<<<blocks, 256, 0, s>>>(has, parent, size, (int)n);
+    components_mark_kernel<<<blocks, 256, 0, s>>>(has, parent, size, has_out, (int)n,
+                                                  (int)std::min<uint64_t>(minimum_nodes, INT32_MAX));
+    return cudaGetLastError() == cudaSuccess ? CHIARO_OK : CHIARO_ERR_CUDA;
+}

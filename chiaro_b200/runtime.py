@@ -53,6 +53,9 @@ SIGNATURES = {
     "chiaro_warp_decisions_filter": (C.c_int, [C.c_void_p, P(C.c_uint8), P(C.c_float), P(C.c_float),
                                                P(C.c_uint8), P(C.c_float), C.c_uint64, C.c_uint64, C.c_int,
                                                C.c_int]),
+    "chiaro_reject_small_components_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                         C.c_uint64, C.c_uint64, C.c_double, C.c_uint64,
+                                                         C.c_void_p]),
 }
 
 HOSTCHECK_SIGNATURES = {

@@ -304,6 +304,24 @@ int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *gl
                                  const float *guidance, uint64_t columns,
                                  uint64_t rows, int consensus, int boundaries);
 
+/* ---- allocation-free operator --------------------------------------------- */
+
+/* No counterpart in the reference: an allocation-free form of
+ * chiaro_reject_small_components for callers that cannot allocate device
+ * memory (a host with a fixed memory budget, a plugin whose framework owns the
+ * allocator, code that wraps its own buffers in a CUDA graph). All pointers are
+ * device memory of the current device; has_out may not alias has. The work is
+ * queued on `stream` (a cudaStream_t, NULL for the default stream) and the
+ * call returns without synchronising. Its union-find scratch lives in a static
+ * device array of 2^20 nodes (8 MiB per GPU, held until exit): grids with more
+ * nodes return CHIARO_ERR_CAPACITY. The first call on a device looks up that
+ * array's address; make it before any stream capture. Calls share the array,
+ * so calls that overlap on the GPU race. Nothing here calls cudaMalloc. */
+int chiaro_reject_small_components_noalloc(void *stream, const uint8_t *has, const double *depth,
+                                           const float *guidance, uint64_t columns, uint64_t rows,
+                                           double inverse_tolerance, uint64_t minimum_nodes,
+                                           uint8_t *has_out);
+
 #ifdef __cplusplus
 }
 #endif
