@@ -20,6 +20,7 @@ struct CostParams {
     int labels;                 // D = planes + 1
     const double *label_depth;  // [D], label 0 unused (the global warp)
     const float *spatial;       // [(2r+1)^2] spatial weights
+    const GeomRec *geometry;    // [node][target]
     int radius;
     int minimum_support, best_view_count;
     float *scores, *costs, *guidance;
@@ -67,28 +68,21 @@ __device__ inline void load_cameras(DevCamera *cams, const DevView *views, int r
     }
 }
 
-// Stage reference patch, tap positions and view geometry for the node at
-// (cx, cy) at the given radius. Ends with __syncthreads().
+// Stage reference patch, tap positions and (from the precomputed records
+// `recs[0..V)`, when given) the view geometry for the node at (cx, cy) at the
+// given radius. Without records the geometry already in s.geom is kept and
+// only taps_ok is recomputed. Ends with __syncthreads().
 __device__ inline void stage_node(const NodeSmem &s, RefPatch &patch, const DevView *views, int reference,
                                   const int *targets, int V, double cx, double cy, int radius, const float *spatial,
-                                  bool geometry) {
+                                  const GeomRec *recs) {
     const int taps = (2 * radius + 1) * (2 * radius + 1);
-    if (geometry) {
-        for (int v = threadIdx.x; v < V; v += blockDim.x) s.geom[v].taps_ok = 1;
-    } else {
-        for (int v = threadIdx.x; v < V; v += blockDim.x) s.geom[v].taps_ok = 1;
+    for (int v = threadIdx.x; v < V; v += blockDim.x) {
+        if (recs) geom_from_rec(recs[v], camera_origin(s.cams[0]), s.geom[v]);
+        s.geom[v].taps_ok = 1;
     }
     ref_patch_setup(views[reference].luma, cx, cy, radius, spatial, s.r, s.w, s.wr, patch);
     for (int v = 0; v < V; ++v) tap_positions(views[targets[v]].warp, cx, cy, radius, s.gq + v * taps, s.geom[v]);
     __syncthreads();
-    if (geometry) {
-        for (int v = threadIdx.x; v < V; v += blockDim.x) {
-            int taps_ok = s.geom[v].taps_ok;
-            view_geometry(s.cams[0], s.cams[1 + v], views[targets[v]].warp, cx, cy, s.geom[v]);
-            s.geom[v].taps_ok = taps_ok;
-        }
-        __syncthreads();
-    }
 }
 
 __global__ void __launch_bounds__(256) cost_volume_kernel(CostParams p) {
@@ -103,7 +97,8 @@ __global__ void __launch_bounds__(256) cost_volume_kernel(CostParams p) {
 
     load_cameras(s.cams, p.views, p.reference, p.targets, V);
     __syncthreads();
-    stage_node(s, patch, p.views, p.reference, p.targets, V, cx, cy, p.radius, p.spatial, true);
+    stage_node(s, patch, p.views, p.reference, p.targets, V, cx, cy, p.radius, p.spatial,
+               p.geometry + (size_t)node * V);
 
     int any_finite = 0;
     for (int label = threadIdx.x; label < p.labels; label += blockDim.x) {

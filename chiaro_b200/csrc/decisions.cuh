@@ -4,9 +4,7 @@
 // classification (458-485), enforce_warp_consensus (582-618),
 // suppress_warp_boundaries (620-672) and the output warp (490-532).
 //
-// One CTA (one warp) per fine node and target. Lanes 0-4 score the five
-// inverse-depth offsets and lane 5 the global baseline; after the first
-// lane picks the best offset, lanes 0-7 score the eight residual shifts.
+// Decisions for every target run in one launch: eight lanes per (node, target).
 #pragma once
 
 #include "cost.cuh"
@@ -24,151 +22,200 @@ struct Decisions {  // NodeWarp (depth.rs:256-271) as arrays
 
 struct DecisionParams {
     const DevView *views;
-    int reference;
-    int target;  // module index of the target
+    int reference, n_targets;
+    int targets[MAX_VIEWS];
     int columns, rows, step;
     Field field;
+    const GeomRec *geometry;  // [node][target] of the fine grid
     double inverse_step, near_depth, far_depth;
     int radius;
     const float *spatial;
     float minimum_score;
-    Decisions out;
+    Decisions out[MAX_VIEWS];  // per target (index into targets)
 };
 
-__global__ void __launch_bounds__(32) target_decision_kernel(DecisionParams p) {
+constexpr int DECISION_LANES = 8;     // lanes per (node, target)
+constexpr int DECISION_NODES = 32;    // nodes per CTA (256 threads)
+
+__host__ __device__ inline size_t decision_smem_bytes(int taps) {
+    // per node slot: r, w, wr, and tap positions of the target
+    return (size_t)DECISION_NODES * (3 * taps * sizeof(float) + taps * sizeof(float2));
+}
+
+// One CTA handles 32 nodes of one target (blockIdx.y); each node belongs to an
+// aligned group of 8 lanes inside one warp. Lanes 0-4 score the five
+// inverse-depth offsets and lane 5 the baseline; after lane 0 picks the best
+// offset, lanes 0-7 score the eight residual shifts; lane 0 classifies.
+__global__ void __launch_bounds__(256) target_decision_kernel(DecisionParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ RefPatch patch;
-    __shared__ float sc[16];
-    __shared__ float2 pts[16];
-    __shared__ int fail;
-    const int node = blockIdx.x;
-    const int column = node % p.columns, row = node / p.columns;
+    __shared__ RefPatch patch[DECISION_NODES];
+    __shared__ float sc[DECISION_NODES][16];
+    __shared__ float2 pts[DECISION_NODES][16];
+    __shared__ int fail[DECISION_NODES], taps_ok[DECISION_NODES];
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
-    const double cx = (double)(column * p.step), cy = (double)(row * p.step);
-    const DevView &tv = p.views[p.target];
-    Decisions o = p.out;
+    const int slot = threadIdx.x / DECISION_LANES, lane = threadIdx.x % DECISION_LANES;
+    const int node = blockIdx.x * DECISION_NODES + slot;
+    const int vi = blockIdx.y;
+    const int target = p.targets[vi];
+    const DevView &tv = p.views[target];
+    const DevView &rv = p.views[p.reference];
+    Decisions o = p.out[vi];
+    float *r = reinterpret_cast<float *>(smem_raw) + (size_t)slot * 3 * taps;
+    float *w = r + taps, *wr = w + taps;
+    float2 *gq = reinterpret_cast<float2 *>(smem_raw + (size_t)DECISION_NODES * 3 * taps * sizeof(float)) +
+                 (size_t)slot * taps;
 
-    float gqx, gqy;
-    if (!warp_map(tv.warp, (float)cx, (float)cy, gqx, gqy)) {
-        if (threadIdx.x == 0) {
-            o.kind[node] = CHIARO_NW_UNDEFINED;
-            o.global[node] = make_float2(0.0f, 0.0f);
-            o.point[node] = make_float2(0.0f, 0.0f);
-            o.confidence[node] = 0.0f;
-            o.measured[node] = 0;
+    bool active = node < p.columns * p.rows;
+    const double cx = active ? (double)((node % p.columns) * p.step) : 0.0;
+    const double cy = active ? (double)((node / p.columns) * p.step) : 0.0;
+    float gqx = 0.0f, gqy = 0.0f;
+    if (active) {
+        bool defined = warp_map(tv.warp, (float)cx, (float)cy, gqx, gqy);
+        if (!defined || !p.field.has[node]) {
+            if (lane == 0) {
+                o.kind[node] = defined ? CHIARO_NW_GLOBAL : CHIARO_NW_UNDEFINED;
+                o.global[node] = make_float2(gqx, gqy);
+                o.point[node] = make_float2(gqx, gqy);
+                o.confidence[node] = 0.0f;
+                o.measured[node] = 0;
+            }
+            active = false;
         }
-        return;
     }
-    const float2 gq = make_float2(gqx, gqy);
-    if (!p.field.has[node]) {
-        if (threadIdx.x == 0) {
-            o.kind[node] = CHIARO_NW_GLOBAL;
-            o.global[node] = gq;
-            o.point[node] = gq;
-            o.confidence[node] = 0.0f;
-            o.measured[node] = 0;
+    const float2 gq_c = make_float2(gqx, gqy);
+    // reference patch and tap positions of this node (8 lanes)
+    float centre = 0.0f;
+    bool centre_ok = false;
+    if (active) {
+        centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+        if (lane == 0) {
+            patch[slot].ok = centre_ok;
+            patch[slot].centre = centre;
+            taps_ok[slot] = 1;
+            fail[slot] = 0;
         }
-        return;
     }
-    const int targets[1] = {p.target};
-    NodeSmem s = carve_node_smem(smem_raw, 1, taps);
-    load_cameras(s.cams, p.views, p.reference, targets, 1);
-    if (threadIdx.x == 0) fail = 0;
-    __syncthreads();
-    stage_node(s, patch, p.views, p.reference, targets, 1, cx, cy, p.radius, p.spatial, true);
-    const ViewGeom &g = s.geom[0];
-    const PlaneRef target_plane = tv.luma;
-    const double shared_depth = p.field.depth[node];
-    const double shared_inverse = 1.0 / shared_depth;
-    const double min_inverse = 1.0 / p.far_depth, max_inverse = 1.0 / p.near_depth;
-    const int lane = threadIdx.x;
-
-    // phase 1: five inverse-depth offsets (lanes 0-4) and the baseline (lane 5)
-    if (lane < 5) {
+    __syncwarp();
+    if (active) {
+        for (int t = lane; t < taps; t += DECISION_LANES) {
+            int dx, dy;
+            tap_offset(t, p.radius, dx, dy);
+            double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+            float value = 0.0f;
+            if (!plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value)) patch[slot].ok = 0;
+            float weight = p.spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
+            r[t] = value;
+            w[t] = weight;
+            wr[t] = weight * value;
+            float qx = 0.0f, qy = 0.0f;
+            if (!warp_map(tv.warp, (float)px, (float)py, qx, qy)) taps_ok[slot] = 0;
+            gq[t] = make_float2(qx, qy);
+        }
+    }
+    __syncwarp();
+    if (active && lane < 3) {  // the three sequential reference sums
+        float sum = 0.0f;
+        if (lane == 0)
+            for (int t = 0; t < taps; ++t) sum += w[t];
+        else if (lane == 1)
+            for (int t = 0; t < taps; ++t) sum += wr[t];
+        else
+            for (int t = 0; t < taps; ++t) sum += wr[t] * r[t];
+        if (lane == 0) patch[slot].count = sum;
+        if (lane == 1) patch[slot].sum_r = sum;
+        if (lane == 2) patch[slot].sum_rr = sum;
+    }
+    __syncwarp();
+    if (active && lane == 0)
+        patch[slot].ref_energy = patch[slot].sum_rr - patch[slot].sum_r * patch[slot].sum_r / patch[slot].count;
+    __syncwarp();
+    ViewGeom g;
+    if (active) geom_from_rec(p.geometry[(size_t)node * p.n_targets + vi], camera_origin(rv.cam), g);
+    const bool zncc_ok = active && patch[slot].ok && taps_ok[slot];
+    double shared_inverse = 0.0, min_inverse = 1.0 / p.far_depth, max_inverse = 1.0 / p.near_depth;
+    if (active) shared_inverse = 1.0 / p.field.depth[node];
+    // phase 1: five inverse-depth offsets and the baseline
+    if (active && lane < 5) {
         const double label_offset = -1.0 + 0.5 * lane;
         double inv = clampd_r(shared_inverse + label_offset * p.inverse_step, min_inverse, max_inverse);
         bool ok = g.ray_ok;
         double qx = 0.0, qy = 0.0;
-        if (ok) ok = project(s.cams[1], along({g.ox, g.oy, g.oz}, {g.dx, g.dy, g.dz}, 1.0 / inv), qx, qy);
+        if (ok) ok = project(tv.cam, along({g.ox, g.oy, g.oz}, {g.dx, g.dy, g.dz}, 1.0 / inv), qx, qy);
         if (ok) ok = isfinite(qx) && isfinite(qy);
         float2 point = make_float2((float)qx, (float)qy);
         float score = 0.0f;
         if (ok) {
-            double ddx = (double)(point.x - gq.x), ddy = (double)(point.y - gq.y);
-            ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && patch.ok && g.taps_ok &&
-                 zncc_score(target_plane, s.gq, s.w, s.wr, patch, taps, ddx, ddy, score);
+            double ddx = (double)(point.x - gq_c.x), ddy = (double)(point.y - gq_c.y);
+            ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && zncc_ok &&
+                 zncc_score(tv.luma, gq, w, wr, patch[slot], taps, ddx, ddy, score);
         }
-        if (!ok) atomicOr(&fail, 1);
-        sc[lane] = score;
-        pts[lane] = point;
-    } else if (lane == 5) {
-        float score = NAN;
-        float sv;
-        if (patch.ok && g.taps_ok && zncc_score(target_plane, s.gq, s.w, s.wr, patch, taps, 0.0, 0.0, sv)) score = sv;
-        sc[5] = score;
+        if (!ok) atomicOr(&fail[slot], 1);
+        sc[slot][lane] = score;
+        pts[slot][lane] = point;
+    } else if (active && lane == 5) {
+        float score = NAN, sv;
+        if (zncc_ok && zncc_score(tv.luma, gq, w, wr, patch[slot], taps, 0.0, 0.0, sv)) score = sv;
+        sc[slot][5] = score;
     }
-    __syncthreads();
-    float2 depth_point = make_float2(0.0f, 0.0f);
-    float depth_score = 0.0f;
-    if (!fail) {
+    __syncwarp();
+    if (active && lane == 0 && !fail[slot]) {  // best offset, in order, strict improvement
         float best_objective = 0.0f;
         for (int k = 0; k < 5; ++k) {
-            double label_offset = -1.0 + 0.5 * k;
-            float objective = sc[k] - (float)fabs(label_offset) * 0.002f;
+            float objective = sc[slot][k] - (float)fabs(-1.0 + 0.5 * k) * 0.002f;
             if (k == 0 || objective > best_objective) {
                 best_objective = objective;
-                depth_score = sc[k];
-                depth_point = pts[k];
+                sc[slot][14] = sc[slot][k];
+                pts[slot][14] = pts[slot][k];
             }
         }
     }
-    const float baseline = sc[5];
-    __syncthreads();
+    __syncwarp();
     // phase 2: eight residual shifts (dy outer, dx inner, centre skipped)
-    if (!fail && lane < 8) {
+    if (active && !fail[slot]) {
         int k = lane < 4 ? lane : lane + 1;
         float dx = -1.5f + 1.5f * (float)(k % 3), dy = -1.5f + 1.5f * (float)(k / 3);
+        float2 depth_point = pts[slot][14];
         float2 point = make_float2(depth_point.x + dx, depth_point.y + dy);
-        double ddx = (double)(point.x - gq.x), ddy = (double)(point.y - gq.y);
+        double ddx = (double)(point.x - gq_c.x), ddy = (double)(point.y - gq_c.y);
         float score = 0.0f;
-        bool ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && patch.ok && g.taps_ok &&
-                  zncc_score(target_plane, s.gq, s.w, s.wr, patch, taps, ddx, ddy, score);
-        if (!ok) atomicOr(&fail, 1);
-        sc[6 + lane] = score;
-        pts[6 + lane] = point;
+        bool ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && zncc_ok &&
+                  zncc_score(tv.luma, gq, w, wr, patch[slot], taps, ddx, ddy, score);
+        if (!ok) atomicOr(&fail[slot], 1);
+        sc[slot][6 + lane] = score;
+        pts[slot][6 + lane] = point;
     }
-    __syncthreads();
-    if (lane != 0) return;
-    bool selected = !fail;
+    __syncwarp();
+    if (!active || lane != 0) return;
+    const bool selected = !fail[slot];
     float sel_score = 0.0f;
     float2 sel_point = make_float2(0.0f, 0.0f);
     if (selected) {
-        float b0 = depth_score, b1 = depth_score;
-        float2 b2 = depth_point;
+        float b0 = sc[slot][14], b1 = sc[slot][14];
+        float2 b2 = pts[slot][14];
         for (int j = 0; j < 8; ++j) {
             int k = j < 4 ? j : j + 1;
             float dx = -1.5f + 1.5f * (float)(k % 3), dy = -1.5f + 1.5f * (float)(k / 3);
-            float residual_sq = dx * dx + dy * dy;
-            float objective = sc[6 + j] - residual_sq * 0.002f;
+            float objective = sc[slot][6 + j] - (dx * dx + dy * dy) * 0.002f;
             if (objective > b0) {
                 b0 = objective;
-                b1 = sc[6 + j];
-                b2 = pts[6 + j];
+                b1 = sc[slot][6 + j];
+                b2 = pts[slot][6 + j];
             }
         }
         sel_score = b1;
         sel_point = b2;
     }
+    const float baseline = sc[slot][5];
     const bool base_ok = baseline == baseline;
     const bool regularized = p.field.regularized[node] != 0;
     const float node_confidence = p.field.confidence[node];
-    bool supported = selected && sel_score >= p.minimum_score && (!base_ok || sel_score + 0.01f >= baseline);
-    bool contradicted = selected && base_ok && sel_score + 0.12f < baseline;
-    o.global[node] = gq;
+    const bool supported = selected && sel_score >= p.minimum_score && (!base_ok || sel_score + 0.01f >= baseline);
+    const bool contradicted = selected && base_ok && sel_score + 0.12f < baseline;
+    o.global[node] = gq_c;
     o.measured[node] = regularized ? 0 : 1;
     if (contradicted) {
         o.kind[node] = CHIARO_NW_OCCLUDED;
-        o.point[node] = gq;
+        o.point[node] = gq_c;
         o.confidence[node] = 0.0f;
     } else if (supported) {
         o.kind[node] = CHIARO_NW_REFINED;
@@ -176,7 +223,7 @@ __global__ void __launch_bounds__(32) target_decision_kernel(DecisionParams p) {
         o.confidence[node] = regularized ? node_confidence * 0.6f : 0.5f + 0.5f * node_confidence;
     } else {
         o.kind[node] = CHIARO_NW_GLOBAL;
-        o.point[node] = gq;
+        o.point[node] = gq_c;
         o.confidence[node] = 0.0f;
         o.measured[node] = 0;
     }

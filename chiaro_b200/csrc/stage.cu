@@ -141,15 +141,33 @@ void set_smem_limits() {
     if (done) return;
     CK(cudaFuncSetAttribute(cost_volume_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(direct_depth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(direct_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(target_decision_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done = true;
+}
+
+// Per (node, target) geometry records of a step-spaced grid.
+void launch_geometry(chiaro_depth_ctx *ctx, const DevView *d_views, int reference, const std::vector<int> &targets,
+                     size_t columns, size_t rows, size_t step, GeomRec *out) {
+    if (targets.empty()) return;
+    GeometryParams p{};
+    p.views = d_views;
+    p.reference = reference;
+    p.n_targets = (int)targets.size();
+    for (size_t v = 0; v < targets.size(); ++v) p.targets[v] = targets[v];
+    p.columns = (int)columns;
+    p.rows = (int)rows;
+    p.step = (int)step;
+    p.out = out;
+    view_geometry_kernel<<<blocks_for(columns * rows * targets.size(), 128), 128, 0, ctx->stream>>>(p);
+    CK(cudaGetLastError());
 }
 
 // ---- SGM ---------------------------------------------------------------------------
 void launch_sgm(chiaro_depth_ctx *ctx, const float *data, const float *guidance, float *out, int columns, int rows,
                 int labels) {
     const int K = (labels + 31) / 32;
-    const int threads = 256;
+    const int threads = SGM_THREADS;
     const int order[4] = {SGM_ROWS, SGM_COLUMNS, SGM_DOWN_RIGHT, SGM_DOWN_LEFT};
     bool first = true;
     for (int f : order) {
@@ -329,8 +347,12 @@ void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const
     float *costs = dbuf<float>(ctx, "costs", N * D);
     float *guidance = dbuf<float>(ctx, "guidance", N);
     uint8_t *tested = dbuf<uint8_t>(ctx, "tested", N);
+    GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
+    launch_geometry(ctx, d_views, reference, targets, g.coarse_columns, g.coarse_rows, g.coarse_step,
+                    coarse_geometry);
     {
         CostParams p{};
+        p.geometry = coarse_geometry;
         p.views = d_views;
         p.reference = reference;
         p.n_targets = V;
@@ -405,8 +427,11 @@ void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const
     Field direct = field_bufs(ctx, "direct", M);
     float *fguidance = dbuf<float>(ctx, "fine_guidance", M);
     uint8_t *ftested = dbuf<uint8_t>(ctx, "fine_tested", M);
+    GeomRec *fine_geometry = dbuf<GeomRec>(ctx, "fine_geometry", M * std::max(V, 1));
+    launch_geometry(ctx, d_views, reference, targets, g.columns, g.rows, g.step, fine_geometry);
     {
         DirectParams p{};
+        p.geometry = fine_geometry;
         p.views = d_views;
         p.reference = reference;
         p.n_targets = V;
@@ -434,8 +459,18 @@ void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const
         p.out = direct;
         p.guidance = fguidance;
         p.tested = ftested;
-        int taps_max = std::max((2 * wide_radius + 1) * (2 * wide_radius + 1), (2 * direct_radius + 1) * (2 * direct_radius + 1));
-        direct_depth_kernel<<<(unsigned)M, 128, node_smem_bytes(V, taps_max), s>>>(p);
+        p.wide_count = dbuf<int>(ctx, "wide_count", 1);
+        p.wide_list = dbuf<int4>(ctx, "wide_list", M);
+        CK(cudaMemsetAsync(p.wide_count, 0, sizeof(int), s));
+        const int taps = (2 * direct_radius + 1) * (2 * direct_radius + 1);
+        const int wide_taps = (2 * wide_radius + 1) * (2 * wide_radius + 1);
+        const size_t slot = direct_slot_bytes(V, taps), wide_slot = direct_slot_bytes(V, wide_taps);
+        p.nodes_per_cta = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / slot));
+        if (slot > 200 * 1024 || 4 * wide_slot > 200 * 1024)
+            throw CudaError{cudaErrorInvalidValue, "direct pass shared memory exceeds 200 KiB"};
+        direct_depth_kernel<<<blocks_for(M, p.nodes_per_cta), 32 * p.nodes_per_cta, p.nodes_per_cta * slot, s>>>(p);
+        CK(cudaGetLastError());
+        direct_wide_kernel<<<148 * 8, 128, 4 * wide_slot, s>>>(p);
         CK(cudaGetLastError());
     }
     if (debug) {
@@ -497,44 +532,54 @@ void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const
     medians_kernel<<<1, 1, 0, s>>>(depth_sorted, imp_sorted, d_results);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->events[5], s));
-    // ---- per-target decisions (depth.rs:420-547)
-    Decisions dec = decision_bufs(ctx, "dec", M), dec2 = decision_bufs(ctx, "dec2", M),
-              dec3 = decision_bufs(ctx, "dec3", M);
+    // ---- per-target decisions (depth.rs:420-547): all targets in one launch
     rewritten.clear();
-    for (int t : targets) {
+    if (V > 0) {
         DecisionParams p{};
         p.views = d_views;
         p.reference = reference;
-        p.target = t;
+        p.n_targets = V;
+        for (int v = 0; v < V; ++v) {
+            p.targets[v] = targets[v];
+            p.out[v] = decision_bufs(ctx, "dec" + std::to_string(v), M);
+        }
         p.columns = (int)g.columns;
         p.rows = (int)g.rows;
         p.step = (int)g.step;
         p.field = fin;
+        p.geometry = fine_geometry;
         p.inverse_step = inverse_step;
         p.near_depth = o.near_depth;
         p.far_depth = o.far_depth;
         p.radius = radius;
         p.spatial = d_sp;
         p.minimum_score = o.minimum_score;
-        p.out = dec;
         int taps = (2 * radius + 1) * (2 * radius + 1);
-        target_decision_kernel<<<(unsigned)M, 32, node_smem_bytes(1, taps), s>>>(p);
+        dim3 grid(blocks_for(M, DECISION_NODES), V);
+        target_decision_kernel<<<grid, DECISION_LANES * DECISION_NODES, decision_smem_bytes(taps), s>>>(p);
         CK(cudaGetLastError());
-        copy_decisions(ctx, dec2, dec, M);
-        warp_consensus_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec, dec2, (int)g.columns, (int)g.rows);
-        copy_decisions(ctx, dec3, dec2, M);
-        warp_boundary_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec2, dec3, fguidance, (int)g.columns, (int)g.rows);
-        warp_output_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec3, out.points[t], out.warp_confidence[t],
-                                                              d_results->target_counts[t], (int)M);
-        CK(cudaGetLastError());
-        if (debug && debug->decision_kind) download(ctx, debug->decision_kind + (size_t)t * M, dec3.kind, M);
-        rewritten.push_back(t);
+        Decisions dec2 = decision_bufs(ctx, "dec_consensus", M), dec3 = decision_bufs(ctx, "dec_boundary", M);
+        for (int v = 0; v < V; ++v) {
+            const int t = targets[v];
+            const Decisions &dec = p.out[v];
+            copy_decisions(ctx, dec2, dec, M);
+            warp_consensus_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec, dec2, (int)g.columns, (int)g.rows);
+            copy_decisions(ctx, dec3, dec2, M);
+            warp_boundary_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec2, dec3, fguidance, (int)g.columns,
+                                                                    (int)g.rows);
+            warp_output_kernel<<<blocks_for(M, 256), 256, 0, s>>>(dec3, out.points[t], out.warp_confidence[t],
+                                                                  d_results->target_counts[t], (int)M);
+            CK(cudaGetLastError());
+            if (debug && debug->decision_kind) download(ctx, debug->decision_kind + (size_t)t * M, dec3.kind, M);
+            rewritten.push_back(t);
+        }
     }
     depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->events[6], s));
-    // cost 1, SGM 8, select 1, completion, direct 1, filters 6, stats 2, 4 per target, map 1
-    ctx->launches = 1 + 8 + 1 + (int)o.completion_iterations + 1 + 6 + 2 + 4 * V + 1;
+    // geometry 2, cost 1, SGM 8, select 1, completion, direct 2, filters 6, stats 2,
+    // decisions 1 + 3 per target, map 1
+    ctx->launches = (V > 0 ? 2 : 0) + 1 + 8 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
     CK(cudaMemcpyAsync(&h_results, d_results, sizeof(Results), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ctx->timings[i], ctx->events[i], ctx->events[i + 1]));

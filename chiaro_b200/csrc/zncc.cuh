@@ -125,6 +125,63 @@ __device__ void view_geometry(const DevCamera &rc, const DevCamera &tc, const Wa
     g.ray_ok = 1;
 }
 
+// Compact per (node, target) geometry kept in HBM between kernels. pixel_to_ray
+// returns the camera centre as the origin for both pose kinds (geometry.rs:152-164),
+// so only the direction varies per node. gcx is NaN when global.map(centre) is
+// None, dx is NaN when the corrected reference pixel is None.
+struct GeomRec {
+    double dx, dy, dz;
+    float gcx, gcy;
+};
+
+__device__ __forceinline__ D3 camera_origin(const DevCamera &c) {
+    return c.pose_kind == 0 ? D3{c.center[0], c.center[1], c.center[2]}
+                            : D3{c.virtual_center[0], c.virtual_center[1], c.virtual_center[2]};
+}
+
+__device__ __forceinline__ void geom_from_rec(const GeomRec &rec, const D3 &origin, ViewGeom &g) {
+    g.gcx = rec.gcx;
+    g.gcy = rec.gcy;
+    g.gc_ok = !(rec.gcx != rec.gcx);
+    g.ray_ok = g.gc_ok && !(rec.dx != rec.dx);
+    g.ox = origin.x;
+    g.oy = origin.y;
+    g.oz = origin.z;
+    g.dx = rec.dx;
+    g.dy = rec.dy;
+    g.dz = rec.dz;
+    g.taps_ok = 1;
+}
+
+// One thread per (node, target) of a step-spaced grid: the label-independent
+// part of map_at_depth (depth.rs:1745-1756).
+struct GeometryParams {
+    const DevView *views;
+    int reference, n_targets;
+    int targets[MAX_VIEWS];
+    int columns, rows, step;
+    GeomRec *out;  // [node][target]
+};
+
+__global__ void __launch_bounds__(128) view_geometry_kernel(GeometryParams p) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long total = (long)p.columns * p.rows * p.n_targets;
+    if (i >= total) return;
+    int v = (int)(i % p.n_targets);
+    int node = (int)(i / p.n_targets);
+    double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
+    const DevView &tv = p.views[p.targets[v]];
+    ViewGeom g;
+    view_geometry(p.views[p.reference].cam, tv.cam, tv.warp, cx, cy, g);
+    GeomRec rec;
+    rec.gcx = g.gc_ok ? g.gcx : NAN;
+    rec.gcy = g.gc_ok ? g.gcy : NAN;
+    rec.dx = g.ray_ok ? g.dx : NAN;
+    rec.dy = g.ray_ok ? g.dy : NAN;
+    rec.dz = g.ray_ok ? g.dz : NAN;
+    p.out[i] = rec;
+}
+
 // map_at_depth's last step and score_one_view's displacement check: the
 // image displacement of a finite depth relative to the global centre. Returns
 // false for None (depth.rs:1604-1614).
