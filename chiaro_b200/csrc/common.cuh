@@ -179,6 +179,21 @@ CH_HD double exp_f64(double x) {
     return fma_d(scale, tmp, scale);
 }
 
+// floor(x) as an int and x - floor(x) for 0 <= x < 2^22, without the
+// conversion pipe: adding 2^23 rounds x to the nearest integer (its value is
+// in the low mantissa bits), and one compare corrects round-up to floor. All
+// steps are exact in that range.
+CH_HD float floor_frac_small(float x, int &ix) {
+    const float magic = 8388608.0f;  // 2^23
+    float t = x + magic;
+    float r = t - magic;  // nearest integer to x
+    int i = (int)(f2u(t) - 0x4B000000u);
+    bool up = r > x;
+    ix = up ? i - 1 : i;
+    r = up ? r - 1.0f : r;
+    return x - r;
+}
+
 // ---- Plane::sample (image.rs:451-466) --------------------------------------------
 struct PlaneRef {
     const float *data;
@@ -372,6 +387,7 @@ CH_HD D3 along(D3 origin, D3 direction, double depth) {
 // ---- device forms of the boundary types -------------------------------------------
 struct DevView {
     PlaneRef luma;
+    const float2 *pairs;  // (L[x], L[x+1]) pair plane of the luminance (targets only)
     WarpRef warp;
     int width, height;
     int has_camera, accepted;

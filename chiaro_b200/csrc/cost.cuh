@@ -32,15 +32,16 @@ struct CostParams {
 struct NodeSmem {
     DevCamera *cams;  // [0] reference, [1 + v] targets
     ViewGeom *geom;   // [V]
+    TapBox *box;      // [V]
     float *r, *w, *wr;  // [T]
-    float2 *gq;       // [V][T]
+    double2 *gh;      // [V][T] g/2 of the tap positions
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16; }
 
 __host__ __device__ inline size_t node_smem_bytes(int V, int taps) {
-    return align16((V + 1) * sizeof(DevCamera)) + align16(V * sizeof(ViewGeom)) + align16(3 * taps * sizeof(float)) +
-           (size_t)V * taps * sizeof(float2);
+    return align16((V + 1) * sizeof(DevCamera)) + align16(V * sizeof(ViewGeom)) + align16(V * sizeof(TapBox)) +
+           align16(3 * taps * sizeof(float)) + (size_t)V * taps * sizeof(double2);
 }
 
 __device__ inline NodeSmem carve_node_smem(unsigned char *base, int V, int taps) {
@@ -50,11 +51,13 @@ __device__ inline NodeSmem carve_node_smem(unsigned char *base, int V, int taps)
     o += align16((V + 1) * sizeof(DevCamera));
     s.geom = reinterpret_cast<ViewGeom *>(base + o);
     o += align16(V * sizeof(ViewGeom));
+    s.box = reinterpret_cast<TapBox *>(base + o);
+    o += align16(V * sizeof(TapBox));
     s.r = reinterpret_cast<float *>(base + o);
     s.w = s.r + taps;
     s.wr = s.w + taps;
     o += align16(3 * taps * sizeof(float));
-    s.gq = reinterpret_cast<float2 *>(base + o);
+    s.gh = reinterpret_cast<double2 *>(base + o);
     return s;
 }
 
@@ -81,7 +84,14 @@ __device__ inline void stage_node(const NodeSmem &s, RefPatch &patch, const DevV
         s.geom[v].taps_ok = 1;
     }
     ref_patch_setup(views[reference].luma, cx, cy, radius, spatial, s.r, s.w, s.wr, patch);
-    for (int v = 0; v < V; ++v) tap_positions(views[targets[v]].warp, cx, cy, radius, s.gq + v * taps, s.geom[v]);
+    for (int v = 0; v < V; ++v)
+        tap_positions(views[targets[v]].warp, cx, cy, radius, s.gh + v * taps, s.geom[v]);
+    __syncthreads();
+    // one warp per view computes its tap box
+    for (int v = threadIdx.x >> 5; v < V; v += blockDim.x >> 5) {
+        TapBox b = warp_tap_box(s.gh + v * taps, taps);
+        if ((threadIdx.x & 31) == 0) s.box[v] = b;
+    }
     __syncthreads();
 }
 
@@ -110,8 +120,10 @@ __global__ void __launch_bounds__(256) cost_volume_kernel(CostParams p) {
             if (!g.gc_ok) continue;
             if (label > 0 && !depth_delta(s.cams[1 + v], g, p.label_depth[label], ddx, ddy)) continue;
             if (!patch.ok || !g.taps_ok) continue;
+            const DevView &tv = p.views[p.targets[v]];
             float score;
-            if (zncc_score(p.views[p.targets[v]].luma, s.gq + v * taps, s.w, s.wr, patch, taps, ddx, ddy, score))
+            if (zncc_any(TargetRef{tv.luma, tv.pairs}, s.gh + v * taps, s.box[v], s.w, s.wr, patch, taps, ddx, ddy,
+                         score))
                 sc[v] = score;
         }
         float agg;
@@ -128,11 +140,9 @@ __global__ void __launch_bounds__(256) cost_volume_kernel(CostParams p) {
         p.scores[o] = score;
         p.costs[o] = cost;
     }
-    int tested = __syncthreads_or(any_finite);
-    if (threadIdx.x == 0) {
-        p.tested[node] = tested ? 1 : 0;
-        p.guidance[node] = patch.centre;  // reference_guidance (depth.rs:1824-1832): sample or 0
-    }
+    // tested: any finite score; p.tested starts zeroed, one store per warp that saw one
+    if (__ballot_sync(0xffffffffu, any_finite) && (threadIdx.x & 31) == 0) p.tested[node] = 1;
+    if (threadIdx.x == 0) p.guidance[node] = patch.centre;  // reference_guidance (depth.rs:1824-1832)
 }
 
 }  // namespace chiaro

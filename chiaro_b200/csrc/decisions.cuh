@@ -38,20 +38,21 @@ constexpr int DECISION_LANES = 8;     // lanes per (node, target)
 constexpr int DECISION_NODES = 32;    // nodes per CTA (256 threads)
 
 __host__ __device__ inline size_t decision_smem_bytes(int taps) {
-    // per node slot: r, w, wr, and tap positions of the target
-    return (size_t)DECISION_NODES * (3 * taps * sizeof(float) + taps * sizeof(float2));
+    // per node slot: r, w, wr, and the target's tap positions (g/2)
+    return (size_t)DECISION_NODES * (3 * taps * sizeof(float) + taps * sizeof(double2));
 }
 
 // One CTA handles 32 nodes of one target (blockIdx.y); each node belongs to an
 // aligned group of 8 lanes inside one warp. Lanes 0-4 score the five
 // inverse-depth offsets and lane 5 the baseline; after lane 0 picks the best
 // offset, lanes 0-7 score the eight residual shifts; lane 0 classifies.
-__global__ void __launch_bounds__(256) target_decision_kernel(DecisionParams p) {
+__global__ void __launch_bounds__(DECISION_LANES * DECISION_NODES) target_decision_kernel(DecisionParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patch[DECISION_NODES];
     __shared__ float sc[DECISION_NODES][16];
     __shared__ float2 pts[DECISION_NODES][16];
     __shared__ int fail[DECISION_NODES], taps_ok[DECISION_NODES];
+    __shared__ TapBox boxes[DECISION_NODES];
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
     const int slot = threadIdx.x / DECISION_LANES, lane = threadIdx.x % DECISION_LANES;
     const int node = blockIdx.x * DECISION_NODES + slot;
@@ -62,8 +63,8 @@ __global__ void __launch_bounds__(256) target_decision_kernel(DecisionParams p) 
     Decisions o = p.out[vi];
     float *r = reinterpret_cast<float *>(smem_raw) + (size_t)slot * 3 * taps;
     float *w = r + taps, *wr = w + taps;
-    float2 *gq = reinterpret_cast<float2 *>(smem_raw + (size_t)DECISION_NODES * 3 * taps * sizeof(float)) +
-                 (size_t)slot * taps;
+    double2 *gh = reinterpret_cast<double2 *>(smem_raw + (size_t)DECISION_NODES * 3 * taps * sizeof(float)) +
+                  (size_t)slot * taps;
 
     bool active = node < p.columns * p.rows;
     const double cx = active ? (double)((node % p.columns) * p.step) : 0.0;
@@ -109,10 +110,20 @@ __global__ void __launch_bounds__(256) target_decision_kernel(DecisionParams p) 
             wr[t] = weight * value;
             float qx = 0.0f, qy = 0.0f;
             if (!warp_map(tv.warp, (float)px, (float)py, qx, qy)) taps_ok[slot] = 0;
-            gq[t] = make_float2(qx, qy);
+            gh[t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
         }
     }
     __syncwarp();
+    if (active && lane == 3) {  // box of this node's taps (one lane of the group)
+        TapBox b{gh[0].x, gh[0].x, gh[0].y, gh[0].y};
+        for (int t = 1; t < taps; ++t) {
+            b.xmin = fmin(b.xmin, gh[t].x);
+            b.xmax = fmax(b.xmax, gh[t].x);
+            b.ymin = fmin(b.ymin, gh[t].y);
+            b.ymax = fmax(b.ymax, gh[t].y);
+        }
+        boxes[slot] = b;
+    }
     if (active && lane < 3) {  // the three sequential reference sums
         float sum = 0.0f;
         if (lane == 0)
@@ -132,6 +143,7 @@ __global__ void __launch_bounds__(256) target_decision_kernel(DecisionParams p) 
     ViewGeom g;
     if (active) geom_from_rec(p.geometry[(size_t)node * p.n_targets + vi], camera_origin(rv.cam), g);
     const bool zncc_ok = active && patch[slot].ok && taps_ok[slot];
+    const TargetRef target_ref{tv.luma, tv.pairs};
     double shared_inverse = 0.0, min_inverse = 1.0 / p.far_depth, max_inverse = 1.0 / p.near_depth;
     if (active) shared_inverse = 1.0 / p.field.depth[node];
     // phase 1: five inverse-depth offsets and the baseline
@@ -147,14 +159,14 @@ __global__ void __launch_bounds__(256) target_decision_kernel(DecisionParams p) 
         if (ok) {
             double ddx = (double)(point.x - gq_c.x), ddy = (double)(point.y - gq_c.y);
             ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && zncc_ok &&
-                 zncc_score(tv.luma, gq, w, wr, patch[slot], taps, ddx, ddy, score);
+                 zncc_any(target_ref, gh, boxes[slot], w, wr, patch[slot], taps, ddx, ddy, score);
         }
         if (!ok) atomicOr(&fail[slot], 1);
         sc[slot][lane] = score;
         pts[slot][lane] = point;
     } else if (active && lane == 5) {
         float score = NAN, sv;
-        if (zncc_ok && zncc_score(tv.luma, gq, w, wr, patch[slot], taps, 0.0, 0.0, sv)) score = sv;
+        if (zncc_ok && zncc_any(target_ref, gh, boxes[slot], w, wr, patch[slot], taps, 0.0, 0.0, sv)) score = sv;
         sc[slot][5] = score;
     }
     __syncwarp();
@@ -179,7 +191,7 @@ __global__ void __launch_bounds__(256) target_decision_kernel(DecisionParams p) 
         double ddx = (double)(point.x - gq_c.x), ddy = (double)(point.y - gq_c.y);
         float score = 0.0f;
         bool ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && zncc_ok &&
-                  zncc_score(tv.luma, gq, w, wr, patch[slot], taps, ddx, ddy, score);
+                  zncc_any(target_ref, gh, boxes[slot], w, wr, patch[slot], taps, ddx, ddy, score);
         if (!ok) atomicOr(&fail[slot], 1);
         sc[slot][6 + lane] = score;
         pts[slot][6 + lane] = point;

@@ -114,14 +114,16 @@ struct DirectParams {
 // Per-warp shared memory of the direct pass for V targets and T taps.
 struct DirectSlot {
     float *r, *w, *wr;   // [T]
-    float2 *gq;          // [V][T]
+    double2 *gh;         // [V][T] g/2 (fast path)
+    TapBox *box;         // [V]
     double *cand;        // [32]
     float *items;        // [33][V]
     float *agg;          // [33]: [0] baseline, [1 + c] candidates
 };
 
 __host__ __device__ inline size_t direct_slot_bytes(int V, int taps) {
-    return align16(3 * taps * sizeof(float)) + align16((size_t)V * taps * sizeof(float2)) +
+    return align16(3 * taps * sizeof(float)) + align16((size_t)V * taps * sizeof(double2)) +
+           align16(V * sizeof(TapBox)) +
            align16(MAX_DIRECT_CANDIDATES * sizeof(double)) +
            align16((size_t)(MAX_DIRECT_CANDIDATES + 1) * V * sizeof(float)) +
            align16((MAX_DIRECT_CANDIDATES + 1) * sizeof(float));
@@ -134,8 +136,10 @@ __device__ inline DirectSlot carve_direct_slot(unsigned char *base, int V, int t
     d.w = d.r + taps;
     d.wr = d.w + taps;
     o += align16(3 * taps * sizeof(float));
-    d.gq = reinterpret_cast<float2 *>(base + o);
-    o += align16((size_t)V * taps * sizeof(float2));
+    d.gh = reinterpret_cast<double2 *>(base + o);
+    o += align16((size_t)V * taps * sizeof(double2));
+    d.box = reinterpret_cast<TapBox *>(base + o);
+    o += align16(V * sizeof(TapBox));
     d.cand = reinterpret_cast<double *>(base + o);
     o += align16(MAX_DIRECT_CANDIDATES * sizeof(double));
     d.items = reinterpret_cast<float *>(base + o);
@@ -200,10 +204,14 @@ __device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot &
         for (int v = 0; v < V; ++v) {
             float qx = 0.0f, qy = 0.0f;
             if (!warp_map(p.views[p.targets[v]].warp, (float)px, (float)py, qx, qy)) geom[v].taps_ok = 0;
-            d.gq[v * taps + t] = make_float2(qx, qy);
+            d.gh[v * taps + t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
         }
     }
     __syncwarp();
+    for (int v = 0; v < V; ++v) {
+        TapBox b = warp_tap_box(d.gh + v * taps, taps);
+        if (lane == 0) d.box[v] = b;
+    }
     if (lane < 3) {
         float sum = 0.0f;
         if (lane == 0)
@@ -236,8 +244,10 @@ __device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlo
         bool ok = g.gc_ok;
         if (ok && c >= 0) ok = depth_delta(p.views[p.targets[v]].cam, g, cand[c], ddx, ddy);
         if (ok && patch.ok && g.taps_ok) {
+            const DevView &tv = p.views[p.targets[v]];
             float sc;
-            if (zncc_score(p.views[p.targets[v]].luma, d.gq + v * taps, d.w, d.wr, patch, taps, ddx, ddy, sc))
+            if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, ddx, ddy,
+                         sc))
                 score = sc;
         }
         d.items[item] = score;

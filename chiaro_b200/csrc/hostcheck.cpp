@@ -55,6 +55,20 @@ uint64_t chiaro_hc_exp_mismatches(uint32_t lo, uint32_t hi, double scale, uint32
     return bad;
 }
 
+// Mismatches of floor_frac_small against floorf over float bit patterns [lo, hi).
+uint64_t chiaro_hc_floor_mismatches(uint32_t lo, uint32_t hi) {
+    uint64_t bad = 0;
+    for (uint32_t u = lo; u < hi; ++u) {
+        float x;
+        memcpy(&x, &u, 4);
+        int i;
+        float frac = floor_frac_small(x, i);
+        float f = std::floor(x);
+        if ((float)i != f || f2u(frac) != f2u(x - f)) ++bad;
+    }
+    return bad;
+}
+
 float chiaro_hc_plane_sample(const float *data, int width, int height, float x, float y, int *ok) {
     PlaneRef p{data, width, height};
     float v = 0.0f;

@@ -1,14 +1,10 @@
 // sgm.cuh — semi_global_costs (crates/chiaro-fusion/src/depth.rs:1279-1383).
 //
-// Eight-path SGM over the label-minor f32 volume. One warp walks one path; a
-// lane holds labels lane, lane+32, ... in registers, the previous node's
-// minimum comes from a warp-shuffle min, and label +-1 neighbours from
-// shuffles. The reference adds the eight path costs into one output in a
+// Eight-path SGM over the label-minor f32 volume. The reference adds the eight path costs into one output in a
 // fixed order per node: rows forward, rows reverse, columns forward, columns
 // reverse, down-right forward/reverse, down-left forward/reverse
-// (depth.rs:1287-1309). Float addition is not associative, so the launches
-// follow that order: each direction is one launch that adds its path costs to
-// the output (the first one stores 0 + L), which keeps the sum bit-identical.
+// (depth.rs:1287-1309). Float addition is not associative, so the passes keep
+// that order exactly (see the schedule below), which keeps the sum bit-identical.
 #pragma once
 
 #include "common.cuh"
@@ -45,121 +41,117 @@ __device__ inline void sgm_path(int family, int p, int columns, int rows, int &r
     }
 }
 
-// accumulate_path for every path of one family and direction.
-// accumulate == 0: out = 0 + L (first direction); otherwise out += L.
-// The cost vector and (when accumulating) the output vector of the node PREFETCH
-// steps ahead are loaded into a register ring, so memory latency stays off the
-// recurrence's critical path (the warp-shuffle minimum and a few adds).
-template <int K>
-struct SgmPrefetch {  // ring depth that keeps the ring in registers without spills
-    static constexpr int value = K <= 4 ? 8 : (K <= 6 ? 6 : 3);
-};
-constexpr int SGM_THREADS = 64;  // two paths per CTA: spread few long paths over all SMs
+// One launch per direction, in the reference's order, so each node receives
+// 0 + L1, then + L2, ..., + L8 exactly as depth.rs:1287-1309 adds them.
+//
+// A path is walked by K warps, one per 32-label chunk (K = ceil(labels / 32)),
+// so each warp handles one label per lane per step. Per step, each warp takes
+// its chunk's minimum with redux.sync.min.f32, publishes it together with its
+// first and last label values in shared memory, and after the path's named
+// barrier reads the other chunks' minima (min is exact, so the combination
+// order does not matter) and its neighbours across the chunk boundary. The
+// exchange buffers alternate between steps, so one barrier per step suffices.
+// Each warp prefetches its chunk of the cost and output vectors P steps ahead.
+constexpr int SGM_PREFETCH = 8;
 
-template <int K>
-__device__ __forceinline__ void sgm_load(const float *__restrict__ data, const float *out, int node, int labels,
-                                         int lane, bool accumulate, float (&c)[K], float (&o)[K]) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        int l = lane + 32 * k;
-        bool in = l < labels;
-        c[k] = in ? __ldg(data + (size_t)node * labels + l) : 0.0f;
-        o[k] = (in && accumulate) ? __ldcg(out + (size_t)node * labels + l) : 0.0f;
-    }
+__device__ __forceinline__ float warp_min_f32(float v) {
+    float r;
+    asm volatile("redux.sync.min.f32 %0, %1, %2;" : "=f"(r) : "f"(v), "r"(0xffffffffu));
+    return r;
 }
 
+__device__ __forceinline__ void path_barrier(int threads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
+}
+
+// One direction of one family: every block walks one path, forward or in
+// reverse, adding its costs to `out` (`first` stores 0 + L).
 template <int K>
-__global__ void __launch_bounds__(SGM_THREADS) sgm_direction_kernel(const float *__restrict__ data,
-                                                            const float *__restrict__ guidance, float *out,
-                                                            int columns, int rows, int labels, int family,
-                                                            int reverse, int accumulate) {
+__global__ void __launch_bounds__(32 * K, 4) sgm_direction_kernel(const float *__restrict__ data,
+                                                                 const float *__restrict__ guidance, float *out,
+                                                                 int columns, int rows, int labels, int family,
+                                                                 int first, int reverse) {
+    __shared__ float xmin[2][K], xfirst[2][K], xlast[2][K];
     const int lane = threadIdx.x & 31;
-    const int path = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (path >= sgm_path_count(family, columns, rows)) return;
+    const int chunk = threadIdx.x >> 5;
     int r0, c0, dr, dc, len;
-    sgm_path(family, path, columns, rows, r0, c0, dr, dc, len);
+    sgm_path(family, blockIdx.x, columns, rows, r0, c0, dr, dc, len);
     if (reverse) {
         r0 += dr * (len - 1);
         c0 += dc * (len - 1);
         dr = -dr;
         dc = -dc;
     }
-    const int dstep = dr * columns + dc;  // node index increment along the path
-    const unsigned full = 0xffffffffu;
-    const bool acc = accumulate != 0;
-    constexpr int SGM_PREFETCH = SgmPrefetch<K>::value;
-    float prev[K];
-    int node = r0 * columns + c0;
+    constexpr int P = SGM_PREFETCH;
+    const int l = chunk * 32 + lane;
+    const bool valid = l < labels;
+    const bool fold = !first;  // out = first ? 0 + L : out + L
+    const long node_step = (long)dr * columns + dc;
+    const long stride = node_step * labels;
+    const int node0 = r0 * columns + c0;
+    const size_t e0 = (size_t)node0 * labels + l;
+    const float *dp = data + e0;
+    float *wp = out + e0;
+    const float *op = out + e0;
+    const float *gp = guidance + node0;
+    float prev;
     {
-        float c[K], o[K];
-        sgm_load<K>(data, out, node, labels, lane, acc, c, o);
+        float c = valid ? __ldg(dp) : 0.0f;
+        float b = valid && fold ? __ldcg(op) : 0.0f;
+        prev = valid ? c : INFINITY;
+        if (valid) *wp = fold ? b + c : 0.0f + c;
+    }
+    float g_prev = __ldg(gp);
+    float ring_c[P], ring_o[P], ring_g[P];
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            int l = lane + 32 * k;
-            prev[k] = l < labels ? c[k] : INFINITY;
-            if (l < labels) out[(size_t)node * labels + l] = acc ? o[k] + c[k] : 0.0f + c[k];
+    for (int j = 0; j < P; ++j) {
+        if (1 + j < len) {
+            ring_c[j] = valid ? __ldg(dp + (1 + j) * stride) : 0.0f;
+            ring_o[j] = valid && fold ? __ldcg(op + (1 + j) * stride) : 0.0f;
+            ring_g[j] = __ldg(gp + (1 + j) * node_step);
         }
     }
-    float g_prev = __ldg(guidance + node);
-    // register ring of the next PREFETCH nodes
-    float ring_c[SGM_PREFETCH][K], ring_o[SGM_PREFETCH][K], ring_g[SGM_PREFETCH];
+    int parity = 0;
+    for (int base = 1; base < len; base += P) {
 #pragma unroll
-    for (int j = 0; j < SGM_PREFETCH; ++j) {
-        int step = 1 + j;
-        if (step < len) {
-            int nj = node + step * dstep;
-            sgm_load<K>(data, out, nj, labels, lane, acc, ring_c[j], ring_o[j]);
-            ring_g[j] = __ldg(guidance + nj);
-        }
-    }
-    for (int base = 1; base < len; base += SGM_PREFETCH) {
-#pragma unroll
-        for (int j = 0; j < SGM_PREFETCH; ++j) {
+        for (int j = 0; j < P; ++j) {
             const int step = base + j;
-            if (step >= len) break;  // warp-uniform
-            const int nd = node + step * dstep;
-            float cur_data[K], cur_out[K];
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                cur_data[k] = ring_c[j][k];
-                cur_out[k] = ring_o[j][k];
+            if (step >= len) break;  // uniform across the path's warps
+            wp += stride;
+            const float cur_data = ring_c[j], cur_base = ring_o[j], g = ring_g[j];
+            if (step + P < len) {
+                ring_c[j] = valid ? __ldg(dp + (step + P) * stride) : 0.0f;
+                ring_o[j] = valid && fold ? __ldcg(op + (step + P) * stride) : 0.0f;
+                ring_g[j] = __ldg(gp + (step + P) * node_step);
             }
-            const float g = ring_g[j];
-            if (step + SGM_PREFETCH < len) {
-                int nn = node + (step + SGM_PREFETCH) * dstep;
-                sgm_load<K>(data, out, nn, labels, lane, acc, ring_c[j], ring_o[j]);
-                ring_g[j] = __ldg(guidance + nn);
+            // publish this chunk's minimum and boundary labels, then combine
+            const float chunk_min = warp_min_f32(prev);
+            if (lane == 0) {
+                xmin[parity][chunk] = chunk_min;
+                xfirst[parity][chunk] = prev;
             }
-            float edge = fabsf(g - g_prev);
+            if (lane == 31) xlast[parity][chunk] = prev;
+            const float rot_up = __shfl_sync(0xffffffffu, prev, (lane + 31) & 31);
+            const float rot_down = __shfl_sync(0xffffffffu, prev, (lane + 1) & 31);
+            const float edge = fabsf(g - g_prev);
             g_prev = g;
-            float edge_scale = 1.0f / (1.0f + 4.0f * edge);
-            float p1 = SGM_SMALL_PENALTY * fmaxf(edge_scale, 0.35f);
-            float p2 = SGM_LARGE_PENALTY * fmaxf(edge_scale, 0.12f);
-            float m = prev[0];
+            const float edge_scale = __frcp_rn(1.0f + 4.0f * edge);  // == 1 / x, correctly rounded
+            const float p1 = SGM_SMALL_PENALTY * fmaxf(edge_scale, 0.35f);
+            const float p2 = SGM_LARGE_PENALTY * fmaxf(edge_scale, 0.12f);
+            if (K > 1) path_barrier(32 * K);
+            float minimum_previous = K > 1 ? xmin[parity][0] : chunk_min;
 #pragma unroll
-            for (int k = 1; k < K; ++k) m = fminf(m, prev[k]);
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_xor_sync(full, m, off));
-            const float minimum_previous = m;
+            for (int k = 1; k < K; ++k) minimum_previous = fminf(minimum_previous, xmin[parity][k]);
+            float below = rot_up, above = rot_down;
+            if (lane == 0) below = chunk > 0 ? xlast[parity][chunk > 0 ? chunk - 1 : 0] : INFINITY;
+            if (lane == 31) above = chunk + 1 < K ? xfirst[parity][chunk + 1 < K ? chunk + 1 : chunk] : INFINITY;
+            parity ^= 1;
             const float jump = minimum_previous + p2;
-            float cur[K];
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                int l = lane + 32 * k;
-                float below = __shfl_up_sync(full, prev[k], 1);
-                float above = __shfl_down_sync(full, prev[k], 1);
-                float wrap_below = k > 0 ? __shfl_sync(full, prev[k > 0 ? k - 1 : 0], 31) : INFINITY;
-                float wrap_above = k + 1 < K ? __shfl_sync(full, prev[k + 1 < K ? k + 1 : k], 0) : INFINITY;
-                if (lane == 0) below = wrap_below;
-                if (lane == 31) above = wrap_above;
-                float lower = l > 0 ? below + p1 : INFINITY;
-                float higher = l + 1 < labels ? above + p1 : INFINITY;
-                float v = cur_data[k] + fminf(fminf(fminf(prev[k], lower), higher), jump) - minimum_previous;
-                cur[k] = l < labels ? v : INFINITY;
-                if (l < labels) out[(size_t)nd * labels + l] = acc ? cur_out[k] + v : 0.0f + v;
-            }
-#pragma unroll
-            for (int k = 0; k < K; ++k) prev[k] = cur[k];
+            const float lower = below + p1;  // INFINITY + p1 = INFINITY
+            const float higher = l + 1 < labels ? above + p1 : INFINITY;
+            const float v = cur_data + fminf(fminf(fminf(prev, lower), higher), jump) - minimum_previous;
+            prev = valid ? v : INFINITY;
+            if (valid) *wp = fold ? cur_base + v : 0.0f + v;
         }
     }
 }

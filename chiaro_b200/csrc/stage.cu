@@ -164,30 +164,35 @@ void launch_geometry(chiaro_depth_ctx *ctx, const DevView *d_views, int referenc
 }
 
 // ---- SGM ---------------------------------------------------------------------------
+template <int K>
+void sgm_pass(chiaro_depth_ctx *ctx, unsigned blocks, const float *data, const float *guidance, float *out,
+              int columns, int rows, int labels, int family, int first, int reverse) {
+    sgm_direction_kernel<K><<<blocks, 32 * K, 0, ctx->stream>>>(data, guidance, out, columns, rows, labels, family,
+                                                                first, reverse);
+    CK(cudaGetLastError());
+}
+
+void sgm_dispatch(chiaro_depth_ctx *ctx, int K, unsigned blocks, const float *data, const float *guidance,
+                  float *out, int columns, int rows, int labels, int family, int first, int reverse) {
+    switch (K) {
+#define SGM_CASE(k)                                                                                              \
+    case k:                                                                                                      \
+        return sgm_pass<k>(ctx, blocks, data, guidance, out, columns, rows, labels, family, first, reverse);
+        SGM_CASE(1) SGM_CASE(2) SGM_CASE(3) SGM_CASE(4) SGM_CASE(5) SGM_CASE(6) SGM_CASE(7) SGM_CASE(8)
+#undef SGM_CASE
+        default: throw CudaError{cudaErrorInvalidValue, "labels exceed 256"};
+    }
+}
+
+// One launch per direction, in the reference's summation order (sgm.cuh).
 void launch_sgm(chiaro_depth_ctx *ctx, const float *data, const float *guidance, float *out, int columns, int rows,
                 int labels) {
-    const int K = (labels + 31) / 32;
-    const int threads = SGM_THREADS;
+    const int K = (labels + 31) / 32;  // warps per path
     const int order[4] = {SGM_ROWS, SGM_COLUMNS, SGM_DOWN_RIGHT, SGM_DOWN_LEFT};
-    bool first = true;
-    for (int f : order) {
-        int paths = sgm_path_count(f, columns, rows);
-        unsigned blocks = blocks_for((size_t)paths * 32, threads);
-        for (int reverse = 0; reverse < 2; ++reverse) {
-            int acc = first ? 0 : 1;
-            switch (K) {
-#define SGM_CASE(k)                                                                                        \
-    case k:                                                                                                \
-        sgm_direction_kernel<k><<<blocks, threads, 0, ctx->stream>>>(data, guidance, out, columns, rows, labels, \
-                                                                     f, reverse, acc);                     \
-        break;
-                SGM_CASE(1) SGM_CASE(2) SGM_CASE(3) SGM_CASE(4) SGM_CASE(5) SGM_CASE(6) SGM_CASE(7) SGM_CASE(8)
-#undef SGM_CASE
-                default: throw CudaError{cudaErrorInvalidValue, "labels exceed 256"};
-            }
-            CK(cudaGetLastError());
-            first = false;
-        }
+    for (int pass = 0; pass < 8; ++pass) {
+        const int f = order[pass / 2];
+        sgm_dispatch(ctx, K, (unsigned)sgm_path_count(f, columns, rows), data, guidance, out, columns, rows, labels,
+                     f, pass == 0, pass % 2);
     }
 }
 
@@ -299,7 +304,7 @@ void download_field(chiaro_depth_ctx *ctx, const Field &f, size_t n, uint8_t *ha
 
 // Run the whole stage on device-resident views. h_views: the DevView array
 // (device pointers inside), d_views: its device copy.
-void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const DevView *d_views, int reference,
+void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_views, int reference,
                const chiaro_depth_options &o, const Grids &g, const StageOutputs &out, Results *d_results,
                Results &h_results, const chiaro_depth_debug *debug, std::vector<int> &rewritten) {
     cudaStream_t s = ctx->stream;
@@ -342,11 +347,22 @@ void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const
     CK(cudaMemsetAsync(d_results, 0, sizeof(Results), s));
 
     CK(cudaEventRecord(ctx->events[0], s));
+    // (L[x], L[x+1]) pair planes of the target luminance for the fast ZNCC path
+    for (int t : targets) {
+        const PlaneRef &lp = h_views[t].luma;
+        size_t n = (size_t)lp.width * lp.height;
+        float2 *pairs = dbuf<float2>(ctx, "pairs" + std::to_string(t), n);
+        pair_plane_kernel<<<blocks_for(n, 256), 256, 0, s>>>(lp.data, lp.width, lp.height, pairs);
+        CK(cudaGetLastError());
+        h_views[t].pairs = pairs;
+    }
+    upload(ctx, d_views, h_views.data(), h_views.size());
     // ---- cost volume
     float *scores = dbuf<float>(ctx, "scores", N * D);
     float *costs = dbuf<float>(ctx, "costs", N * D);
     float *guidance = dbuf<float>(ctx, "guidance", N);
     uint8_t *tested = dbuf<uint8_t>(ctx, "tested", N);
+    CK(cudaMemsetAsync(tested, 0, N, s));  // the cost kernel only sets tested nodes
     GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
     launch_geometry(ctx, d_views, reference, targets, g.coarse_columns, g.coarse_rows, g.coarse_step,
                     coarse_geometry);
@@ -577,9 +593,9 @@ void run_stage(chiaro_depth_ctx *ctx, const std::vector<DevView> &h_views, const
     depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->events[6], s));
-    // geometry 2, cost 1, SGM 8, select 1, completion, direct 2, filters 6, stats 2,
+    // pair planes 1 per target, geometry 2, cost 1, SGM 8, select 1, completion, direct 2, filters 6, stats 2,
     // decisions 1 + 3 per target, map 1
-    ctx->launches = (V > 0 ? 2 : 0) + 1 + 8 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
+    ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 8 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
     CK(cudaMemcpyAsync(&h_results, d_results, sizeof(Results), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ctx->timings[i], ctx->events[i], ctx->events[i + 1]));
@@ -626,6 +642,10 @@ int validate(const chiaro_view *views, size_t n_views, size_t reference_index, c
         const chiaro_view &v = views[i];
         if (!v.luminance || v.luma_width < 1 || v.luma_height < 1 || !v.warp.points || v.warp.step < 1 ||
             v.warp.columns < 1 || v.warp.rows < 1)
+            return CHIARO_ERR_ARGUMENT;
+        // planes and grids addressed with 32-bit indices; planes below 2^22 pixels per side
+        if (v.luma_width >= (1u << 22) || v.luma_height >= (1u << 22) ||
+            v.luma_width * v.luma_height >= (1ull << 31) || v.warp.columns * v.warp.rows >= (1ull << 31))
             return CHIARO_ERR_ARGUMENT;
     }
     return CHIARO_OK;

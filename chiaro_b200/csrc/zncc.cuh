@@ -33,6 +33,10 @@ struct ViewGeom {
     int pad;
 };
 
+struct TapBox {
+    double xmin, xmax, ymin, ymax;  // of g/2 over the taps
+};
+
 __device__ __forceinline__ void tap_offset(int t, int radius, int &dx, int &dy) {
     int side = 2 * radius + 1;
     dy = t / side - radius;
@@ -86,9 +90,10 @@ __device__ void ref_patch_setup(const PlaneRef &ref, double cx, double cy, int r
     __syncthreads();
 }
 
-// Global-warp positions of every tap for one target warp; clears
-// geom.taps_ok when one is undefined. Block-cooperative, no trailing sync.
-__device__ void tap_positions(const WarpRef &warp, double cx, double cy, int radius, float2 *gq, ViewGeom &geom) {
+// Global-warp positions g of every tap for one target warp, stored as g/2 in
+// f64 (exact: g is f32); clears geom.taps_ok when one is undefined.
+// Block-cooperative, no trailing sync.
+__device__ void tap_positions(const WarpRef &warp, double cx, double cy, int radius, double2 *gh, ViewGeom &geom) {
     int taps = (2 * radius + 1) * (2 * radius + 1);
     for (int t = threadIdx.x; t < taps; t += blockDim.x) {
         int dx, dy;
@@ -96,8 +101,29 @@ __device__ void tap_positions(const WarpRef &warp, double cx, double cy, int rad
         double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
         float qx = 0.0f, qy = 0.0f;
         if (!warp_map(warp, (float)px, (float)py, qx, qy)) geom.taps_ok = 0;
-        gq[t] = make_float2(qx, qy);
+        gh[t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
     }
+}
+
+// Bounding box of g/2 over the taps, computed by one whole warp (min/max are
+// exact, so the reduction order does not matter). Every lane gets the box.
+__device__ inline TapBox warp_tap_box(const double2 *gh, int taps) {
+    const int lane = threadIdx.x & 31;
+    TapBox b{gh[0].x, gh[0].x, gh[0].y, gh[0].y};
+    for (int t = lane; t < taps; t += 32) {
+        b.xmin = fmin(b.xmin, gh[t].x);
+        b.xmax = fmax(b.xmax, gh[t].x);
+        b.ymin = fmin(b.ymin, gh[t].y);
+        b.ymax = fmax(b.ymax, gh[t].y);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        b.xmin = fmin(b.xmin, __shfl_xor_sync(0xffffffffu, b.xmin, off));
+        b.xmax = fmax(b.xmax, __shfl_xor_sync(0xffffffffu, b.xmax, off));
+        b.ymin = fmin(b.ymin, __shfl_xor_sync(0xffffffffu, b.ymin, off));
+        b.ymax = fmax(b.ymax, __shfl_xor_sync(0xffffffffu, b.ymax, off));
+    }
+    return b;
 }
 
 // Label-independent geometry of map_at_depth for one (node, target); one thread.
@@ -198,11 +224,12 @@ __device__ __forceinline__ bool depth_delta(const DevCamera &tc, const ViewGeom 
 
 // Hypothesis-dependent part of warped_patch_zncc: sample the target at every
 // tap shifted by (ddx, ddy) and finish the correlation. False for None.
-__device__ __forceinline__ bool zncc_score(const PlaneRef &target, const float2 *gq, const float *w, const float *wr,
+__device__ __forceinline__ bool zncc_score(const PlaneRef &target, const double2 *gh, const float *w, const float *wr,
                                            const RefPatch &patch, int taps, double ddx, double ddy, float &score) {
     float st = 0.0f, stt = 0.0f, srt = 0.0f;
     for (int t = 0; t < taps; ++t) {
-        float2 g = gq[t];
+        // the tap's global-warp position, stored halved; doubling is exact
+        const float2 g = make_float2((float)(gh[t].x * 2.0), (float)(gh[t].y * 2.0));
         double qx = (double)g.x + ddx;
         double qy = (double)g.y + ddy;
         float tv;
@@ -218,6 +245,82 @@ __device__ __forceinline__ bool zncc_score(const PlaneRef &target, const float2 
     if (!(denominator > 1.0e-6f)) return false;
     score = clampf_r(covariance / denominator, -1.0f, 1.0f);
     return true;
+}
+
+// ---- fast path ---------------------------------------------------------------------
+// The reference computes each target sample coordinate as
+//   x = (f32)(((f64)g + d - 0.5) * 0.5)
+// with two f64 roundings. Multiplying by 0.5 is exact and commutes with
+// rounding, so the same bits come from x = (f32)((g/2 + d/2) - 0.25), where g/2
+// is stored per tap (TapHalf) and d/2 is computed once per hypothesis. The
+// coordinate is monotone in g, so the bounding box of the taps' g decides for
+// every tap at once whether all samples fall strictly inside [0, w-1) x [0, h-1);
+// inside, the reference's bounds checks and edge clamps cannot trigger and the
+// bilinear fetch reads a (L[x], L[x+1]) pair plane with two 8-byte loads.
+
+// Pair plane: pairs[y * w + x] = (L[y][x], L[y][min(x + 1, w - 1)]).
+__global__ void pair_plane_kernel(const float *__restrict__ plane, int width, int height, float2 *pairs) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)width * height) return;
+    int x = (int)(i % width);
+    pairs[i] = make_float2(plane[i], plane[x + 1 < width ? i + 1 : i]);
+}
+
+struct TargetRef {
+    PlaneRef plane;
+    const float2 *pairs;
+};
+
+// True when every tap at displacement (hdx, hdy) = (ddx/2, ddy/2) samples
+// strictly inside the plane.
+__device__ __forceinline__ bool taps_inside(const TapBox &box, double hdx, double hdy, int width, int height) {
+    float x0 = (float)((box.xmin + hdx) - 0.25), x1 = (float)((box.xmax + hdx) - 0.25);
+    float y0 = (float)((box.ymin + hdy) - 0.25), y1 = (float)((box.ymax + hdy) - 0.25);
+    // width, height < 2^22 (checked on the host), so inside also means < 2^22
+    return x0 >= 0.0f && y0 >= 0.0f && x1 < (float)(width - 1) && y1 < (float)(height - 1);
+}
+
+// warped_patch_zncc's hypothesis-dependent part for taps known to be inside
+// (see taps_inside). gh holds g/2 per tap.
+__device__ __forceinline__ float zncc_inside(const float2 *__restrict__ pairs, int width, const double2 *gh,
+                                             const float *w, const float *wr, const RefPatch &patch, int taps,
+                                             double hdx, double hdy, bool &ok) {
+    float st = 0.0f, stt = 0.0f, srt = 0.0f;
+#pragma unroll 9
+    for (int t = 0; t < taps; ++t) {
+        double2 g = gh[t];
+        float x = (float)((g.x + hdx) - 0.25);
+        float y = (float)((g.y + hdy) - 0.25);
+        int ix, iy;
+        float tx = floor_frac_small(x, ix), ty = floor_frac_small(y, iy);
+        const float2 *row = pairs + (size_t)iy * width + ix;
+        float2 a = __ldg(row), b = __ldg(row + width);
+        float top = a.x * (1.0f - tx) + a.y * tx;
+        float bottom = b.x * (1.0f - tx) + b.y * tx;
+        float tv = top * (1.0f - ty) + bottom * ty;
+        float wt = w[t] * tv;
+        st += wt;
+        stt += wt * tv;
+        srt += wr[t] * tv;
+    }
+    float covariance = srt - patch.sum_r * st / patch.count;
+    float target_energy = stt - st * st / patch.count;
+    float denominator = sqrtf(fmaxf(patch.ref_energy, 0.0f) * fmaxf(target_energy, 0.0f));
+    ok = denominator > 1.0e-6f;
+    return clampf_r(covariance / denominator, -1.0f, 1.0f);
+}
+
+// Either path, bit-identical to warped_patch_zncc: fast when the box is inside,
+// exact per-tap checks otherwise. gh: g/2 per tap.
+__device__ __forceinline__ bool zncc_any(const TargetRef &target, const double2 *gh, const TapBox &box, const float *w, const float *wr, const RefPatch &patch,
+                                         int taps, double ddx, double ddy, float &score) {
+    double hdx = ddx * 0.5, hdy = ddy * 0.5;
+    if (taps_inside(box, hdx, hdy, target.plane.width, target.plane.height)) {
+        bool ok;
+        score = zncc_inside(target.pairs, target.plane.width, gh, w, wr, patch, taps, hdx, hdy, ok);
+        return ok;
+    }
+    return zncc_score(target.plane, gh, w, wr, patch, taps, ddx, ddy, score);
 }
 
 // aggregate (depth.rs:1761-1770) over up to MAX_VIEWS scores (NaN = None).

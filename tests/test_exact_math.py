@@ -74,6 +74,16 @@ def test_exp_f64_plane_fit_spatial_values_and_specials(hc):
         assert np.float64(libm.exp(x)).view(np.uint64) == np.float64(hc.chiaro_hc_exp_f64(x)).view(np.uint64), x
 
 
+def test_magic_floor_is_exact_below_2_pow_22(hc):
+    # every float in [0, 2^22): the fast bilinear fetch relies on it
+    hi = _float_bits(4194304.0)
+    if EXHAUSTIVE:
+        assert hc.chiaro_hc_floor_mismatches(0, hi) == 0
+    else:
+        for e in range(0, hi, 0x00400000):
+            assert hc.chiaro_hc_floor_mismatches(e, min(hi, e + 262144)) == 0
+
+
 def test_plane_sample_matches_oracle(hc, oracle_lib):
     rng = np.random.default_rng(3)
     data = rng.uniform(0, 7, (37, 53)).astype(np.float32)
