@@ -4,7 +4,9 @@
 // classification (458-485), enforce_warp_consensus (582-618),
 // suppress_warp_boundaries (620-672) and the output warp (490-532).
 //
-// Decisions for every target run in one launch: eight lanes per (node, target).
+// Decisions for every target run in one launch: a warp per fine node stages
+// the reference patch once and spreads the (target, offset) and (target, shift)
+// correlations over its lanes.
 #pragma once
 
 #include "cost.cuh"
@@ -34,211 +36,253 @@ struct DecisionParams {
     Decisions out[MAX_VIEWS];  // per target (index into targets)
 };
 
-constexpr int DECISION_LANES = 8;     // lanes per (node, target)
-constexpr int DECISION_NODES = 32;    // nodes per CTA (256 threads)
+constexpr int DECISION_WARPS = 8;  // most nodes (warps) per CTA
 
-__host__ __device__ inline size_t decision_smem_bytes(int taps) {
-    // per node slot: r, w, wr, and the target's tap positions (g/2)
-    return (size_t)DECISION_NODES * (3 * taps * sizeof(float) + taps * sizeof(double2));
+// Per-warp shared memory of the decisions for V targets and T taps.
+struct DecisionSlot {
+    float *rr, *w, *wr;    // [T] reference patch: (w r) r, w, w r
+    double2 *gh;           // [V][T] tap positions g/2
+    TapBox *box;           // [V]
+    float *sc;             // [V][16]: 0-4 offsets, 5 baseline, 6-13 shifts, 14 best offset
+    float2 *pts;           // [V][16]
+    double2 *disp;         // [8 V] displacement of each listed correlation
+    unsigned short *list;  // [8 V] listed correlations
+    int *flags;            // [V]: nonzero once the target's refinement failed
+};
+
+__host__ __device__ inline size_t decision_slot_bytes(int V, int taps) {
+    return align16(3 * taps * sizeof(float)) + align16((size_t)V * taps * sizeof(double2)) +
+           align16(V * sizeof(TapBox)) + align16((size_t)V * 16 * sizeof(float)) +
+           align16((size_t)V * 16 * sizeof(float2)) + align16((size_t)8 * V * sizeof(double2)) +
+           align16((size_t)8 * V * sizeof(unsigned short)) + align16(V * sizeof(int));
 }
 
-// One CTA handles 32 nodes of one target (blockIdx.y); each node belongs to an
-// aligned group of 8 lanes inside one warp. Lanes 0-4 score the five
-// inverse-depth offsets and lane 5 the baseline; after lane 0 picks the best
-// offset, lanes 0-7 score the eight residual shifts; lane 0 classifies.
-__global__ void __launch_bounds__(DECISION_LANES * DECISION_NODES) target_decision_kernel(DecisionParams p) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ RefPatch patch[DECISION_NODES];
-    __shared__ float sc[DECISION_NODES][16];
-    __shared__ float2 pts[DECISION_NODES][16];
-    __shared__ int fail[DECISION_NODES], taps_ok[DECISION_NODES];
-    __shared__ TapBox boxes[DECISION_NODES];
-    const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
-    const int slot = threadIdx.x / DECISION_LANES, lane = threadIdx.x % DECISION_LANES;
-    const int node = blockIdx.x * DECISION_NODES + slot;
-    const int vi = blockIdx.y;
-    const int target = p.targets[vi];
-    const DevView &tv = p.views[target];
-    const DevView &rv = p.views[p.reference];
-    Decisions o = p.out[vi];
-    float *r = reinterpret_cast<float *>(smem_raw) + (size_t)slot * 3 * taps;
-    float *w = r + taps, *wr = w + taps;
-    double2 *gh = reinterpret_cast<double2 *>(smem_raw + (size_t)DECISION_NODES * 3 * taps * sizeof(float)) +
-                  (size_t)slot * taps;
+__device__ inline DecisionSlot carve_decision_slot(unsigned char *base, int V, int taps) {
+    DecisionSlot d;
+    size_t o = 0;
+    d.rr = reinterpret_cast<float *>(base);
+    d.w = d.rr + taps;
+    d.wr = d.w + taps;
+    o += align16(3 * taps * sizeof(float));
+    d.gh = reinterpret_cast<double2 *>(base + o);
+    o += align16((size_t)V * taps * sizeof(double2));
+    d.box = reinterpret_cast<TapBox *>(base + o);
+    o += align16(V * sizeof(TapBox));
+    d.sc = reinterpret_cast<float *>(base + o);
+    o += align16((size_t)V * 16 * sizeof(float));
+    d.pts = reinterpret_cast<float2 *>(base + o);
+    o += align16((size_t)V * 16 * sizeof(float2));
+    d.disp = reinterpret_cast<double2 *>(base + o);
+    o += align16((size_t)8 * V * sizeof(double2));
+    d.list = reinterpret_cast<unsigned short *>(base + o);
+    o += align16((size_t)8 * V * sizeof(unsigned short));
+    d.flags = reinterpret_cast<int *>(base + o);
+    return d;
+}
 
-    bool active = node < p.columns * p.rows;
-    const double cx = active ? (double)((node % p.columns) * p.step) : 0.0;
-    const double cy = active ? (double)((node / p.columns) * p.step) : 0.0;
-    float gqx = 0.0f, gqy = 0.0f;
-    if (active) {
-        bool defined = warp_map(tv.warp, (float)cx, (float)cy, gqx, gqy);
-        if (!defined || !p.field.has[node]) {
-            if (lane == 0) {
-                o.kind[node] = defined ? CHIARO_NW_GLOBAL : CHIARO_NW_UNDEFINED;
-                o.global[node] = make_float2(gqx, gqy);
-                o.point[node] = make_float2(gqx, gqy);
-                o.confidence[node] = 0.0f;
-                o.measured[node] = 0;
+__device__ __forceinline__ void write_decision(const Decisions &o, int node, uint8_t kind, float2 g, float2 pt,
+                                               float confidence, uint8_t measured) {
+    o.kind[node] = kind;
+    o.global[node] = g;
+    o.point[node] = pt;
+    o.confidence[node] = confidence;
+    o.measured[node] = measured;
+}
+
+// Append the items whose `listed` is set to d.list (in item order) with their
+// displacement; returns the new length on every lane. Every lane calls it.
+__device__ __forceinline__ int list_items(const DecisionSlot &d, int count, bool listed, int item, double ddx,
+                                          double ddy) {
+    const unsigned mask = __ballot_sync(0xffffffffu, listed);
+    if (listed) {
+        const int at = count + __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
+        d.list[at] = (unsigned short)item;
+        d.disp[at] = make_double2(ddx, ddy);
+    }
+    return count + __popc(mask);
+}
+
+// A warp per fine node, every target (depth.rs:420-485 with refine_one_view,
+// depth.rs:1634-1708). Each phase first settles which correlations run, lists
+// them, and runs the list from one call site, so the lanes stay converged.
+__global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(DecisionParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ RefPatch patches[DECISION_WARPS];
+    const unsigned full = 0xffffffffu;
+    const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int node = blockIdx.x * (blockDim.x >> 5) + slot;
+    if (node >= p.columns * p.rows) return;  // whole warp
+    const int V = p.n_targets;
+    const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
+    DecisionSlot d = carve_decision_slot(smem_raw + (size_t)slot * decision_slot_bytes(V, taps), V, taps);
+    RefPatch &patch = patches[slot];
+    const DevView &rv = p.views[p.reference];
+    const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
+    const bool has = p.field.has[node];
+    // the global warp at the node: Undefined, or Global without a depth (depth.rs:433-440);
+    // lane v holds target v's mapping
+    unsigned defined = 0u;
+    float2 gq = make_float2(0.0f, 0.0f);
+    if (lane < V) {
+        float gx = 0.0f, gy = 0.0f;
+        const bool ok = warp_map(p.views[p.targets[lane]].warp, (float)cx, (float)cy, gx, gy);
+        gq = make_float2(gx, gy);
+        if (ok) defined = 1u << lane;
+        if (!ok || !has)
+            write_decision(p.out[lane], node, ok ? CHIARO_NW_GLOBAL : CHIARO_NW_UNDEFINED, gq, gq, 0.0f, 0);
+        d.flags[lane] = 0;
+    }
+    defined = __reduce_or_sync(full, defined);
+    if (!has || !defined) return;  // whole warp
+    const unsigned undefined_taps = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, p.radius,
+                                                     p.spatial, d.rr, d.w, d.wr, d.gh, d.box, patch);
+    const bool patch_ok = patch.ok;
+    const D3 origin = camera_origin(rv.cam);
+    const double shared_inverse = 1.0 / p.field.depth[node];
+    const double min_inverse = 1.0 / p.far_depth, max_inverse = 1.0 / p.near_depth;
+    // phase 1: per target, five inverse-depth offsets (k < 5) and the baseline (k = 5)
+    int listed = 0;
+    for (int base = 0; base < 6 * V; base += 32) {
+        const int item = base + lane;
+        const int v = item / 6, k = item - v * 6;
+        const int vs = v < V ? v : 0;
+        const float2 gq_c = make_float2(__shfl_sync(full, gq.x, vs), __shfl_sync(full, gq.y, vs));
+        bool zncc = false;
+        double ddx = 0.0, ddy = 0.0;
+        if (item < 6 * V && ((defined >> v) & 1u)) {
+            const DevView &tv = p.views[p.targets[v]];
+            const bool zncc_ok = patch_ok && !((undefined_taps >> v) & 1u);
+            if (k < 5) {
+                ViewGeom g;
+                geom_from_rec(p.geometry[(size_t)node * V + v], origin, g);
+                const double label_offset = -1.0 + 0.5 * k;
+                double inv = clampd_r(shared_inverse + label_offset * p.inverse_step, min_inverse, max_inverse);
+                bool ok = g.ray_ok;
+                double qx = 0.0, qy = 0.0;
+                if (ok) ok = project(tv.cam, along({g.ox, g.oy, g.oz}, {g.dx, g.dy, g.dz}, 1.0 / inv), qx, qy);
+                if (ok) ok = isfinite(qx) && isfinite(qy);
+                const float2 point = make_float2((float)qx, (float)qy);
+                if (ok) {
+                    ddx = (double)(point.x - gq_c.x);
+                    ddy = (double)(point.y - gq_c.y);
+                    ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && zncc_ok;
+                }
+                if (!ok) atomicOr(&d.flags[v], 1);
+                d.sc[v * 16 + k] = 0.0f;
+                d.pts[v * 16 + k] = point;
+                zncc = ok;
+            } else {
+                d.sc[v * 16 + 5] = NAN;
+                zncc = zncc_ok;
             }
-            active = false;
         }
-    }
-    const float2 gq_c = make_float2(gqx, gqy);
-    // reference patch and tap positions of this node (8 lanes)
-    float centre = 0.0f;
-    bool centre_ok = false;
-    if (active) {
-        centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
-        if (lane == 0) {
-            patch[slot].ok = centre_ok;
-            patch[slot].centre = centre;
-            taps_ok[slot] = 1;
-            fail[slot] = 0;
-        }
+        listed = list_items(d, listed, zncc, item, ddx, ddy);
     }
     __syncwarp();
-    if (active) {
-        for (int t = lane; t < taps; t += DECISION_LANES) {
-            int dx, dy;
-            tap_offset(t, p.radius, dx, dy);
-            double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
-            float value = 0.0f;
-            if (!plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value)) patch[slot].ok = 0;
-            float weight = p.spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
-            r[t] = value;
-            w[t] = weight;
-            wr[t] = weight * value;
-            float qx = 0.0f, qy = 0.0f;
-            if (!warp_map(tv.warp, (float)px, (float)py, qx, qy)) taps_ok[slot] = 0;
-            gh[t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
-        }
+    for (int j = lane; j < listed; j += 32) {
+        const int item = d.list[j];
+        const int v = item / 6, k = item - v * 6;
+        const DevView &tv = p.views[p.targets[v]];
+        const double2 dd = d.disp[j];
+        float score;
+        if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
+                     score))
+            d.sc[v * 16 + k] = score;
+        else if (k < 5)
+            atomicOr(&d.flags[v], 1);
     }
     __syncwarp();
-    if (active && lane == 3) {  // box of this node's taps (one lane of the group)
-        TapBox b{gh[0].x, gh[0].x, gh[0].y, gh[0].y};
-        for (int t = 1; t < taps; ++t) {
-            b.xmin = fmin(b.xmin, gh[t].x);
-            b.xmax = fmax(b.xmax, gh[t].x);
-            b.ymin = fmin(b.ymin, gh[t].y);
-            b.ymax = fmax(b.ymax, gh[t].y);
-        }
-        boxes[slot] = b;
-    }
-    if (active && lane < 3) {  // the three sequential reference sums
-        float sum = 0.0f;
-        if (lane == 0)
-            for (int t = 0; t < taps; ++t) sum += w[t];
-        else if (lane == 1)
-            for (int t = 0; t < taps; ++t) sum += wr[t];
-        else
-            for (int t = 0; t < taps; ++t) sum += wr[t] * r[t];
-        if (lane == 0) patch[slot].count = sum;
-        if (lane == 1) patch[slot].sum_r = sum;
-        if (lane == 2) patch[slot].sum_rr = sum;
-    }
-    __syncwarp();
-    if (active && lane == 0)
-        patch[slot].ref_energy = patch[slot].sum_rr - patch[slot].sum_r * patch[slot].sum_r / patch[slot].count;
-    __syncwarp();
-    ViewGeom g;
-    if (active) geom_from_rec(p.geometry[(size_t)node * p.n_targets + vi], camera_origin(rv.cam), g);
-    const bool zncc_ok = active && patch[slot].ok && taps_ok[slot];
-    const TargetRef target_ref{tv.luma, tv.pairs};
-    double shared_inverse = 0.0, min_inverse = 1.0 / p.far_depth, max_inverse = 1.0 / p.near_depth;
-    if (active) shared_inverse = 1.0 / p.field.depth[node];
-    // phase 1: five inverse-depth offsets and the baseline
-    if (active && lane < 5) {
-        const double label_offset = -1.0 + 0.5 * lane;
-        double inv = clampd_r(shared_inverse + label_offset * p.inverse_step, min_inverse, max_inverse);
-        bool ok = g.ray_ok;
-        double qx = 0.0, qy = 0.0;
-        if (ok) ok = project(tv.cam, along({g.ox, g.oy, g.oz}, {g.dx, g.dy, g.dz}, 1.0 / inv), qx, qy);
-        if (ok) ok = isfinite(qx) && isfinite(qy);
-        float2 point = make_float2((float)qx, (float)qy);
-        float score = 0.0f;
-        if (ok) {
-            double ddx = (double)(point.x - gq_c.x), ddy = (double)(point.y - gq_c.y);
-            ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && zncc_ok &&
-                 zncc_any(target_ref, gh, boxes[slot], w, wr, patch[slot], taps, ddx, ddy, score);
-        }
-        if (!ok) atomicOr(&fail[slot], 1);
-        sc[slot][lane] = score;
-        pts[slot][lane] = point;
-    } else if (active && lane == 5) {
-        float score = NAN, sv;
-        if (zncc_ok && zncc_any(target_ref, gh, boxes[slot], w, wr, patch[slot], taps, 0.0, 0.0, sv)) score = sv;
-        sc[slot][5] = score;
-    }
-    __syncwarp();
-    if (active && lane == 0 && !fail[slot]) {  // best offset, in order, strict improvement
+    // best offset per target: in order, strict improvement
+    const unsigned failed = __ballot_sync(full, lane < V && d.flags[lane < V ? lane : 0]);
+    if (lane < V && ((defined >> lane) & 1u) && !((failed >> lane) & 1u)) {
+        float *sc = d.sc + lane * 16;
+        float2 *pts = d.pts + lane * 16;
         float best_objective = 0.0f;
         for (int k = 0; k < 5; ++k) {
-            float objective = sc[slot][k] - (float)fabs(-1.0 + 0.5 * k) * 0.002f;
+            float objective = sc[k] - (float)fabs(-1.0 + 0.5 * k) * 0.002f;
             if (k == 0 || objective > best_objective) {
                 best_objective = objective;
-                sc[slot][14] = sc[slot][k];
-                pts[slot][14] = pts[slot][k];
+                sc[14] = sc[k];
+                pts[14] = pts[k];
             }
         }
     }
     __syncwarp();
-    // phase 2: eight residual shifts (dy outer, dx inner, centre skipped)
-    if (active && !fail[slot]) {
-        int k = lane < 4 ? lane : lane + 1;
-        float dx = -1.5f + 1.5f * (float)(k % 3), dy = -1.5f + 1.5f * (float)(k / 3);
-        float2 depth_point = pts[slot][14];
-        float2 point = make_float2(depth_point.x + dx, depth_point.y + dy);
-        double ddx = (double)(point.x - gq_c.x), ddy = (double)(point.y - gq_c.y);
-        float score = 0.0f;
-        bool ok = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && zncc_ok &&
-                  zncc_any(target_ref, gh, boxes[slot], w, wr, patch[slot], taps, ddx, ddy, score);
-        if (!ok) atomicOr(&fail[slot], 1);
-        sc[slot][6 + lane] = score;
-        pts[slot][6 + lane] = point;
+    // phase 2: per target, eight residual shifts (dy outer, dx inner, centre skipped)
+    listed = 0;
+    for (int base = 0; base < 8 * V; base += 32) {
+        const int item = base + lane;
+        const int v = item >> 3, j = item & 7;
+        const int vs = v < V ? v : 0;
+        const float2 gq_c = make_float2(__shfl_sync(full, gq.x, vs), __shfl_sync(full, gq.y, vs));
+        bool zncc = false;
+        double ddx = 0.0, ddy = 0.0;
+        if (item < 8 * V && ((defined >> v) & 1u) && !((failed >> v) & 1u)) {
+            const int k = j < 4 ? j : j + 1;
+            const float dx = -1.5f + 1.5f * (float)(k % 3), dy = -1.5f + 1.5f * (float)(k / 3);
+            const float2 depth_point = d.pts[v * 16 + 14];
+            const float2 point = make_float2(depth_point.x + dx, depth_point.y + dy);
+            ddx = (double)(point.x - gq_c.x);
+            ddy = (double)(point.y - gq_c.y);
+            zncc = !(fabs(ddx) > 128.0 || fabs(ddy) > 128.0) && patch_ok && !((undefined_taps >> v) & 1u);
+            if (!zncc) atomicOr(&d.flags[v], 1);
+            d.sc[v * 16 + 6 + j] = 0.0f;
+            d.pts[v * 16 + 6 + j] = point;
+        }
+        listed = list_items(d, listed, zncc, item, ddx, ddy);
     }
     __syncwarp();
-    if (!active || lane != 0) return;
-    const bool selected = !fail[slot];
+    for (int j = lane; j < listed; j += 32) {
+        const int item = d.list[j];
+        const int v = item >> 3;
+        const DevView &tv = p.views[p.targets[v]];
+        const double2 dd = d.disp[j];
+        float score;
+        if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
+                     score))
+            d.sc[v * 16 + 6 + (item & 7)] = score;
+        else
+            atomicOr(&d.flags[v], 1);
+    }
+    __syncwarp();
+    // classification (depth.rs:458-485), lane v for target v
+    if (lane >= V || !((defined >> lane) & 1u)) return;
+    const Decisions o = p.out[lane];
+    const float *sc = d.sc + lane * 16;
+    const float2 *pts = d.pts + lane * 16;
+    const bool selected = !d.flags[lane];
     float sel_score = 0.0f;
     float2 sel_point = make_float2(0.0f, 0.0f);
     if (selected) {
-        float b0 = sc[slot][14], b1 = sc[slot][14];
-        float2 b2 = pts[slot][14];
+        float b0 = sc[14], b1 = sc[14];
+        float2 b2 = pts[14];
         for (int j = 0; j < 8; ++j) {
             int k = j < 4 ? j : j + 1;
             float dx = -1.5f + 1.5f * (float)(k % 3), dy = -1.5f + 1.5f * (float)(k / 3);
-            float objective = sc[slot][6 + j] - (dx * dx + dy * dy) * 0.002f;
+            float objective = sc[6 + j] - (dx * dx + dy * dy) * 0.002f;
             if (objective > b0) {
                 b0 = objective;
-                b1 = sc[slot][6 + j];
-                b2 = pts[slot][6 + j];
+                b1 = sc[6 + j];
+                b2 = pts[6 + j];
             }
         }
         sel_score = b1;
         sel_point = b2;
     }
-    const float baseline = sc[slot][5];
+    const float baseline = sc[5];
     const bool base_ok = baseline == baseline;
     const bool regularized = p.field.regularized[node] != 0;
     const float node_confidence = p.field.confidence[node];
     const bool supported = selected && sel_score >= p.minimum_score && (!base_ok || sel_score + 0.01f >= baseline);
     const bool contradicted = selected && base_ok && sel_score + 0.12f < baseline;
-    o.global[node] = gq_c;
-    o.measured[node] = regularized ? 0 : 1;
-    if (contradicted) {
-        o.kind[node] = CHIARO_NW_OCCLUDED;
-        o.point[node] = gq_c;
-        o.confidence[node] = 0.0f;
-    } else if (supported) {
-        o.kind[node] = CHIARO_NW_REFINED;
-        o.point[node] = sel_point;
-        o.confidence[node] = regularized ? node_confidence * 0.6f : 0.5f + 0.5f * node_confidence;
-    } else {
-        o.kind[node] = CHIARO_NW_GLOBAL;
-        o.point[node] = gq_c;
-        o.confidence[node] = 0.0f;
-        o.measured[node] = 0;
-    }
+    const uint8_t measured = regularized ? 0 : 1;
+    if (contradicted)
+        write_decision(o, node, CHIARO_NW_OCCLUDED, gq, gq, 0.0f, measured);
+    else if (supported)
+        write_decision(o, node, CHIARO_NW_REFINED, gq, sel_point,
+                       regularized ? node_confidence * 0.6f : 0.5f + 0.5f * node_confidence, measured);
+    else
+        write_decision(o, node, CHIARO_NW_GLOBAL, gq, gq, 0.0f, 0);
 }
 
 // warp_decisions_agree (depth.rs:682-712)

@@ -2,11 +2,13 @@
 // with nearest_coarse_depth (1062-1076), direct_depth_candidates (1078-1107),
 // select_direct_depth (1109-1165) and best_depth_candidate (1167-1185).
 //
-// A warp per fine-grid node, several nodes per CTA. The candidate list is built
-// serially (its deduplication depends on the previous entry); the baseline and
-// candidate scores are independent (candidate, view) ZNCC items spread over the
-// warp; the selection follows the reference. Nodes that need the wide-radius
-// retry go to a list that a second kernel processes with its larger patch.
+// A warp per fine-grid node, as many nodes per CTA as keep the most warps
+// resident. The thirteen seeded candidates are computed one per lane and
+// deduplicated by a uniform scan; the baseline and candidate scores are
+// independent (candidate, view) ZNCC items, listed fast-path first and spread
+// over the warp; the selection replaces the reference's sort by warp
+// reductions. Nodes that need the wide-radius retry go to a list that a second
+// kernel processes with its larger patch.
 #pragma once
 
 #include "cost.cuh"
@@ -15,44 +17,52 @@
 namespace chiaro {
 
 constexpr int MAX_DIRECT_CANDIDATES = 32;
+constexpr int KEY_NONE = -2147483647 - 1;  // below every total_key of a non-NaN float
 
-// select_direct_depth on (depth, score) pairs; score NaN = None. One thread.
-__device__ inline bool select_direct(const double *depths, const float *scores, int n, bool has_baseline,
-                                     float baseline, bool seeded, double far_depth, double near_depth,
-                                     float minimum_score, float minimum_margin, float minimum_improvement,
-                                     double &out_depth, float &out_confidence, float &out_improvement) {
+// select_direct_depth (depth.rs:1109-1165) and best_depth_candidate
+// (depth.rs:1167-1185) over (depth, score) pairs, score NaN = None, computed by
+// a whole warp: lane c < n holds candidate c's objective. The reference sorts
+// the objectives stably in descending total order; its head is the first
+// maximum, and its first entry more than one index away from the head has the
+// largest objective among those entries, so two warp max-reductions replace
+// the sort. best_depth_candidate keeps the last maximum (`best_last`, -1 for
+// None). Every lane returns the same result.
+__device__ inline bool warp_select_direct(const double *depths, const float *scores, int n, bool has_baseline,
+                                          float baseline, bool seeded, double far_depth, double near_depth,
+                                          float minimum_score, float minimum_margin, float minimum_improvement,
+                                          double &out_depth, float &out_confidence, float &out_improvement,
+                                          int &best_last) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     double far_inverse = 1.0 / far_depth;
     double inverse_range = 1.0 / near_depth - far_inverse;
-    int idx[MAX_DIRECT_CANDIDATES + 1];
-    float obj[MAX_DIRECT_CANDIDATES + 1];
-    int m = 0;
-    for (int i = 0; i < n; ++i) {
-        if (scores[i] != scores[i]) continue;
-        double near_fraction = clampd_r((1.0 / depths[i] - far_inverse) / inverse_range, 0.0, 1.0);
-        float objective = scores[i] - NEAR_DEPTH_PRIOR * (float)near_fraction;
-        // stable insertion, descending by total order
-        int j = m - 1;
-        while (j >= 0 && total_key(obj[j]) < total_key(objective)) {
-            idx[j + 1] = idx[j];
-            obj[j + 1] = obj[j];
-            --j;
+    bool valid = false;
+    float objective = 0.0f;
+    if (lane < n) {
+        float s = scores[lane];
+        valid = !(s != s);
+        if (valid) {
+            double near_fraction = clampd_r((1.0 / depths[lane] - far_inverse) / inverse_range, 0.0, 1.0);
+            objective = s - NEAR_DEPTH_PRIOR * (float)near_fraction;
         }
-        idx[j + 1] = i;
-        obj[j + 1] = objective;
-        ++m;
     }
-    if (m == 0) return false;
-    int best = idx[0];
-    float best_objective = obj[0];
-    float score = scores[best];
+    best_last = -1;
+    if (!__ballot_sync(full, valid)) return false;
+    const int key = valid ? total_key(objective) : KEY_NONE;
+    const int top = __reduce_max_sync(full, key);
+    const unsigned at_top = __ballot_sync(full, valid && key == top);
+    const int best = __ffs(at_top) - 1;
+    best_last = 31 - __clz(at_top);
+    const float best_objective = __shfl_sync(full, objective, best);
+    const bool away = valid && (lane - best > 1 || lane - best < -1);
+    const unsigned away_mask = __ballot_sync(full, away);
     float competing = best_objective;
-    for (int k = 0; k < m; ++k) {
-        int d = idx[k] - best;
-        if (d > 1 || d < -1) {
-            competing = obj[k];
-            break;
-        }
+    if (away_mask) {
+        const int away_top = __reduce_max_sync(full, away ? key : KEY_NONE);
+        const int c = __ffs(__ballot_sync(full, away && key == away_top)) - 1;
+        competing = __shfl_sync(full, objective, c);
     }
+    float score = scores[best];
     float margin = fmaxf(best_objective - competing, 0.0f);
     float improvement = has_baseline ? score - baseline : 0.0f;
     float score_floor = fmaxf(minimum_score - 0.03f, MINIMUM_REGULARIZED_SCORE);
@@ -67,25 +77,6 @@ __device__ inline bool select_direct(const double *depths, const float *scores, 
     out_confidence = clampf_r(0.30f + 0.45f * score_confidence + 0.25f * margin_confidence, 0.0f, 1.0f);
     out_improvement = improvement;
     return true;
-}
-
-// best_depth_candidate: last maximum of the objective; -1 for None.
-__device__ inline int best_candidate(const double *depths, const float *scores, int n, double far_depth,
-                                     double near_depth) {
-    double far_inverse = 1.0 / far_depth;
-    double inverse_range = 1.0 / near_depth - far_inverse;
-    int best = -1;
-    float best_objective = 0.0f;
-    for (int i = 0; i < n; ++i) {
-        if (scores[i] != scores[i]) continue;
-        double near_fraction = clampd_r((1.0 / depths[i] - far_inverse) / inverse_range, 0.0, 1.0);
-        float objective = scores[i] - NEAR_DEPTH_PRIOR * (float)near_fraction;
-        if (best < 0 || !(total_key(objective) < total_key(best_objective))) {
-            best = i;
-            best_objective = objective;
-        }
-    }
-    return best;
 }
 
 // ---- warp-per-node direct pass ---------------------------------------------------
@@ -113,29 +104,34 @@ struct DirectParams {
 
 // Per-warp shared memory of the direct pass for V targets and T taps.
 struct DirectSlot {
-    float *r, *w, *wr;   // [T]
-    double2 *gh;         // [V][T] g/2 (fast path)
-    TapBox *box;         // [V]
-    double *cand;        // [32]
-    float *items;        // [33][V]
-    float *agg;          // [33]: [0] baseline, [1 + c] candidates
+    float *rr, *w, *wr;    // [T]: (w r) r, w, w r
+    ViewGeom *geom;        // [V]
+    double2 *gh;           // [V][T] g/2 (fast path)
+    TapBox *box;           // [V]
+    double *cand;          // [32]
+    float *items;          // [33][V]
+    float *agg;            // [33]: [0] baseline, [1 + c] candidates
+    unsigned short *list;  // [33][V] scored items: fast path from the front, exact path from the back
 };
 
 __host__ __device__ inline size_t direct_slot_bytes(int V, int taps) {
-    return align16(3 * taps * sizeof(float)) + align16((size_t)V * taps * sizeof(double2)) +
-           align16(V * sizeof(TapBox)) +
+    return align16(3 * taps * sizeof(float)) + align16(V * sizeof(ViewGeom)) +
+           align16((size_t)V * taps * sizeof(double2)) + align16(V * sizeof(TapBox)) +
            align16(MAX_DIRECT_CANDIDATES * sizeof(double)) +
            align16((size_t)(MAX_DIRECT_CANDIDATES + 1) * V * sizeof(float)) +
-           align16((MAX_DIRECT_CANDIDATES + 1) * sizeof(float));
+           align16((MAX_DIRECT_CANDIDATES + 1) * sizeof(float)) +
+           align16((size_t)(MAX_DIRECT_CANDIDATES + 1) * V * sizeof(unsigned short));
 }
 
 __device__ inline DirectSlot carve_direct_slot(unsigned char *base, int V, int taps) {
     DirectSlot d;
     size_t o = 0;
-    d.r = reinterpret_cast<float *>(base);
-    d.w = d.r + taps;
+    d.rr = reinterpret_cast<float *>(base);
+    d.w = d.rr + taps;
     d.wr = d.w + taps;
     o += align16(3 * taps * sizeof(float));
+    d.geom = reinterpret_cast<ViewGeom *>(base + o);
+    o += align16(V * sizeof(ViewGeom));
     d.gh = reinterpret_cast<double2 *>(base + o);
     o += align16((size_t)V * taps * sizeof(double2));
     d.box = reinterpret_cast<TapBox *>(base + o);
@@ -145,111 +141,118 @@ __device__ inline DirectSlot carve_direct_slot(unsigned char *base, int V, int t
     d.items = reinterpret_cast<float *>(base + o);
     o += align16((size_t)(MAX_DIRECT_CANDIDATES + 1) * V * sizeof(float));
     d.agg = reinterpret_cast<float *>(base + o);
+    o += align16((MAX_DIRECT_CANDIDATES + 1) * sizeof(float));
+    d.list = reinterpret_cast<unsigned short *>(base + o);
     return d;
 }
 
 // nearest_coarse_depth (depth.rs:1062-1076) and direct_depth_candidates
-// (depth.rs:1078-1107); returns the candidate count, sets *seeded.
-__device__ inline int direct_candidates(const DirectParams &p, double cx, double cy, double *cand, int *seeded) {
+// (depth.rs:1078-1107) by a whole warp; returns the candidate count (every
+// lane) and sets `seeded`. Lane k < 13 computes offset k - 6's depth and its
+// inverse; the deduplication against the last kept entry is a uniform scan of
+// those inverses (1 / cand[n - 1] is the kept entry's inverse, computed the
+// same way), then the kept depths are written in order.
+__device__ inline int warp_direct_candidates(const DirectParams &p, double cx, double cy, double *cand,
+                                             int &seeded) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     int cc = sat_index_d(clampd_r(round(cx / (double)p.coarse_step), 0.0, (double)(p.coarse_columns - 1)),
                          p.coarse_columns - 1);
     int cr = sat_index_d(clampd_r(round(cy / (double)p.coarse_step), 0.0, (double)(p.coarse_rows - 1)),
                          p.coarse_rows - 1);
     int ci = cr * p.coarse_columns + cc;
-    *seeded = p.coarse.has[ci];
-    if (!*seeded) {
-        for (int i = 0; i < 32; ++i) cand[i] = p.unseeded[i];
+    seeded = p.coarse.has[ci];
+    if (!seeded) {
+        cand[lane] = p.unseeded[lane];  // 32 candidates
         return 32;
     }
     double seed = p.coarse.depth[ci];
     double far_inverse = 1.0 / p.far_depth, near_inverse = 1.0 / p.near_depth;
-    int n = 0;
-    for (int offset = -6; offset <= 6; ++offset) {
-        double inv = clampd_r(1.0 / seed + (double)offset * p.inverse_step * 0.5, far_inverse, near_inverse);
-        double depth = 1.0 / inv;
-        if (n == 0 || fabs(1.0 / cand[n - 1] - 1.0 / depth) > p.inverse_step * 0.1) cand[n++] = depth;
+    double depth = 0.0, inverse = 0.0;
+    if (lane < 13) {
+        double inv = clampd_r(1.0 / seed + (double)(lane - 6) * p.inverse_step * 0.5, far_inverse, near_inverse);
+        depth = 1.0 / inv;
+        inverse = 1.0 / depth;
     }
-    return n;
-}
-
-// Warp-cooperative: reference patch (r, w, wr and the sums) and every target's
-// tap positions for one node at `radius`; geometry from the records.
-__device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot &d, RefPatch &patch, ViewGeom *geom,
-                                       double cx, double cy, int radius, const float *spatial, const GeomRec *recs) {
-    const int lane = threadIdx.x & 31;
-    const int taps = (2 * radius + 1) * (2 * radius + 1);
-    const int V = p.n_targets;
-    const DevView &rv = p.views[p.reference];
-    float centre = 0.0f;
-    bool centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
-    if (lane == 0) {
-        patch.ok = centre_ok;
-        patch.centre = centre;
-    }
-    if (lane < V) {
-        if (recs) geom_from_rec(recs[lane], camera_origin(rv.cam), geom[lane]);
-        geom[lane].taps_ok = 1;
-    }
-    __syncwarp();
-    for (int t = lane; t < taps; t += 32) {
-        int dx, dy;
-        tap_offset(t, radius, dx, dy);
-        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
-        float value = 0.0f;
-        if (!plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value)) patch.ok = 0;
-        float weight = spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
-        d.r[t] = value;
-        d.w[t] = weight;
-        d.wr[t] = weight * value;
-        for (int v = 0; v < V; ++v) {
-            float qx = 0.0f, qy = 0.0f;
-            if (!warp_map(p.views[p.targets[v]].warp, (float)px, (float)py, qx, qy)) geom[v].taps_ok = 0;
-            d.gh[v * taps + t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
+    unsigned kept = 1u;
+    double last = __shfl_sync(full, inverse, 0);
+    for (int k = 1; k < 13; ++k) {
+        double current = __shfl_sync(full, inverse, k);
+        if (fabs(last - current) > p.inverse_step * 0.1) {
+            kept |= 1u << k;
+            last = current;
         }
     }
-    __syncwarp();
-    for (int v = 0; v < V; ++v) {
-        TapBox b = warp_tap_box(d.gh + v * taps, taps);
-        if (lane == 0) d.box[v] = b;
+    if (lane < 13 && ((kept >> lane) & 1u)) cand[__popc(kept & ((1u << lane) - 1u))] = depth;
+    return __popc(kept);
+}
+
+// Warp-cooperative: reference patch and every target's tap positions for one
+// node at `radius` (warp_stage_patch); geometry from the records.
+__device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot &d, RefPatch &patch, double cx,
+                                       double cy, int radius, const float *spatial, const GeomRec *recs) {
+    const int lane = threadIdx.x & 31;
+    const int V = p.n_targets;
+    const unsigned undefined = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, radius, spatial, d.rr,
+                                                d.w, d.wr, d.gh, d.box, patch);
+    if (lane < V) {
+        geom_from_rec(recs[lane], camera_origin(p.views[p.reference].cam), d.geom[lane]);
+        d.geom[lane].taps_ok = ((undefined >> lane) & 1u) ? 0 : 1;
     }
-    if (lane < 3) {
-        float sum = 0.0f;
-        if (lane == 0)
-            for (int t = 0; t < taps; ++t) sum += d.w[t];
-        else if (lane == 1)
-            for (int t = 0; t < taps; ++t) sum += d.wr[t];
-        else
-            for (int t = 0; t < taps; ++t) sum += d.wr[t] * d.r[t];
-        if (lane == 0) patch.count = sum;
-        if (lane == 1) patch.sum_r = sum;
-        if (lane == 2) patch.sum_rr = sum;
-    }
-    __syncwarp();
-    if (lane == 0) patch.ref_energy = patch.sum_rr - patch.sum_r * patch.sum_r / patch.count;
     __syncwarp();
 }
 
 // Warp-cooperative scores of the baseline and candidates cand[0..n) over all
-// targets, aggregated into d.agg[0..n]. NaN = None.
+// targets, aggregated into d.agg[0..n]. NaN = None. Item i is (candidate
+// i / V - 1, target i % V), candidate -1 being the baseline. A first sweep
+// settles which items reach the correlation and whether their taps are all
+// inside (the fast path), and lists them fast-first; the correlations then run
+// over that list, so lanes idle only in the last round.
 __device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlot &d, const RefPatch &patch,
-                                          const ViewGeom *geom, const double *cand, int n, int radius) {
+                                          const double *cand, int n, int radius) {
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
     const int V = p.n_targets;
     const int taps = (2 * radius + 1) * (2 * radius + 1);
-    for (int item = lane; item < (n + 1) * V; item += 32) {
-        int c = item / V - 1, v = item % V;
-        float score = NAN;
-        const ViewGeom &g = geom[v];
-        double ddx = 0.0, ddy = 0.0;
-        bool ok = g.gc_ok;
-        if (ok && c >= 0) ok = depth_delta(p.views[p.targets[v]].cam, g, cand[c], ddx, ddy);
-        if (ok && patch.ok && g.taps_ok) {
-            const DevView &tv = p.views[p.targets[v]];
-            float sc;
-            if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, ddx, ddy,
-                         sc))
-                score = sc;
+    const int total = (n + 1) * V;
+    const ViewGeom *geom = d.geom;
+    int n_fast = 0, n_exact = 0;
+    for (int base = 0; base < total; base += 32) {
+        const int item = base + lane;
+        bool scored = false, fast = false;
+        if (item < total) {
+            const int c = item / V - 1, v = item - (item / V) * V;
+            const ViewGeom &g = geom[v];
+            double ddx = 0.0, ddy = 0.0;
+            bool ok = g.gc_ok;
+            if (ok && c >= 0) ok = depth_delta(p.views[p.targets[v]].cam, g, cand[c], ddx, ddy);
+            scored = ok && patch.ok && g.taps_ok;
+            if (scored) {
+                const PlaneRef &plane = p.views[p.targets[v]].luma;
+                fast = taps_inside(d.box[v], ddx * 0.5, ddy * 0.5, plane.width, plane.height);
+            } else {
+                d.items[item] = NAN;
+            }
         }
+        const unsigned fast_mask = __ballot_sync(full, scored && fast);
+        const unsigned exact_mask = __ballot_sync(full, scored && !fast);
+        if (scored && fast) d.list[n_fast + __popc(fast_mask & below)] = (unsigned short)item;
+        if (scored && !fast) d.list[total - 1 - (n_exact + __popc(exact_mask & below))] = (unsigned short)item;
+        n_fast += __popc(fast_mask);
+        n_exact += __popc(exact_mask);
+    }
+    __syncwarp();
+    const int listed = n_fast + n_exact;
+    for (int j = lane; j < listed; j += 32) {
+        const int item = j < n_fast ? d.list[j] : d.list[total - 1 - (j - n_fast)];
+        const int c = item / V - 1, v = item - (item / V) * V;
+        const DevView &tv = p.views[p.targets[v]];
+        double ddx = 0.0, ddy = 0.0;
+        if (c >= 0) depth_delta(tv.cam, geom[v], cand[c], ddx, ddy);
+        float score = NAN, sc;
+        if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, ddx, ddy, sc))
+            score = sc;
         d.items[item] = score;
     }
     __syncwarp();
@@ -262,11 +265,10 @@ __device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlo
     __syncwarp();
 }
 
+// A warp per fine node; the CTA holds nodes_per_cta nodes.
 __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patches[8];
-    __shared__ ViewGeom geoms[8][MAX_VIEWS];
-    __shared__ int n_cand[8], seeded_s[8];
     const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int node = blockIdx.x * p.nodes_per_cta + slot;
     if (slot >= p.nodes_per_cta || node >= p.columns * p.rows) return;  // whole warps
@@ -275,18 +277,20 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
     DirectSlot d = carve_direct_slot(smem_raw + (size_t)slot * direct_slot_bytes(V, taps), V, taps);
     RefPatch &patch = patches[slot];
     const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
-    if (lane == 0) n_cand[slot] = direct_candidates(p, cx, cy, d.cand, &seeded_s[slot]);
-    warp_stage_node(p, d, patch, geoms[slot], cx, cy, p.radius, p.spatial, p.geometry + (size_t)node * V);
-    const int n = n_cand[slot];
-    warp_direct_scores(p, d, patch, geoms[slot], d.cand, n, p.radius);
-    if (lane != 0) return;
-    bool tested = d.agg[0] == d.agg[0];
-    for (int c = 0; c < n; ++c) tested |= d.agg[1 + c] == d.agg[1 + c];
+    int seeded;
+    const int n = warp_direct_candidates(p, cx, cy, d.cand, seeded);
+    warp_stage_node(p, d, patch, cx, cy, p.radius, p.spatial, p.geometry + (size_t)node * V);
+    warp_direct_scores(p, d, patch, d.cand, n, p.radius);
+    bool seen = false;
+    for (int c = lane; c <= n; c += 32) seen |= d.agg[c] == d.agg[c];
+    const bool tested = __any_sync(0xffffffffu, seen);
     double depth = 0.0;
     float confidence = 0.0f, improvement = 0.0f;
-    bool has = select_direct(d.cand, d.agg + 1, n, d.agg[0] == d.agg[0], d.agg[0], seeded_s[slot], p.far_depth,
-                             p.near_depth, p.minimum_score, p.minimum_margin, p.minimum_improvement, depth,
-                             confidence, improvement);
+    int best;
+    const bool has = warp_select_direct(d.cand, d.agg + 1, n, d.agg[0] == d.agg[0], d.agg[0], seeded, p.far_depth,
+                                        p.near_depth, p.minimum_score, p.minimum_margin, p.minimum_improvement,
+                                        depth, confidence, improvement, best);
+    if (lane != 0) return;
     p.tested[node] = tested;
     p.guidance[node] = patch.centre;  // reference_guidance (depth.rs:1824-1832)
     p.out.has[node] = has;
@@ -294,14 +298,11 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
     p.out.confidence[node] = has ? confidence : 0.0f;
     p.out.improvement[node] = has ? improvement : 0.0f;
     p.out.regularized[node] = 0;
-    if (!has) {
-        int best = best_candidate(d.cand, d.agg + 1, n, p.far_depth, p.near_depth);
-        if (best >= 0 && d.agg[1 + best] == d.agg[1 + best] && d.agg[1 + best] >= MINIMUM_REGULARIZED_SCORE) {
-            int first = best >= 3 ? best - 3 : 0;
-            int last = best + 3 < n - 1 ? best + 3 : n - 1;
-            int k = atomicAdd(p.wide_count, 1);
-            p.wide_list[k] = make_int4(node, first, last, seeded_s[slot]);
-        }
+    if (!has && best >= 0 && d.agg[1 + best] == d.agg[1 + best] && d.agg[1 + best] >= MINIMUM_REGULARIZED_SCORE) {
+        int first = best >= 3 ? best - 3 : 0;
+        int last = best + 3 < n - 1 ? best + 3 : n - 1;
+        int k = atomicAdd(p.wide_count, 1);
+        p.wide_list[k] = make_int4(node, first, last, seeded);
     }
 }
 
@@ -310,7 +311,6 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
 __global__ void __launch_bounds__(128) direct_wide_kernel(DirectParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patches[4];
-    __shared__ ViewGeom geoms[4][MAX_VIEWS];
     const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int V = p.n_targets;
     const int taps = (2 * p.wide_radius + 1) * (2 * p.wide_radius + 1);
@@ -321,27 +321,23 @@ __global__ void __launch_bounds__(128) direct_wide_kernel(DirectParams p) {
         int4 entry = p.wide_list[e];
         const int node = entry.x, first = entry.y, last = entry.z;
         const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
-        if (lane == 0) {
-            int seeded;
-            direct_candidates(p, cx, cy, d.cand, &seeded);
-        }
-        __syncwarp();
-        warp_stage_node(p, d, patch, geoms[slot], cx, cy, p.wide_radius, p.spatial_wide,
-                        p.geometry + (size_t)node * V);
+        int seeded;
+        warp_direct_candidates(p, cx, cy, d.cand, seeded);
+        warp_stage_node(p, d, patch, cx, cy, p.wide_radius, p.spatial_wide, p.geometry + (size_t)node * V);
         const int n = last - first + 1;
-        warp_direct_scores(p, d, patch, geoms[slot], d.cand + first, n, p.wide_radius);
-        if (lane == 0) {
-            double depth = 0.0;
-            float confidence = 0.0f, improvement = 0.0f;
-            bool has = select_direct(d.cand + first, d.agg + 1, n, d.agg[0] == d.agg[0], d.agg[0], entry.w != 0,
-                                     p.far_depth, p.near_depth, p.minimum_score, p.minimum_margin,
-                                     p.minimum_improvement, depth, confidence, improvement);
-            if (has) {
-                p.out.has[node] = 1;
-                p.out.depth[node] = depth;
-                p.out.confidence[node] = confidence;
-                p.out.improvement[node] = improvement;
-            }
+        warp_direct_scores(p, d, patch, d.cand + first, n, p.wide_radius);
+        double depth = 0.0;
+        float confidence = 0.0f, improvement = 0.0f;
+        int best;
+        const bool has = warp_select_direct(d.cand + first, d.agg + 1, n, d.agg[0] == d.agg[0], d.agg[0],
+                                            entry.w != 0, p.far_depth, p.near_depth, p.minimum_score,
+                                            p.minimum_margin, p.minimum_improvement, depth, confidence,
+                                            improvement, best);
+        if (has && lane == 0) {
+            p.out.has[node] = 1;
+            p.out.depth[node] = depth;
+            p.out.confidence[node] = confidence;
+            p.out.improvement[node] = improvement;
         }
         __syncwarp();
     }

@@ -29,6 +29,7 @@ using namespace chiaro;
 
 struct chiaro_depth_ctx {
     int device = 0;
+    int sm_count = 1;
     cudaStream_t stream = nullptr;
     std::string error;
     struct Buffer {
@@ -109,6 +110,22 @@ std::vector<float> spatial_weights(int radius) {
 }
 
 unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)div_ceil(n, threads); }
+
+// Warps per CTA (1..most) for a warp-per-node kernel with `slot_bytes` of
+// dynamic shared memory per warp: the count that keeps the most warps resident.
+template <typename Kernel>
+int warps_per_cta(Kernel kernel, size_t slot_bytes, int most) {
+    int best = 1, resident = 0;
+    for (int k = most; k >= 1; --k) {
+        int blocks = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, 32 * k, k * slot_bytes));
+        if (blocks * k > resident) {
+            resident = blocks * k;
+            best = k;
+        }
+    }
+    return best;
+}
 
 struct Grids {
     size_t coarse_step, coarse_columns, coarse_rows;
@@ -481,12 +498,14 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         const int taps = (2 * direct_radius + 1) * (2 * direct_radius + 1);
         const int wide_taps = (2 * wide_radius + 1) * (2 * wide_radius + 1);
         const size_t slot = direct_slot_bytes(V, taps), wide_slot = direct_slot_bytes(V, wide_taps);
-        p.nodes_per_cta = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / slot));
         if (slot > 200 * 1024 || 4 * wide_slot > 200 * 1024)
             throw CudaError{cudaErrorInvalidValue, "direct pass shared memory exceeds 200 KiB"};
+        p.nodes_per_cta = warps_per_cta(direct_depth_kernel, slot, 8);
         direct_depth_kernel<<<blocks_for(M, p.nodes_per_cta), 32 * p.nodes_per_cta, p.nodes_per_cta * slot, s>>>(p);
         CK(cudaGetLastError());
-        direct_wide_kernel<<<148 * 8, 128, 4 * wide_slot, s>>>(p);
+        int wide_blocks = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wide_blocks, direct_wide_kernel, 128, 4 * wide_slot));
+        direct_wide_kernel<<<ctx->sm_count * std::max(1, wide_blocks), 128, 4 * wide_slot, s>>>(p);
         CK(cudaGetLastError());
     }
     if (debug) {
@@ -571,8 +590,10 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         p.spatial = d_sp;
         p.minimum_score = o.minimum_score;
         int taps = (2 * radius + 1) * (2 * radius + 1);
-        dim3 grid(blocks_for(M, DECISION_NODES), V);
-        target_decision_kernel<<<grid, DECISION_LANES * DECISION_NODES, decision_smem_bytes(taps), s>>>(p);
+        const size_t slot = decision_slot_bytes(V, taps);
+        if (slot > 200 * 1024) throw CudaError{cudaErrorInvalidValue, "decision shared memory exceeds 200 KiB"};
+        const int warps = warps_per_cta(target_decision_kernel, slot, DECISION_WARPS);
+        target_decision_kernel<<<blocks_for(M, warps), 32 * warps, warps * slot, s>>>(p);
         CK(cudaGetLastError());
         Decisions dec2 = decision_bufs(ctx, "dec_consensus", M), dec3 = decision_bufs(ctx, "dec_boundary", M);
         for (int v = 0; v < V; ++v) {
@@ -774,6 +795,7 @@ int chiaro_depth_ctx_create(int device, chiaro_depth_ctx **out) {
     ctx->device = device;
     try {
         CK(cudaSetDevice(device));
+        CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
         CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         for (auto &e : ctx->events) CK(cudaEventCreate(&e));
     } catch (const CudaError &e) {

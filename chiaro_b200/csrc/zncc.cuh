@@ -126,6 +126,96 @@ __device__ inline TapBox warp_tap_box(const double2 *gh, int taps) {
     return b;
 }
 
+// The same box computed by an aligned group of eight lanes over one target's
+// taps. Every lane of the warp calls it (the groups reduce with shuffles).
+__device__ inline TapBox group8_tap_box(const double2 *gh, int taps) {
+    TapBox b{gh[0].x, gh[0].x, gh[0].y, gh[0].y};
+    for (int t = threadIdx.x & 7; t < taps; t += 8) {
+        b.xmin = fmin(b.xmin, gh[t].x);
+        b.xmax = fmax(b.xmax, gh[t].x);
+        b.ymin = fmin(b.ymin, gh[t].y);
+        b.ymax = fmax(b.ymax, gh[t].y);
+    }
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) {
+        b.xmin = fmin(b.xmin, __shfl_xor_sync(0xffffffffu, b.xmin, off));
+        b.xmax = fmax(b.xmax, __shfl_xor_sync(0xffffffffu, b.xmax, off));
+        b.ymin = fmin(b.ymin, __shfl_xor_sync(0xffffffffu, b.ymin, off));
+        b.ymax = fmax(b.ymax, __shfl_xor_sync(0xffffffffu, b.ymax, off));
+    }
+    return b;
+}
+
+// A sequential f32 sum in tap order (the reference's three patch sums add w,
+// w r and (w r) r tap by tap).
+__device__ inline float sequential_sum(const float *a, int taps) {
+    float sum = 0.0f;
+    for (int t = 0; t < taps; ++t) sum += a[t];
+    return sum;
+}
+
+__device__ inline void store_reference_sum(RefPatch &patch, int which, float sum) {
+    if (which == 0)
+        patch.count = sum;
+    else if (which == 1)
+        patch.sum_r = sum;
+    else
+        patch.sum_rr = sum;
+}
+
+// Warp-cooperative staging of one node at (cx, cy) and `radius`: the
+// reference patch (w, w r, (w r) r per tap, the three sums, the energy and the
+// centre sample) and, for each target, g/2 of every tap and their box. Returns
+// on every lane the mask of targets with a tap where the global warp is None
+// (bit v); `patch` is written by lanes 0-2 and valid after the trailing
+// __syncwarp().
+__device__ inline unsigned warp_stage_patch(const DevView *views, int reference, const int *targets, int V,
+                                            double cx, double cy, int radius, const float *spatial, float *rr,
+                                            float *w, float *wr, double2 *gh, TapBox *box, RefPatch &patch) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int taps = (2 * radius + 1) * (2 * radius + 1);
+    const DevView &rv = views[reference];
+    float centre = 0.0f;
+    const bool centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+    bool sampled = true;
+    unsigned undefined = 0u;
+    for (int t = lane; t < taps; t += 32) {
+        int dx, dy;
+        tap_offset(t, radius, dx, dy);
+        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+        float value = 0.0f;
+        sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+        float weight = spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
+        float weighted = weight * value;
+        w[t] = weight;
+        wr[t] = weighted;
+        rr[t] = weighted * value;
+        for (int v = 0; v < V; ++v) {
+            float qx = 0.0f, qy = 0.0f;
+            if (!warp_map(views[targets[v]].warp, (float)px, (float)py, qx, qy)) undefined |= 1u << v;
+            gh[v * taps + t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
+        }
+    }
+    undefined = __reduce_or_sync(full, undefined);
+    sampled = __all_sync(full, sampled);
+    __syncwarp();
+    for (int vb = 0; vb < V; vb += 4) {  // eight lanes per target
+        const int v = vb + (lane >> 3);
+        TapBox b = group8_tap_box(gh + (v < V ? v : V - 1) * taps, taps);
+        if ((lane & 7) == 0 && v < V) box[v] = b;
+    }
+    if (lane < 3) store_reference_sum(patch, lane, sequential_sum(lane == 0 ? w : lane == 1 ? wr : rr, taps));
+    __syncwarp();
+    if (lane == 0) {
+        patch.centre = centre;
+        patch.ok = centre_ok && sampled;
+        patch.ref_energy = patch.sum_rr - patch.sum_r * patch.sum_r / patch.count;
+    }
+    __syncwarp();
+    return undefined;
+}
+
 // Label-independent geometry of map_at_depth for one (node, target); one thread.
 __device__ void view_geometry(const DevCamera &rc, const DevCamera &tc, const WarpRef &warp, double cx, double cy,
                               ViewGeom &g) {
