@@ -1,10 +1,15 @@
 // cost.cuh — build_cost_volume (crates/chiaro-fusion/src/depth.rs:1187-1277).
 //
-// One CTA per coarse node. The CTA stages the node's reference patch, every
-// target's tap positions and the label-independent geometry in shared memory,
-// then each thread evaluates one depth label across all targets, aggregates
-// the views (depth.rs:1761-1770) and writes the label-minor score and cost rows
-// (node-major [N][D], as the reference lays them out).
+// One CTA of four warps per coarse node. The CTA stages the node's reference
+// patch, every target's tap positions and the label-independent geometry in
+// shared memory. It then settles, for every (target, label) item, whether the
+// hypothesis projects within reach and whether all its taps sample inside the
+// target (the fast path), and lists the items that are scored, fast ones first,
+// view-major so neighbouring lanes share a target. All four warps run the
+// correlations of that list, so no lane waits on an item that is never scored
+// and the D = planes + 1 labels leave no nearly empty warp. Last, a thread per
+// label aggregates the views (depth.rs:1761-1770) and writes the label-minor
+// score and cost rows (node-major [N][D], as the reference lays them out).
 #pragma once
 
 #include "zncc.cuh"
@@ -27,122 +32,227 @@ struct CostParams {
     uint8_t *tested;
 };
 
-// Dynamic shared memory of a node CTA: cameras, view geometry, reference
-// patch arrays and per-view tap positions.
-struct NodeSmem {
-    DevCamera *cams;  // [0] reference, [1 + v] targets
-    ViewGeom *geom;   // [V]
-    TapBox *box;      // [V]
-    float *r, *w, *wr;  // [T]
-    double2 *gh;      // [V][T] g/2 of the tap positions
-};
+constexpr int COST_THREADS = 128;
+constexpr int COST_MAX_CHUNKS = 32;  // item chunks listed per barrier pair
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16; }
 
-__host__ __device__ inline size_t node_smem_bytes(int V, int taps) {
-    return align16((V + 1) * sizeof(DevCamera)) + align16(V * sizeof(ViewGeom)) + align16(V * sizeof(TapBox)) +
-           align16(3 * taps * sizeof(float)) + (size_t)V * taps * sizeof(double2);
+// Dynamic shared memory of a node CTA.
+struct NodeSmem {
+    ViewGeom *geom;        // [V]
+    TapBox *box;           // [V]
+    float *rr, *w, *wr;    // [T]: (w r) r, w, w r
+    double2 *gh;           // [V][T] g/2 of the tap positions
+    float *score;          // [V][D] per-view scores, NaN = None
+    unsigned short *list;  // [V][D] scored items: fast path from the front, exact path from the back
+    double2 *disp;         // [V][D] displacement (ddx, ddy) of each item; ddx NaN: out of reach
+};
+
+__host__ __device__ inline size_t node_smem_bytes(int V, int taps, int labels) {
+    const size_t items = (size_t)V * labels;
+    return align16(V * sizeof(ViewGeom)) + align16(V * sizeof(TapBox)) +
+           align16(3 * taps * sizeof(float)) + align16((size_t)V * taps * sizeof(double2)) +
+           align16(items * sizeof(float)) + align16(items * sizeof(unsigned short)) + items * sizeof(double2);
 }
 
-__device__ inline NodeSmem carve_node_smem(unsigned char *base, int V, int taps) {
+__device__ inline NodeSmem carve_node_smem(unsigned char *base, int V, int taps, int labels) {
+    const size_t items = (size_t)V * labels;
     NodeSmem s;
     size_t o = 0;
-    s.cams = reinterpret_cast<DevCamera *>(base + o);
-    o += align16((V + 1) * sizeof(DevCamera));
     s.geom = reinterpret_cast<ViewGeom *>(base + o);
     o += align16(V * sizeof(ViewGeom));
     s.box = reinterpret_cast<TapBox *>(base + o);
     o += align16(V * sizeof(TapBox));
-    s.r = reinterpret_cast<float *>(base + o);
-    s.w = s.r + taps;
+    s.rr = reinterpret_cast<float *>(base + o);
+    s.w = s.rr + taps;
     s.wr = s.w + taps;
     o += align16(3 * taps * sizeof(float));
     s.gh = reinterpret_cast<double2 *>(base + o);
+    o += align16((size_t)V * taps * sizeof(double2));
+    s.score = reinterpret_cast<float *>(base + o);
+    o += align16(items * sizeof(float));
+    s.list = reinterpret_cast<unsigned short *>(base + o);
+    o += align16(items * sizeof(unsigned short));
+    s.disp = reinterpret_cast<double2 *>(base + o);
     return s;
 }
 
-// Copy the reference camera and the target cameras into shared memory.
-__device__ inline void load_cameras(DevCamera *cams, const DevView *views, int reference, const int *targets, int V) {
-    const int words = sizeof(DevCamera) / 8;
-    for (int i = threadIdx.x; i < (V + 1) * words; i += blockDim.x) {
-        int c = i / words, k = i % words;
-        const DevCamera &src = c == 0 ? views[reference].cam : views[targets[c - 1]].cam;
-        reinterpret_cast<uint64_t *>(&cams[c])[k] = reinterpret_cast<const uint64_t *>(&src)[k];
-    }
-}
-
-// Stage reference patch, tap positions and (from the precomputed records
-// `recs[0..V)`, when given) the view geometry for the node at (cx, cy) at the
-// given radius. Without records the geometry already in s.geom is kept and
-// only taps_ok is recomputed. Ends with __syncthreads().
-__device__ inline void stage_node(const NodeSmem &s, RefPatch &patch, const DevView *views, int reference,
-                                  const int *targets, int V, double cx, double cy, int radius, const float *spatial,
-                                  const GeomRec *recs) {
-    const int taps = (2 * radius + 1) * (2 * radius + 1);
-    for (int v = threadIdx.x; v < V; v += blockDim.x) {
-        if (recs) geom_from_rec(recs[v], camera_origin(s.cams[0]), s.geom[v]);
-        s.geom[v].taps_ok = 1;
-    }
-    ref_patch_setup(views[reference].luma, cx, cy, radius, spatial, s.r, s.w, s.wr, patch);
-    for (int v = 0; v < V; ++v)
-        tap_positions(views[targets[v]].warp, cx, cy, radius, s.gh + v * taps, s.geom[v]);
-    __syncthreads();
-    // one warp per view computes its tap box
-    for (int v = threadIdx.x >> 5; v < V; v += blockDim.x >> 5) {
-        TapBox b = warp_tap_box(s.gh + v * taps, taps);
-        if ((threadIdx.x & 31) == 0) s.box[v] = b;
-    }
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(256) cost_volume_kernel(CostParams p) {
+__global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patch;
+    __shared__ unsigned warp_undefined[COST_THREADS / 32];  // bit v: a tap of target v has no global warp
+    __shared__ int counts[COST_MAX_CHUNKS][2][COST_THREADS / 32];  // [chunk][fast, exact][warp]
+    const unsigned full = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int warps = COST_THREADS / 32;
     const int node = blockIdx.x;
-    const int column = node % p.columns, row = node / p.columns;
+    const int V = p.n_targets, D = p.labels;
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
-    const int V = p.n_targets;
-    NodeSmem s = carve_node_smem(smem_raw, V, taps);
-    const double cx = (double)(column * p.step), cy = (double)(row * p.step);
+    const int total = V * D;
+    const int chunks = (total + COST_THREADS - 1) / COST_THREADS;
+    NodeSmem s = carve_node_smem(smem_raw, V, taps, D);
+    const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
+    const DevView &rv = p.views[p.reference];
+    const D3 origin = camera_origin(rv.cam);
 
-    load_cameras(s.cams, p.views, p.reference, p.targets, V);
-    __syncthreads();
-    stage_node(s, patch, p.views, p.reference, p.targets, V, cx, cy, p.radius, p.spatial,
-               p.geometry + (size_t)node * V);
-
-    int any_finite = 0;
-    for (int label = threadIdx.x; label < p.labels; label += blockDim.x) {
-        float sc[MAX_VIEWS];
-        for (int v = 0; v < V; ++v) {
-            sc[v] = NAN;
-            const ViewGeom &g = s.geom[v];
-            double ddx = 0.0, ddy = 0.0;
-            if (!g.gc_ok) continue;
-            if (label > 0 && !depth_delta(s.cams[1 + v], g, p.label_depth[label], ddx, ddy)) continue;
-            if (!patch.ok || !g.taps_ok) continue;
-            const DevView &tv = p.views[p.targets[v]];
-            float score;
-            if (zncc_any(TargetRef{tv.luma, tv.pairs}, s.gh + v * taps, s.box[v], s.w, s.wr, patch, taps, ddx, ddy,
-                         score))
-                sc[v] = score;
+    // ---- staging: geometry, reference patch, tap positions
+    if (tid < V) geom_from_rec(p.geometry[(size_t)node * V + tid], origin, s.geom[tid]);
+    float centre = 0.0f;
+    const bool centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+    bool sampled = true;
+    for (int t = tid; t < taps; t += COST_THREADS) {
+        int dx, dy;
+        tap_offset(t, p.radius, dx, dy);
+        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+        float value = 0.0f;
+        sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+        float weight = p.spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
+        float weighted = weight * value;
+        s.w[t] = weight;
+        s.wr[t] = weighted;
+        s.rr[t] = weighted * value;
+    }
+    unsigned undefined = 0u;
+    for (int i = tid; i < V * taps; i += COST_THREADS) {
+        const int v = i / taps, t = i - v * taps;
+        int dx, dy;
+        tap_offset(t, p.radius, dx, dy);
+        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+        float qx = 0.0f, qy = 0.0f;
+        if (!warp_map(p.views[p.targets[v]].warp, (float)px, (float)py, qx, qy)) undefined |= 1u << v;
+        s.gh[i] = make_double2((double)qx * 0.5, (double)qy * 0.5);
+    }
+    // displacement of every (target, label) item, view-major: item = v * D + label
+    for (int item = tid; item < total; item += COST_THREADS) {
+        const int v = item / D, label = item - v * D;
+        ViewGeom g;
+        geom_from_rec(p.geometry[(size_t)node * V + v], origin, g);
+        double ddx = 0.0, ddy = 0.0;
+        bool ok = g.gc_ok;
+        if (ok && label > 0) ok = depth_delta(p.views[p.targets[v]].cam, g, p.label_depth[label], ddx, ddy);
+        s.disp[item] = make_double2(ok ? ddx : NAN, ddy);
+    }
+    undefined = __reduce_or_sync(full, undefined);
+    if (lane == 0) warp_undefined[warp] = undefined;
+    const bool all_sampled = __syncthreads_and(sampled);
+    // tap boxes (eight lanes per target) and the three sequential reference
+    // sums (lanes 0-2 of the warp after the box warps)
+    for (int vb = warp * 4; vb < V; vb += 4 * warps) {
+        const int v = vb + (lane >> 3);
+        TapBox b = group8_tap_box(s.gh + (v < V ? v : V - 1) * taps, taps);
+        if ((lane & 7) == 0 && v < V) s.box[v] = b;
+    }
+    if (warp == ((V + 3) / 4) % warps) {
+        float sum = 0.0f;
+        if (lane < 3) sum = sequential_sum(lane == 0 ? s.w : lane == 1 ? s.wr : s.rr, taps);
+        const float count = __shfl_sync(full, sum, 0), sum_r = __shfl_sync(full, sum, 1);
+        const float sum_rr = __shfl_sync(full, sum, 2);
+        if (lane == 0) {
+            patch.count = count;
+            patch.sum_r = sum_r;
+            patch.sum_rr = sum_rr;
+            patch.ref_energy = sum_rr - sum_r * sum_r / count;
+            patch.centre = centre;
+            patch.ok = centre_ok && all_sampled;
         }
+    }
+    __syncthreads();
+
+    // ---- which items are scored, and on which path; then list them, fast
+    // first. Chunk c holds items c * COST_THREADS + tid; the counts of up to
+    // COST_MAX_CHUNKS chunks are exchanged per barrier pair.
+    const bool patch_ok = patch.ok;
+    unsigned taps_bad = 0u;
+    for (int w = 0; w < warps; ++w) taps_bad |= warp_undefined[w];
+    const unsigned below = (1u << lane) - 1u;
+    int n_fast = 0, n_exact = 0;
+    for (int c0 = 0; c0 < chunks; c0 += COST_MAX_CHUNKS) {
+        const int c1 = min(chunks, c0 + COST_MAX_CHUNKS);
+        unsigned fast_bits = 0u, exact_bits = 0u;
+        for (int c = c0; c < c1; ++c) {
+            const int item = c * COST_THREADS + tid;
+            bool scored = false, fast = false;
+            if (item < total) {
+                const int v = item / D;
+                const double2 dd = s.disp[item];
+                scored = !(dd.x != dd.x) && patch_ok && !((taps_bad >> v) & 1u);
+                if (scored) {
+                    const PlaneRef &plane = p.views[p.targets[v]].luma;
+                    fast = taps_inside(s.box[v], dd.x * 0.5, dd.y * 0.5, plane.width, plane.height);
+                } else {
+                    s.score[item] = NAN;
+                }
+            }
+            const unsigned fast_mask = __ballot_sync(full, scored && fast);
+            const unsigned exact_mask = __ballot_sync(full, scored && !fast);
+            if (lane == 0) {
+                counts[c - c0][0][warp] = __popc(fast_mask);
+                counts[c - c0][1][warp] = __popc(exact_mask);
+            }
+            if (scored && fast) fast_bits |= 1u << (c - c0);
+            if (scored && !fast) exact_bits |= 1u << (c - c0);
+        }
+        __syncthreads();
+        for (int c = c0; c < c1; ++c) {
+            int fast_at = n_fast, exact_at = n_exact;
+            for (int w = 0; w < warps; ++w) {
+                const int f = counts[c - c0][0][w], e = counts[c - c0][1][w];
+                if (w < warp) {
+                    fast_at += f;
+                    exact_at += e;
+                }
+                n_fast += f;
+                n_exact += e;
+            }
+            const bool is_fast = (fast_bits >> (c - c0)) & 1u, is_exact = (exact_bits >> (c - c0)) & 1u;
+            const unsigned fast_mask = __ballot_sync(full, is_fast);
+            const unsigned exact_mask = __ballot_sync(full, is_exact);
+            const int item = c * COST_THREADS + tid;
+            if (is_fast) s.list[fast_at + __popc(fast_mask & below)] = (unsigned short)item;
+            if (is_exact) s.list[total - 1 - (exact_at + __popc(exact_mask & below))] = (unsigned short)item;
+        }
+        __syncthreads();
+    }
+
+    // ---- the correlations of the listed items
+    const int listed = n_fast + n_exact;
+    for (int j = tid; j < listed; j += COST_THREADS) {
+        const int item = s.list[j < n_fast ? j : total - 1 - (j - n_fast)];
+        const int v = item / D;
+        const DevView &tv = p.views[p.targets[v]];
+        const double2 dd = s.disp[item];
+        float score;
+        if (!zncc_any(TargetRef{tv.luma, tv.pairs}, s.gh + v * taps, s.box[v], s.w, s.wr, patch, taps, dd.x, dd.y,
+                      score))
+            score = NAN;
+        s.score[item] = score;
+    }
+    __syncthreads();
+
+    // ---- aggregate the views per label and price the label (depth.rs:1233-1246)
+    int any_finite = 0;
+    for (int label = tid; label < D; label += COST_THREADS) {
+        float sc[MAX_VIEWS];
+        for (int v = 0; v < V; ++v) sc[v] = s.score[v * D + label];
         float agg;
         float score = aggregate_scores(sc, V, p.minimum_support, p.best_view_count, agg) ? agg : NAN;
         float cost;
         if (isfinite(score)) {
             any_finite = 1;
-            float near_prior = label == 0 ? 0.0f : NEAR_DEPTH_PRIOR * (float)(label - 1) / (float)(p.labels - 2);
+            float near_prior = label == 0 ? 0.0f : NEAR_DEPTH_PRIOR * (float)(label - 1) / (float)(D - 2);
             cost = clampf_r(1.0f - score, 0.0f, 2.0f) + near_prior;
         } else {
             cost = MISSING_COST;
         }
-        size_t o = (size_t)node * p.labels + label;
+        size_t o = (size_t)node * D + label;
         p.scores[o] = score;
         p.costs[o] = cost;
     }
-    // tested: any finite score; p.tested starts zeroed, one store per warp that saw one
-    if (__ballot_sync(0xffffffffu, any_finite) && (threadIdx.x & 31) == 0) p.tested[node] = 1;
-    if (threadIdx.x == 0) p.guidance[node] = patch.centre;  // reference_guidance (depth.rs:1824-1832)
+    const bool tested = __syncthreads_or(any_finite);
+    if (tid == 0) {
+        p.tested[node] = tested;
+        p.guidance[node] = patch.centre;  // reference_guidance (depth.rs:1824-1832)
+    }
 }
 
 }  // namespace chiaro

@@ -404,8 +404,10 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         p.guidance = guidance;
         p.tested = tested;
         int taps = (2 * radius + 1) * (2 * radius + 1);
-        unsigned threads = (unsigned)std::min(256, (D + 31) / 32 * 32);
-        cost_volume_kernel<<<(unsigned)N, threads, node_smem_bytes(V, taps), s>>>(p);
+        const size_t smem = node_smem_bytes(V, taps, D);
+        if ((size_t)V * D > 65535 || smem > 200 * 1024)
+            throw CudaError{cudaErrorInvalidValue, "cost volume: targets x labels exceed the node CTA's shared memory"};
+        cost_volume_kernel<<<(unsigned)N, COST_THREADS, smem, s>>>(p);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(ctx->events[1], s));

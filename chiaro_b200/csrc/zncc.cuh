@@ -43,91 +43,9 @@ __device__ __forceinline__ void tap_offset(int t, int radius, int &dx, int &dy) 
     dx = t % side - radius;
 }
 
-// Reference patch of the node at (cx, cy): r[], w[], wr[] and the sums.
-// Block-cooperative; ends with __syncthreads().
-__device__ void ref_patch_setup(const PlaneRef &ref, double cx, double cy, int radius, const float *spatial,
-                                float *r, float *w, float *wr, RefPatch &patch) {
-    int taps = (2 * radius + 1) * (2 * radius + 1);
-    float centre = 0.0f;
-    bool centre_ok = plane_sample(ref, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
-    if (threadIdx.x == 0) {
-        patch.ok = centre_ok ? 1 : 0;
-        patch.centre = centre;
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < taps; t += blockDim.x) {
-        int dx, dy;
-        tap_offset(t, radius, dx, dy);
-        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
-        float rv = 0.0f;
-        if (!plane_sample(ref, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), rv)) patch.ok = 0;
-        float weight = spatial[t] * exp_f32(-1.2f * fabsf(rv - centre));
-        r[t] = rv;
-        w[t] = weight;
-        wr[t] = weight * rv;
-    }
-    __syncthreads();
-    // Three independent sequential sums: threads 0, 32 and 64 when the block
-    // has three warps, otherwise all on thread 0.
-    bool three = blockDim.x >= 96;
-    if (threadIdx.x == 0) {
-        float s = 0.0f;
-        for (int t = 0; t < taps; ++t) s += w[t];
-        patch.count = s;
-    }
-    if ((three && threadIdx.x == 32) || (!three && threadIdx.x == 0)) {
-        float s = 0.0f;
-        for (int t = 0; t < taps; ++t) s += wr[t];
-        patch.sum_r = s;
-    }
-    if ((three && threadIdx.x == 64) || (!three && threadIdx.x == 0)) {
-        float s = 0.0f;
-        for (int t = 0; t < taps; ++t) s += wr[t] * r[t];
-        patch.sum_rr = s;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) patch.ref_energy = patch.sum_rr - patch.sum_r * patch.sum_r / patch.count;
-    __syncthreads();
-}
-
-// Global-warp positions g of every tap for one target warp, stored as g/2 in
-// f64 (exact: g is f32); clears geom.taps_ok when one is undefined.
-// Block-cooperative, no trailing sync.
-__device__ void tap_positions(const WarpRef &warp, double cx, double cy, int radius, double2 *gh, ViewGeom &geom) {
-    int taps = (2 * radius + 1) * (2 * radius + 1);
-    for (int t = threadIdx.x; t < taps; t += blockDim.x) {
-        int dx, dy;
-        tap_offset(t, radius, dx, dy);
-        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
-        float qx = 0.0f, qy = 0.0f;
-        if (!warp_map(warp, (float)px, (float)py, qx, qy)) geom.taps_ok = 0;
-        gh[t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
-    }
-}
-
-// Bounding box of g/2 over the taps, computed by one whole warp (min/max are
-// exact, so the reduction order does not matter). Every lane gets the box.
-__device__ inline TapBox warp_tap_box(const double2 *gh, int taps) {
-    const int lane = threadIdx.x & 31;
-    TapBox b{gh[0].x, gh[0].x, gh[0].y, gh[0].y};
-    for (int t = lane; t < taps; t += 32) {
-        b.xmin = fmin(b.xmin, gh[t].x);
-        b.xmax = fmax(b.xmax, gh[t].x);
-        b.ymin = fmin(b.ymin, gh[t].y);
-        b.ymax = fmax(b.ymax, gh[t].y);
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        b.xmin = fmin(b.xmin, __shfl_xor_sync(0xffffffffu, b.xmin, off));
-        b.xmax = fmax(b.xmax, __shfl_xor_sync(0xffffffffu, b.xmax, off));
-        b.ymin = fmin(b.ymin, __shfl_xor_sync(0xffffffffu, b.ymin, off));
-        b.ymax = fmax(b.ymax, __shfl_xor_sync(0xffffffffu, b.ymax, off));
-    }
-    return b;
-}
-
-// The same box computed by an aligned group of eight lanes over one target's
-// taps. Every lane of the warp calls it (the groups reduce with shuffles).
+// Bounding box of g/2 over one target's taps, computed by an aligned group of
+// eight lanes (min and max are exact, so the reduction order does not matter).
+// Every lane of the warp calls it; the groups reduce with shuffles.
 __device__ inline TapBox group8_tap_box(const double2 *gh, int taps) {
     TapBox b{gh[0].x, gh[0].x, gh[0].y, gh[0].y};
     for (int t = threadIdx.x & 7; t < taps; t += 8) {
