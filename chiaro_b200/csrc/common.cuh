@@ -387,7 +387,7 @@ CH_HD D3 along(D3 origin, D3 direction, double depth) {
 // ---- device forms of the boundary types -------------------------------------------
 struct DevView {
     PlaneRef luma;
-    const float2 *pairs;  // (L[x], L[x+1]) pair plane of the luminance (targets only)
+    const float4 *quads;  // bilinear neighbourhood (quad) plane of the luminance (targets only)
     WarpRef warp;
     int width, height;
     int has_camera, accepted;

@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = s.disp[item];
         float score;
-        if (!zncc_any(TargetRef{tv.luma, tv.pairs}, s.gh + v * taps, s.box[v], s.w, s.wr, patch, taps, dd.x, dd.y,
+        if (!zncc_any(TargetRef{tv.luma, tv.quads}, s.gh + v * taps, s.box[v], s.w, s.wr, patch, taps, dd.x, dd.y,
                       score))
             score = NAN;
         s.score[item] = score;

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = d.disp[j];
         float score;
-        if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
+        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
                      score))
             d.sc[v * 16 + k] = score;
         else if (k < 5)
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = d.disp[j];
         float score;
-        if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
+        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
                      score))
             d.sc[v * 16 + 6 + (item & 7)] = score;
         else

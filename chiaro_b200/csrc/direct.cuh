@@ -251,7 +251,7 @@ __device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlo
         double ddx = 0.0, ddy = 0.0;
         if (c >= 0) depth_delta(tv.cam, geom[v], cand[c], ddx, ddy);
         float score = NAN, sc;
-        if (zncc_any(TargetRef{tv.luma, tv.pairs}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, ddx, ddy, sc))
+        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, ddx, ddy, sc))
             score = sc;
         d.items[item] = score;
     }

@@ -364,14 +364,14 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     CK(cudaMemsetAsync(d_results, 0, sizeof(Results), s));
 
     CK(cudaEventRecord(ctx->events[0], s));
-    // (L[x], L[x+1]) pair planes of the target luminance for the fast ZNCC path
+    // quad planes of the target luminance for the fast ZNCC path
     for (int t : targets) {
         const PlaneRef &lp = h_views[t].luma;
         size_t n = (size_t)lp.width * lp.height;
-        float2 *pairs = dbuf<float2>(ctx, "pairs" + std::to_string(t), n);
-        pair_plane_kernel<<<blocks_for(n, 256), 256, 0, s>>>(lp.data, lp.width, lp.height, pairs);
+        float4 *quads = dbuf<float4>(ctx, "quads" + std::to_string(t), n);
+        quad_plane_kernel<<<blocks_for(n, 256), 256, 0, s>>>(lp.data, lp.width, lp.height, quads);
         CK(cudaGetLastError());
-        h_views[t].pairs = pairs;
+        h_views[t].quads = quads;
     }
     upload(ctx, d_views, h_views.data(), h_views.size());
     // ---- cost volume
@@ -616,7 +616,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->events[6], s));
-    // pair planes 1 per target, geometry 2, cost 1, SGM 8, select 1, completion, direct 2, filters 6, stats 2,
+    // quad planes 1 per target, geometry 2, cost 1, SGM 8, select 1, completion, direct 2, filters 6, stats 2,
     // decisions 1 + 3 per target, map 1
     ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 8 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
     CK(cudaMemcpyAsync(&h_results, d_results, sizeof(Results), cudaMemcpyDeviceToHost, s));

@@ -264,19 +264,22 @@ __device__ __forceinline__ bool zncc_score(const PlaneRef &target, const double2
 // coordinate is monotone in g, so the bounding box of the taps' g decides for
 // every tap at once whether all samples fall strictly inside [0, w-1) x [0, h-1);
 // inside, the reference's bounds checks and edge clamps cannot trigger and the
-// bilinear fetch reads a (L[x], L[x+1]) pair plane with two 8-byte loads.
+// bilinear fetch reads the four neighbours from a quad plane with one 16-byte
+// load.
 
-// Pair plane: pairs[y * w + x] = (L[y][x], L[y][min(x + 1, w - 1)]).
-__global__ void pair_plane_kernel(const float *__restrict__ plane, int width, int height, float2 *pairs) {
+// Quad plane: quads[y * w + x] = (L[y][x], L[y][x1], L[y1][x], L[y1][x1]) with
+// x1 = min(x + 1, w - 1) and y1 = min(y + 1, h - 1).
+__global__ void quad_plane_kernel(const float *__restrict__ plane, int width, int height, float4 *quads) {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long)width * height) return;
-    int x = (int)(i % width);
-    pairs[i] = make_float2(plane[i], plane[x + 1 < width ? i + 1 : i]);
+    int x = (int)(i % width), y = (int)(i / width);
+    long right = x + 1 < width ? 1 : 0, down = y + 1 < height ? width : 0;
+    quads[i] = make_float4(plane[i], plane[i + right], plane[i + down], plane[i + down + right]);
 }
 
 struct TargetRef {
     PlaneRef plane;
-    const float2 *pairs;
+    const float4 *quads;
 };
 
 // True when every tap at displacement (hdx, hdy) = (ddx/2, ddy/2) samples
@@ -290,7 +293,7 @@ __device__ __forceinline__ bool taps_inside(const TapBox &box, double hdx, doubl
 
 // warped_patch_zncc's hypothesis-dependent part for taps known to be inside
 // (see taps_inside). gh holds g/2 per tap.
-__device__ __forceinline__ float zncc_inside(const float2 *__restrict__ pairs, int width, const double2 *gh,
+__device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, int width, const double2 *gh,
                                              const float *w, const float *wr, const RefPatch &patch, int taps,
                                              double hdx, double hdy, bool &ok) {
     float st = 0.0f, stt = 0.0f, srt = 0.0f;
@@ -301,10 +304,9 @@ __device__ __forceinline__ float zncc_inside(const float2 *__restrict__ pairs, i
         float y = (float)((g.y + hdy) - 0.25);
         int ix, iy;
         float tx = floor_frac_small(x, ix), ty = floor_frac_small(y, iy);
-        const float2 *row = pairs + (size_t)iy * width + ix;
-        float2 a = __ldg(row), b = __ldg(row + width);
-        float top = a.x * (1.0f - tx) + a.y * tx;
-        float bottom = b.x * (1.0f - tx) + b.y * tx;
+        const float4 q = __ldg(quads + (size_t)iy * width + ix);
+        float top = q.x * (1.0f - tx) + q.y * tx;
+        float bottom = q.z * (1.0f - tx) + q.w * tx;
         float tv = top * (1.0f - ty) + bottom * ty;
         float wt = w[t] * tv;
         st += wt;
@@ -325,7 +327,7 @@ __device__ __forceinline__ bool zncc_any(const TargetRef &target, const double2 
     double hdx = ddx * 0.5, hdy = ddy * 0.5;
     if (taps_inside(box, hdx, hdy, target.plane.width, target.plane.height)) {
         bool ok;
-        score = zncc_inside(target.pairs, target.plane.width, gh, w, wr, patch, taps, hdx, hdy, ok);
+        score = zncc_inside(target.quads, target.plane.width, gh, w, wr, patch, taps, hdx, hdy, ok);
         return ok;
     }
     return zncc_score(target.plane, gh, w, wr, patch, taps, ddx, ddy, score);
