@@ -41,7 +41,8 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16;
 struct NodeSmem {
     ViewGeom *geom;        // [V]
     TapBox *box;           // [V]
-    float *rr, *w, *wr;    // [T]: (w r) r, w, w r
+    float *rr;             // [T] (w r) r
+    float2 *wt;            // [T] (w, w r)
     double2 *gh;           // [V][T] g/2 of the tap positions
     float *score;          // [V][D] per-view scores, NaN = None
     unsigned short *list;  // [V][D] scored items: fast path from the front, exact path from the back
@@ -51,7 +52,8 @@ struct NodeSmem {
 __host__ __device__ inline size_t node_smem_bytes(int V, int taps, int labels) {
     const size_t items = (size_t)V * labels;
     return align16(V * sizeof(ViewGeom)) + align16(V * sizeof(TapBox)) +
-           align16(3 * taps * sizeof(float)) + align16((size_t)V * taps * sizeof(double2)) +
+           align16(taps * sizeof(float)) + align16(taps * sizeof(float2)) +
+           align16((size_t)V * taps * sizeof(double2)) +
            align16(items * sizeof(float)) + align16(items * sizeof(unsigned short)) + items * sizeof(double2);
 }
 
@@ -64,9 +66,9 @@ __device__ inline NodeSmem carve_node_smem(unsigned char *base, int V, int taps,
     s.box = reinterpret_cast<TapBox *>(base + o);
     o += align16(V * sizeof(TapBox));
     s.rr = reinterpret_cast<float *>(base + o);
-    s.w = s.rr + taps;
-    s.wr = s.w + taps;
-    o += align16(3 * taps * sizeof(float));
+    o += align16(taps * sizeof(float));
+    s.wt = reinterpret_cast<float2 *>(base + o);
+    o += align16(taps * sizeof(float2));
     s.gh = reinterpret_cast<double2 *>(base + o);
     o += align16((size_t)V * taps * sizeof(double2));
     s.score = reinterpret_cast<float *>(base + o);
@@ -108,8 +110,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
         float weight = p.spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
         float weighted = weight * value;
-        s.w[t] = weight;
-        s.wr[t] = weighted;
+        s.wt[t] = make_float2(weight, weighted);
         s.rr[t] = weighted * value;
     }
     unsigned undefined = 0u;
@@ -144,7 +145,9 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
     }
     if (warp == ((V + 3) / 4) % warps) {
         float sum = 0.0f;
-        if (lane < 3) sum = sequential_sum(lane == 0 ? s.w : lane == 1 ? s.wr : s.rr, taps);
+        if (lane < 3)
+            sum = lane == 2 ? sequential_sum(s.rr, 1, taps)
+                            : sequential_sum(reinterpret_cast<const float *>(s.wt) + lane, 2, taps);
         const float count = __shfl_sync(full, sum, 0), sum_r = __shfl_sync(full, sum, 1);
         const float sum_rr = __shfl_sync(full, sum, 2);
         if (lane == 0) {
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = s.disp[item];
         float score;
-        if (!zncc_any(TargetRef{tv.luma, tv.quads}, s.gh + v * taps, s.box[v], s.w, s.wr, patch, taps, dd.x, dd.y,
+        if (!zncc_any(TargetRef{tv.luma, tv.quads}, s.gh + v * taps, s.box[v], s.wt, patch, taps, dd.x, dd.y,
                       score))
             score = NAN;
         s.score[item] = score;

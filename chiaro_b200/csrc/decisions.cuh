@@ -40,7 +40,8 @@ constexpr int DECISION_WARPS = 8;  // most nodes (warps) per CTA
 
 // Per-warp shared memory of the decisions for V targets and T taps.
 struct DecisionSlot {
-    float *rr, *w, *wr;    // [T] reference patch: (w r) r, w, w r
+    float *rr;             // [T] reference patch (w r) r
+    float2 *wt;            // [T] reference patch (w, w r)
     double2 *gh;           // [V][T] tap positions g/2
     TapBox *box;           // [V]
     float *sc;             // [V][16]: 0-4 offsets, 5 baseline, 6-13 shifts, 14 best offset
@@ -51,7 +52,7 @@ struct DecisionSlot {
 };
 
 __host__ __device__ inline size_t decision_slot_bytes(int V, int taps) {
-    return align16(3 * taps * sizeof(float)) + align16((size_t)V * taps * sizeof(double2)) +
+    return align16(taps * sizeof(float)) + align16(taps * sizeof(float2)) + align16((size_t)V * taps * sizeof(double2)) +
            align16(V * sizeof(TapBox)) + align16((size_t)V * 16 * sizeof(float)) +
            align16((size_t)V * 16 * sizeof(float2)) + align16((size_t)8 * V * sizeof(double2)) +
            align16((size_t)8 * V * sizeof(unsigned short)) + align16(V * sizeof(int));
@@ -61,9 +62,9 @@ __device__ inline DecisionSlot carve_decision_slot(unsigned char *base, int V, i
     DecisionSlot d;
     size_t o = 0;
     d.rr = reinterpret_cast<float *>(base);
-    d.w = d.rr + taps;
-    d.wr = d.w + taps;
-    o += align16(3 * taps * sizeof(float));
+    o += align16(taps * sizeof(float));
+    d.wt = reinterpret_cast<float2 *>(base + o);
+    o += align16(taps * sizeof(float2));
     d.gh = reinterpret_cast<double2 *>(base + o);
     o += align16((size_t)V * taps * sizeof(double2));
     d.box = reinterpret_cast<TapBox *>(base + o);
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
     defined = __reduce_or_sync(full, defined);
     if (!has || !defined) return;  // whole warp
     const unsigned undefined_taps = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, p.radius,
-                                                     p.spatial, d.rr, d.w, d.wr, d.gh, d.box, patch);
+                                                     p.spatial, d.rr, d.wt, d.gh, d.box, patch);
     const bool patch_ok = patch.ok;
     const D3 origin = camera_origin(rv.cam);
     const double shared_inverse = 1.0 / p.field.depth[node];
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = d.disp[j];
         float score;
-        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
+        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, dd.x, dd.y,
                      score))
             d.sc[v * 16 + k] = score;
         else if (k < 5)
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = d.disp[j];
         float score;
-        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, dd.x, dd.y,
+        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, dd.x, dd.y,
                      score))
             d.sc[v * 16 + 6 + (item & 7)] = score;
         else

@@ -104,7 +104,8 @@ struct DirectParams {
 
 // Per-warp shared memory of the direct pass for V targets and T taps.
 struct DirectSlot {
-    float *rr, *w, *wr;    // [T]: (w r) r, w, w r
+    float *rr;             // [T] (w r) r
+    float2 *wt;            // [T] (w, w r)
     ViewGeom *geom;        // [V]
     double2 *gh;           // [V][T] g/2 (fast path)
     TapBox *box;           // [V]
@@ -115,7 +116,7 @@ struct DirectSlot {
 };
 
 __host__ __device__ inline size_t direct_slot_bytes(int V, int taps) {
-    return align16(3 * taps * sizeof(float)) + align16(V * sizeof(ViewGeom)) +
+    return align16(taps * sizeof(float)) + align16(taps * sizeof(float2)) + align16(V * sizeof(ViewGeom)) +
            align16((size_t)V * taps * sizeof(double2)) + align16(V * sizeof(TapBox)) +
            align16(MAX_DIRECT_CANDIDATES * sizeof(double)) +
            align16((size_t)(MAX_DIRECT_CANDIDATES + 1) * V * sizeof(float)) +
@@ -127,9 +128,9 @@ __device__ inline DirectSlot carve_direct_slot(unsigned char *base, int V, int t
     DirectSlot d;
     size_t o = 0;
     d.rr = reinterpret_cast<float *>(base);
-    d.w = d.rr + taps;
-    d.wr = d.w + taps;
-    o += align16(3 * taps * sizeof(float));
+    o += align16(taps * sizeof(float));
+    d.wt = reinterpret_cast<float2 *>(base + o);
+    o += align16(taps * sizeof(float2));
     d.geom = reinterpret_cast<ViewGeom *>(base + o);
     o += align16(V * sizeof(ViewGeom));
     d.gh = reinterpret_cast<double2 *>(base + o);
@@ -194,7 +195,7 @@ __device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot &
     const int lane = threadIdx.x & 31;
     const int V = p.n_targets;
     const unsigned undefined = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, radius, spatial, d.rr,
-                                                d.w, d.wr, d.gh, d.box, patch);
+                                                d.wt, d.gh, d.box, patch);
     if (lane < V) {
         geom_from_rec(recs[lane], camera_origin(p.views[p.reference].cam), d.geom[lane]);
         d.geom[lane].taps_ok = ((undefined >> lane) & 1u) ? 0 : 1;
@@ -251,7 +252,7 @@ __device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlo
         double ddx = 0.0, ddy = 0.0;
         if (c >= 0) depth_delta(tv.cam, geom[v], cand[c], ddx, ddy);
         float score = NAN, sc;
-        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.w, d.wr, patch, taps, ddx, ddy, sc))
+        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, ddx, ddy, sc))
             score = sc;
         d.items[item] = score;
     }

@@ -64,11 +64,11 @@ __device__ inline TapBox group8_tap_box(const double2 *gh, int taps) {
     return b;
 }
 
-// A sequential f32 sum in tap order (the reference's three patch sums add w,
-// w r and (w r) r tap by tap).
-__device__ inline float sequential_sum(const float *a, int taps) {
+// A sequential f32 sum in tap order of a[t * stride] (the reference's three
+// patch sums add w, w r and (w r) r tap by tap).
+__device__ inline float sequential_sum(const float *a, int stride, int taps) {
     float sum = 0.0f;
-    for (int t = 0; t < taps; ++t) sum += a[t];
+    for (int t = 0; t < taps; ++t) sum += a[t * stride];
     return sum;
 }
 
@@ -82,14 +82,14 @@ __device__ inline void store_reference_sum(RefPatch &patch, int which, float sum
 }
 
 // Warp-cooperative staging of one node at (cx, cy) and `radius`: the
-// reference patch (w, w r, (w r) r per tap, the three sums, the energy and the
+// reference patch ((w, w r) and (w r) r per tap, the three sums, the energy and the
 // centre sample) and, for each target, g/2 of every tap and their box. Returns
 // on every lane the mask of targets with a tap where the global warp is None
 // (bit v); `patch` is written by lanes 0-2 and valid after the trailing
 // __syncwarp().
 __device__ inline unsigned warp_stage_patch(const DevView *views, int reference, const int *targets, int V,
                                             double cx, double cy, int radius, const float *spatial, float *rr,
-                                            float *w, float *wr, double2 *gh, TapBox *box, RefPatch &patch) {
+                                            float2 *wt, double2 *gh, TapBox *box, RefPatch &patch) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int taps = (2 * radius + 1) * (2 * radius + 1);
@@ -106,8 +106,7 @@ __device__ inline unsigned warp_stage_patch(const DevView *views, int reference,
         sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
         float weight = spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
         float weighted = weight * value;
-        w[t] = weight;
-        wr[t] = weighted;
+        wt[t] = make_float2(weight, weighted);
         rr[t] = weighted * value;
         for (int v = 0; v < V; ++v) {
             float qx = 0.0f, qy = 0.0f;
@@ -123,7 +122,10 @@ __device__ inline unsigned warp_stage_patch(const DevView *views, int reference,
         TapBox b = group8_tap_box(gh + (v < V ? v : V - 1) * taps, taps);
         if ((lane & 7) == 0 && v < V) box[v] = b;
     }
-    if (lane < 3) store_reference_sum(patch, lane, sequential_sum(lane == 0 ? w : lane == 1 ? wr : rr, taps));
+    if (lane < 3)
+        store_reference_sum(patch, lane,
+                            lane == 2 ? sequential_sum(rr, 1, taps)
+                                      : sequential_sum(reinterpret_cast<const float *>(wt) + lane, 2, taps));
     __syncwarp();
     if (lane == 0) {
         patch.centre = centre;
@@ -232,7 +234,7 @@ __device__ __forceinline__ bool depth_delta(const DevCamera &tc, const ViewGeom 
 
 // Hypothesis-dependent part of warped_patch_zncc: sample the target at every
 // tap shifted by (ddx, ddy) and finish the correlation. False for None.
-__device__ __forceinline__ bool zncc_score(const PlaneRef &target, const double2 *gh, const float *w, const float *wr,
+__device__ __forceinline__ bool zncc_score(const PlaneRef &target, const double2 *gh, const float2 *wt,
                                            const RefPatch &patch, int taps, double ddx, double ddy, float &score) {
     float st = 0.0f, stt = 0.0f, srt = 0.0f;
     for (int t = 0; t < taps; ++t) {
@@ -242,10 +244,11 @@ __device__ __forceinline__ bool zncc_score(const PlaneRef &target, const double2
         double qy = (double)g.y + ddy;
         float tv;
         if (!plane_sample(target, (float)((qx - 0.5) * 0.5), (float)((qy - 0.5) * 0.5), tv)) return false;
-        float wt = w[t] * tv;
-        st += wt;
-        stt += wt * tv;
-        srt += wr[t] * tv;
+        const float2 weights = wt[t];
+        float wv = weights.x * tv;
+        st += wv;
+        stt += wv * tv;
+        srt += weights.y * tv;
     }
     float covariance = srt - patch.sum_r * st / patch.count;
     float target_energy = stt - st * st / patch.count;
@@ -294,7 +297,7 @@ __device__ __forceinline__ bool taps_inside(const TapBox &box, double hdx, doubl
 // warped_patch_zncc's hypothesis-dependent part for taps known to be inside
 // (see taps_inside). gh holds g/2 per tap.
 __device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, int width, const double2 *gh,
-                                             const float *w, const float *wr, const RefPatch &patch, int taps,
+                                             const float2 *wt, const RefPatch &patch, int taps,
                                              double hdx, double hdy, bool &ok) {
     float st = 0.0f, stt = 0.0f, srt = 0.0f;
 #pragma unroll 9
@@ -308,10 +311,11 @@ __device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, i
         float top = q.x * (1.0f - tx) + q.y * tx;
         float bottom = q.z * (1.0f - tx) + q.w * tx;
         float tv = top * (1.0f - ty) + bottom * ty;
-        float wt = w[t] * tv;
-        st += wt;
-        stt += wt * tv;
-        srt += wr[t] * tv;
+        const float2 weights = wt[t];
+        float wv = weights.x * tv;
+        st += wv;
+        stt += wv * tv;
+        srt += weights.y * tv;
     }
     float covariance = srt - patch.sum_r * st / patch.count;
     float target_energy = stt - st * st / patch.count;
@@ -322,15 +326,15 @@ __device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, i
 
 // Either path, bit-identical to warped_patch_zncc: fast when the box is inside,
 // exact per-tap checks otherwise. gh: g/2 per tap.
-__device__ __forceinline__ bool zncc_any(const TargetRef &target, const double2 *gh, const TapBox &box, const float *w, const float *wr, const RefPatch &patch,
+__device__ __forceinline__ bool zncc_any(const TargetRef &target, const double2 *gh, const TapBox &box, const float2 *wt, const RefPatch &patch,
                                          int taps, double ddx, double ddy, float &score) {
     double hdx = ddx * 0.5, hdy = ddy * 0.5;
     if (taps_inside(box, hdx, hdy, target.plane.width, target.plane.height)) {
         bool ok;
-        score = zncc_inside(target.quads, target.plane.width, gh, w, wr, patch, taps, hdx, hdy, ok);
+        score = zncc_inside(target.quads, target.plane.width, gh, wt, patch, taps, hdx, hdy, ok);
         return ok;
     }
-    return zncc_score(target.plane, gh, w, wr, patch, taps, ddx, ddy, score);
+    return zncc_score(target.plane, gh, wt, patch, taps, ddx, ddy, score);
 }
 
 // aggregate (depth.rs:1761-1770) over up to MAX_VIEWS scores (NaN = None).
