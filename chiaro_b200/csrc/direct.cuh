@@ -102,12 +102,14 @@ struct DirectParams {
     int4 *wide_list;                                   // (node, first, last, seeded)
 };
 
-// Per-warp shared memory of the direct pass for V targets and T taps.
+// Per-warp shared memory of the direct pass for V targets and T taps; TapT
+// is the tap-position storage (double2 g/2 or float2 g).
+template <typename TapT>
 struct DirectSlot {
     float *rr;             // [T] (w r) r
     float2 *wt;            // [T] (w, w r)
     ViewGeom *geom;        // [V]
-    double2 *gh;           // [V][T] g/2 (fast path)
+    TapT *gh;              // [V][T] tap positions
     TapBox *box;           // [V]
     double *cand;          // [32]
     float *items;          // [33][V]
@@ -115,17 +117,19 @@ struct DirectSlot {
     unsigned short *list;  // [33][V] scored items: fast path from the front, exact path from the back
 };
 
+template <typename TapT>
 __host__ __device__ inline size_t direct_slot_bytes(int V, int taps) {
     return align16(taps * sizeof(float)) + align16(taps * sizeof(float2)) + align16(V * sizeof(ViewGeom)) +
-           align16((size_t)V * taps * sizeof(double2)) + align16(V * sizeof(TapBox)) +
+           align16((size_t)V * taps * sizeof(TapT)) + align16(V * sizeof(TapBox)) +
            align16(MAX_DIRECT_CANDIDATES * sizeof(double)) +
            align16((size_t)(MAX_DIRECT_CANDIDATES + 1) * V * sizeof(float)) +
            align16((MAX_DIRECT_CANDIDATES + 1) * sizeof(float)) +
            align16((size_t)(MAX_DIRECT_CANDIDATES + 1) * V * sizeof(unsigned short));
 }
 
-__device__ inline DirectSlot carve_direct_slot(unsigned char *base, int V, int taps) {
-    DirectSlot d;
+template <typename TapT>
+__device__ inline DirectSlot<TapT> carve_direct_slot(unsigned char *base, int V, int taps) {
+    DirectSlot<TapT> d;
     size_t o = 0;
     d.rr = reinterpret_cast<float *>(base);
     o += align16(taps * sizeof(float));
@@ -133,8 +137,8 @@ __device__ inline DirectSlot carve_direct_slot(unsigned char *base, int V, int t
     o += align16(taps * sizeof(float2));
     d.geom = reinterpret_cast<ViewGeom *>(base + o);
     o += align16(V * sizeof(ViewGeom));
-    d.gh = reinterpret_cast<double2 *>(base + o);
-    o += align16((size_t)V * taps * sizeof(double2));
+    d.gh = reinterpret_cast<TapT *>(base + o);
+    o += align16((size_t)V * taps * sizeof(TapT));
     d.box = reinterpret_cast<TapBox *>(base + o);
     o += align16(V * sizeof(TapBox));
     d.cand = reinterpret_cast<double *>(base + o);
@@ -190,7 +194,8 @@ __device__ inline int warp_direct_candidates(const DirectParams &p, double cx, d
 
 // Warp-cooperative: reference patch and every target's tap positions for one
 // node at `radius` (warp_stage_patch); geometry from the records.
-__device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot &d, RefPatch &patch, double cx,
+template <typename TapT>
+__device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot<TapT> &d, RefPatch &patch, double cx,
                                        double cy, int radius, const float *spatial, const GeomRec *recs) {
     const int lane = threadIdx.x & 31;
     const int V = p.n_targets;
@@ -209,7 +214,8 @@ __device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot &
 // settles which items reach the correlation and whether their taps are all
 // inside (the fast path), and lists them fast-first; the correlations then run
 // over that list, so lanes idle only in the last round.
-__device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlot &d, const RefPatch &patch,
+template <typename TapT>
+__device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlot<TapT> &d, const RefPatch &patch,
                                           const double *cand, int n, int radius) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -275,7 +281,8 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
     if (slot >= p.nodes_per_cta || node >= p.columns * p.rows) return;  // whole warps
     const int V = p.n_targets;
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
-    DirectSlot d = carve_direct_slot(smem_raw + (size_t)slot * direct_slot_bytes(V, taps), V, taps);
+    DirectSlot<double2> d =
+        carve_direct_slot<double2>(smem_raw + (size_t)slot * direct_slot_bytes<double2>(V, taps), V, taps);
     RefPatch &patch = patches[slot];
     const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
     int seeded;
@@ -308,14 +315,16 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
 }
 
 // The wide-radius retry (depth.rs:803-846) for the listed nodes; a warp per
-// entry, persistent over the list.
+// entry, persistent over the list. Its 225-tap positions are kept as f32 g,
+// which halves their shared memory and lets more warps stay resident.
 __global__ void __launch_bounds__(128) direct_wide_kernel(DirectParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patches[4];
     const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int V = p.n_targets;
     const int taps = (2 * p.wide_radius + 1) * (2 * p.wide_radius + 1);
-    DirectSlot d = carve_direct_slot(smem_raw + (size_t)slot * direct_slot_bytes(V, taps), V, taps);
+    DirectSlot<float2> d =
+        carve_direct_slot<float2>(smem_raw + (size_t)slot * direct_slot_bytes<float2>(V, taps), V, taps);
     RefPatch &patch = patches[slot];
     const int count = *p.wide_count;
     for (int e = blockIdx.x * 4 + slot; e < count; e += gridDim.x * 4) {

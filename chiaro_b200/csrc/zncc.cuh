@@ -43,16 +43,36 @@ __device__ __forceinline__ void tap_offset(int t, int radius, int &dx, int &dy) 
     dx = t % side - radius;
 }
 
+// Tap positions are kept either as g/2 in f64 (double2: one 16-byte load per
+// tap on the fast path) or as g in f32 (float2: half the shared memory, halved
+// to f64 at use). g is f32 and halving is exact in f64, so both give the same
+// bits everywhere.
+__device__ __forceinline__ double2 tap_half(const double2 &v) { return v; }
+__device__ __forceinline__ double2 tap_half(const float2 &v) {
+    return make_double2((double)v.x * 0.5, (double)v.y * 0.5);
+}
+__device__ __forceinline__ float2 tap_g(const double2 &v) {
+    return make_float2((float)(v.x * 2.0), (float)(v.y * 2.0));
+}
+__device__ __forceinline__ float2 tap_g(const float2 &v) { return v; }
+__device__ __forceinline__ void store_tap(double2 &d, float qx, float qy) {
+    d = make_double2((double)qx * 0.5, (double)qy * 0.5);
+}
+__device__ __forceinline__ void store_tap(float2 &d, float qx, float qy) { d = make_float2(qx, qy); }
+
 // Bounding box of g/2 over one target's taps, computed by an aligned group of
 // eight lanes (min and max are exact, so the reduction order does not matter).
 // Every lane of the warp calls it; the groups reduce with shuffles.
-__device__ inline TapBox group8_tap_box(const double2 *gh, int taps) {
-    TapBox b{gh[0].x, gh[0].x, gh[0].y, gh[0].y};
+template <typename TapT>
+__device__ inline TapBox group8_tap_box(const TapT *gh, int taps) {
+    const double2 g0 = tap_half(gh[0]);
+    TapBox b{g0.x, g0.x, g0.y, g0.y};
     for (int t = threadIdx.x & 7; t < taps; t += 8) {
-        b.xmin = fmin(b.xmin, gh[t].x);
-        b.xmax = fmax(b.xmax, gh[t].x);
-        b.ymin = fmin(b.ymin, gh[t].y);
-        b.ymax = fmax(b.ymax, gh[t].y);
+        const double2 g = tap_half(gh[t]);
+        b.xmin = fmin(b.xmin, g.x);
+        b.xmax = fmax(b.xmax, g.x);
+        b.ymin = fmin(b.ymin, g.y);
+        b.ymax = fmax(b.ymax, g.y);
     }
 #pragma unroll
     for (int off = 4; off > 0; off >>= 1) {
@@ -87,9 +107,10 @@ __device__ inline void store_reference_sum(RefPatch &patch, int which, float sum
 // on every lane the mask of targets with a tap where the global warp is None
 // (bit v); `patch` is written by lanes 0-2 and valid after the trailing
 // __syncwarp().
+template <typename TapT>
 __device__ inline unsigned warp_stage_patch(const DevView *views, int reference, const int *targets, int V,
                                             double cx, double cy, int radius, const float *spatial, float *rr,
-                                            float2 *wt, double2 *gh, TapBox *box, RefPatch &patch) {
+                                            float2 *wt, TapT *gh, TapBox *box, RefPatch &patch) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int taps = (2 * radius + 1) * (2 * radius + 1);
@@ -111,7 +132,7 @@ __device__ inline unsigned warp_stage_patch(const DevView *views, int reference,
         for (int v = 0; v < V; ++v) {
             float qx = 0.0f, qy = 0.0f;
             if (!warp_map(views[targets[v]].warp, (float)px, (float)py, qx, qy)) undefined |= 1u << v;
-            gh[v * taps + t] = make_double2((double)qx * 0.5, (double)qy * 0.5);
+            store_tap(gh[v * taps + t], qx, qy);
         }
     }
     undefined = __reduce_or_sync(full, undefined);
@@ -234,12 +255,12 @@ __device__ __forceinline__ bool depth_delta(const DevCamera &tc, const ViewGeom 
 
 // Hypothesis-dependent part of warped_patch_zncc: sample the target at every
 // tap shifted by (ddx, ddy) and finish the correlation. False for None.
-__device__ __forceinline__ bool zncc_score(const PlaneRef &target, const double2 *gh, const float2 *wt,
+template <typename TapT>
+__device__ __forceinline__ bool zncc_score(const PlaneRef &target, const TapT *gh, const float2 *wt,
                                            const RefPatch &patch, int taps, double ddx, double ddy, float &score) {
     float st = 0.0f, stt = 0.0f, srt = 0.0f;
     for (int t = 0; t < taps; ++t) {
-        // the tap's global-warp position, stored halved; doubling is exact
-        const float2 g = make_float2((float)(gh[t].x * 2.0), (float)(gh[t].y * 2.0));
+        const float2 g = tap_g(gh[t]);  // the tap's global-warp position
         double qx = (double)g.x + ddx;
         double qy = (double)g.y + ddy;
         float tv;
@@ -296,13 +317,14 @@ __device__ __forceinline__ bool taps_inside(const TapBox &box, double hdx, doubl
 
 // warped_patch_zncc's hypothesis-dependent part for taps known to be inside
 // (see taps_inside). gh holds g/2 per tap.
-__device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, int width, const double2 *gh,
+template <typename TapT>
+__device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, int width, const TapT *gh,
                                              const float2 *wt, const RefPatch &patch, int taps,
                                              double hdx, double hdy, bool &ok) {
     float st = 0.0f, stt = 0.0f, srt = 0.0f;
 #pragma unroll 9
     for (int t = 0; t < taps; ++t) {
-        double2 g = gh[t];
+        const double2 g = tap_half(gh[t]);
         float x = (float)((g.x + hdx) - 0.25);
         float y = (float)((g.y + hdy) - 0.25);
         int ix, iy;
@@ -326,7 +348,8 @@ __device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, i
 
 // Either path, bit-identical to warped_patch_zncc: fast when the box is inside,
 // exact per-tap checks otherwise. gh: g/2 per tap.
-__device__ __forceinline__ bool zncc_any(const TargetRef &target, const double2 *gh, const TapBox &box, const float2 *wt, const RefPatch &patch,
+template <typename TapT>
+__device__ __forceinline__ bool zncc_any(const TargetRef &target, const TapT *gh, const TapBox &box, const float2 *wt, const RefPatch &patch,
                                          int taps, double ddx, double ddy, float &score) {
     double hdx = ddx * 0.5, hdy = ddy * 0.5;
     if (taps_inside(box, hdx, hdy, target.plane.width, target.plane.height)) {
