@@ -281,8 +281,8 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
     if (slot >= p.nodes_per_cta || node >= p.columns * p.rows) return;  // whole warps
     const int V = p.n_targets;
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
-    DirectSlot<double2> d =
-        carve_direct_slot<double2>(smem_raw + (size_t)slot * direct_slot_bytes<double2>(V, taps), V, taps);
+    DirectSlot<float2> d =
+        carve_direct_slot<float2>(smem_raw + (size_t)slot * direct_slot_bytes<float2>(V, taps), V, taps);
     RefPatch &patch = patches[slot];
     const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
     int seeded;

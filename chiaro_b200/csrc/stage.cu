@@ -499,7 +499,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         CK(cudaMemsetAsync(p.wide_count, 0, sizeof(int), s));
         const int taps = (2 * direct_radius + 1) * (2 * direct_radius + 1);
         const int wide_taps = (2 * wide_radius + 1) * (2 * wide_radius + 1);
-        const size_t slot = direct_slot_bytes<double2>(V, taps), wide_slot = direct_slot_bytes<float2>(V, wide_taps);
+        const size_t slot = direct_slot_bytes<float2>(V, taps), wide_slot = direct_slot_bytes<float2>(V, wide_taps);
         if (slot > 200 * 1024 || 4 * wide_slot > 200 * 1024)
             throw CudaError{cudaErrorInvalidValue, "direct pass shared memory exceeds 200 KiB"};
         p.nodes_per_cta = warps_per_cta(direct_depth_kernel, slot, 8);
