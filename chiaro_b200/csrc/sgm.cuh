@@ -41,18 +41,24 @@ __device__ inline void sgm_path(int family, int p, int columns, int rows, int &r
     }
 }
 
-// One launch per direction, in the reference's order, so each node receives
-// 0 + L1, then + L2, ..., + L8 exactly as depth.rs:1287-1309 adds them.
+// All eight directions run in one launch, each path writing its own path
+// costs L_k into buffer k; a second kernel then forms, per cell,
+// ((0 + L1) + L2) + ... + L8 in the reference's order (depth.rs:1287-1309), so
+// the sum is bit-identical to the reference's in-place accumulation while the
+// GPU walks every path of every direction at once.
 //
-// A path is walked by K warps, one per 32-label chunk (K = ceil(labels / 32)),
-// so each warp handles one label per lane per step. Per step, each warp takes
-// its chunk's minimum with redux.sync.min.f32, publishes it together with its
-// first and last label values in shared memory, and after the path's named
-// barrier reads the other chunks' minima (min is exact, so the combination
-// order does not matter) and its neighbours across the chunk boundary. The
-// exchange buffers alternate between steps, so one barrier per step suffices.
-// Each warp prefetches its chunk of the cost and output vectors P steps ahead.
-constexpr int SGM_PREFETCH = 8;
+// A path is walked by one warp. Lane i holds labels i, i + 32, ..., i + 32 (K - 1)
+// (K = ceil(labels / 32) sets), so the step's minimum is a local min and one
+// redux.sync.min.f32, and the label neighbours come from two shuffles per set:
+// the neighbour below lane 0 of set k is lane 31 of set k - 1, the one above
+// lane 31 of set k is lane 0 of set k + 1. No shared memory and no barrier sit
+// on the step's critical path. The penalties p1, p2 depend only on the guidance
+// along the path: lane j computes those of step base + j once per 32 steps and
+// each step reads them by shuffle. Labels past the last one carry +inf data,
+// which keeps them at +inf without a select. The data is prefetched P steps
+// ahead.
+constexpr int SGM_PREFETCH = 4;
+constexpr int SGM_PATHS_PER_CTA = 4;
 
 __device__ __forceinline__ float warp_min_f32(float v) {
     float r;
@@ -60,99 +66,130 @@ __device__ __forceinline__ float warp_min_f32(float v) {
     return r;
 }
 
-__device__ __forceinline__ void path_barrier(int threads) {
-    asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
+// Paths of the launch: for each family (rows, columns, down-right, down-left)
+// its forward paths, then its reverse paths. Pass = 2 * family + reverse is
+// the reference's summation order.
+__host__ __device__ inline unsigned sgm_total_paths(int columns, int rows) {
+    return 2u * (unsigned)(rows + columns + 2 * (columns + rows - 1));
 }
 
-// One direction of one family: every block walks one path, forward or in
-// reverse, adding its costs to `out` (`first` stores 0 + L).
+__device__ inline void sgm_path_of(int b, int columns, int rows, int &pass, int &path) {
+    for (int family = 0; family < 4; ++family) {
+        const int n = sgm_path_count(family, columns, rows);
+        if (b < 2 * n) {
+            pass = 2 * family + (b >= n ? 1 : 0);
+            path = b >= n ? b - n : b;
+            return;
+        }
+        b -= 2 * n;
+    }
+    pass = 0;
+    path = 0;
+}
+
+// Path costs of every path of every direction; pass k writes paths + k * pitch.
 template <int K>
-__global__ void __launch_bounds__(32 * K, 4) sgm_direction_kernel(const float *__restrict__ data,
-                                                                 const float *__restrict__ guidance, float *out,
-                                                                 int columns, int rows, int labels, int family,
-                                                                 int first, int reverse) {
-    __shared__ float xmin[2][K], xfirst[2][K], xlast[2][K];
+__global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_paths_kernel(const float *__restrict__ data,
+                                                                          const float *__restrict__ guidance,
+                                                                          float *__restrict__ paths, size_t pitch,
+                                                                          int columns, int rows, int labels) {
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int chunk = threadIdx.x >> 5;
+    const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
+    if (warp_path >= (int)sgm_total_paths(columns, rows)) return;  // whole warp
+    int pass, path;
+    sgm_path_of(warp_path, columns, rows, pass, path);
     int r0, c0, dr, dc, len;
-    sgm_path(family, blockIdx.x, columns, rows, r0, c0, dr, dc, len);
-    if (reverse) {
+    sgm_path(pass >> 1, path, columns, rows, r0, c0, dr, dc, len);
+    if (pass & 1) {
         r0 += dr * (len - 1);
         c0 += dc * (len - 1);
         dr = -dr;
         dc = -dc;
     }
     constexpr int P = SGM_PREFETCH;
-    const int l = chunk * 32 + lane;
-    const bool valid = l < labels;
-    const bool fold = !first;  // out = first ? 0 + L : out + L
+    bool valid[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) valid[k] = lane + 32 * k < labels;
     const long node_step = (long)dr * columns + dc;
     const long stride = node_step * labels;
     const int node0 = r0 * columns + c0;
-    const size_t e0 = (size_t)node0 * labels + l;
-    const float *dp = data + e0;
-    float *wp = out + e0;
-    const float *op = out + e0;
+    const size_t e0 = (size_t)node0 * labels + lane;
+    const float *pf = data + e0;                      // data of step + P (after the ring fill)
+    float *wp = paths + (size_t)pass * pitch + e0;    // path costs of the current step
     const float *gp = guidance + node0;
-    float prev;
-    {
-        float c = valid ? __ldg(dp) : 0.0f;
-        float b = valid && fold ? __ldcg(op) : 0.0f;
-        prev = valid ? c : INFINITY;
-        if (valid) *wp = fold ? b + c : 0.0f + c;
+    float prev[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        prev[k] = valid[k] ? __ldg(pf + 32 * k) : INFINITY;
+        if (valid[k]) wp[32 * k] = prev[k];
     }
-    float g_prev = __ldg(gp);
-    float ring_c[P], ring_o[P], ring_g[P];
+    float ring[P][K];
 #pragma unroll
     for (int j = 0; j < P; ++j) {
-        if (1 + j < len) {
-            ring_c[j] = valid ? __ldg(dp + (1 + j) * stride) : 0.0f;
-            ring_o[j] = valid && fold ? __ldcg(op + (1 + j) * stride) : 0.0f;
-            ring_g[j] = __ldg(gp + (1 + j) * node_step);
+        pf += stride;
+#pragma unroll
+        for (int k = 0; k < K; ++k) ring[j][k] = valid[k] && 1 + j < len ? __ldg(pf + 32 * k) : INFINITY;
+    }
+    float p1s = 0.0f, p2s = 0.0f;
+    for (int base = 1; base < len; base += 32) {
+        {  // lane j: penalties of step base + j (depth.rs:1358-1361)
+            const int s = base + lane;
+            if (s < len) {
+                const float g = __ldg(gp + s * node_step), g_prev = __ldg(gp + (s - 1) * node_step);
+                const float edge_scale = __frcp_rn(1.0f + 4.0f * fabsf(g - g_prev));  // == 1 / x, correctly rounded
+                p1s = SGM_SMALL_PENALTY * fmaxf(edge_scale, 0.35f);
+                p2s = SGM_LARGE_PENALTY * fmaxf(edge_scale, 0.12f);
+            }
+        }
+        for (int jj = 0; jj < 32; jj += P) {
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                const int step = base + jj + j;
+                if (step >= len) break;  // uniform over the warp
+                float cur[K];
+                pf += stride;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    cur[k] = ring[j][k];
+                    ring[j][k] = valid[k] && step + P < len ? __ldg(pf + 32 * k) : INFINITY;
+                }
+                const float p1 = __shfl_sync(full, p1s, jj + j), p2 = __shfl_sync(full, p2s, jj + j);
+                float local = prev[0];
+#pragma unroll
+                for (int k = 1; k < K; ++k) local = fminf(local, prev[k]);
+                const float minimum_previous = warp_min_f32(local);
+                float up[K], down[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    up[k] = __shfl_sync(full, prev[k], (lane + 31) & 31);   // label - 1 (lane 0: set k - 1's last)
+                    down[k] = __shfl_sync(full, prev[k], (lane + 1) & 31);  // label + 1 (lane 31: set k + 1's first)
+                }
+                const float jump = minimum_previous + p2;
+                wp += stride;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float below = lane == 0 ? (k > 0 ? up[k > 0 ? k - 1 : 0] : INFINITY) : up[k];
+                    const float above = lane == 31 ? (k + 1 < K ? down[k + 1 < K ? k + 1 : k] : INFINITY) : down[k];
+                    const float v =
+                        cur[k] + fminf(fminf(fminf(prev[k], below + p1), above + p1), jump) - minimum_previous;
+                    prev[k] = v;
+                    if (valid[k]) wp[32 * k] = v;
+                }
+            }
         }
     }
-    int parity = 0;
-    for (int base = 1; base < len; base += P) {
+}
+
+// out = ((0 + L1) + L2) + ... + L8 per cell, the reference's order.
+__global__ void sgm_sum_kernel(const float *__restrict__ paths, size_t pitch, size_t total,
+                               float *__restrict__ out) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        float s = 0.0f;
 #pragma unroll
-        for (int j = 0; j < P; ++j) {
-            const int step = base + j;
-            if (step >= len) break;  // uniform across the path's warps
-            wp += stride;
-            const float cur_data = ring_c[j], cur_base = ring_o[j], g = ring_g[j];
-            if (step + P < len) {
-                ring_c[j] = valid ? __ldg(dp + (step + P) * stride) : 0.0f;
-                ring_o[j] = valid && fold ? __ldcg(op + (step + P) * stride) : 0.0f;
-                ring_g[j] = __ldg(gp + (step + P) * node_step);
-            }
-            // publish this chunk's minimum and boundary labels, then combine
-            const float chunk_min = warp_min_f32(prev);
-            if (lane == 0) {
-                xmin[parity][chunk] = chunk_min;
-                xfirst[parity][chunk] = prev;
-            }
-            if (lane == 31) xlast[parity][chunk] = prev;
-            const float rot_up = __shfl_sync(0xffffffffu, prev, (lane + 31) & 31);
-            const float rot_down = __shfl_sync(0xffffffffu, prev, (lane + 1) & 31);
-            const float edge = fabsf(g - g_prev);
-            g_prev = g;
-            const float edge_scale = __frcp_rn(1.0f + 4.0f * edge);  // == 1 / x, correctly rounded
-            const float p1 = SGM_SMALL_PENALTY * fmaxf(edge_scale, 0.35f);
-            const float p2 = SGM_LARGE_PENALTY * fmaxf(edge_scale, 0.12f);
-            if (K > 1) path_barrier(32 * K);
-            float minimum_previous = K > 1 ? xmin[parity][0] : chunk_min;
-#pragma unroll
-            for (int k = 1; k < K; ++k) minimum_previous = fminf(minimum_previous, xmin[parity][k]);
-            float below = rot_up, above = rot_down;
-            if (lane == 0) below = chunk > 0 ? xlast[parity][chunk > 0 ? chunk - 1 : 0] : INFINITY;
-            if (lane == 31) above = chunk + 1 < K ? xfirst[parity][chunk + 1 < K ? chunk + 1 : chunk] : INFINITY;
-            parity ^= 1;
-            const float jump = minimum_previous + p2;
-            const float lower = below + p1;  // INFINITY + p1 = INFINITY
-            const float higher = l + 1 < labels ? above + p1 : INFINITY;
-            const float v = cur_data + fminf(fminf(fminf(prev, lower), higher), jump) - minimum_previous;
-            prev = valid ? v : INFINITY;
-            if (valid) *wp = fold ? cur_base + v : 0.0f + v;
-        }
+        for (int k = 0; k < 8; ++k) s = s + __ldcs(paths + k * pitch + i);
+        out[i] = s;
     }
 }
 

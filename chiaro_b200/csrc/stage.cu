@@ -182,35 +182,33 @@ void launch_geometry(chiaro_depth_ctx *ctx, const DevView *d_views, int referenc
 
 // ---- SGM ---------------------------------------------------------------------------
 template <int K>
-void sgm_pass(chiaro_depth_ctx *ctx, unsigned blocks, const float *data, const float *guidance, float *out,
-              int columns, int rows, int labels, int family, int first, int reverse) {
-    sgm_direction_kernel<K><<<blocks, 32 * K, 0, ctx->stream>>>(data, guidance, out, columns, rows, labels, family,
-                                                                first, reverse);
+void sgm_paths(chiaro_depth_ctx *ctx, const float *data, const float *guidance, float *paths, size_t pitch,
+               int columns, int rows, int labels) {
+    const unsigned blocks = (unsigned)div_ceil(sgm_total_paths(columns, rows), SGM_PATHS_PER_CTA);
+    sgm_paths_kernel<K><<<blocks, 32 * SGM_PATHS_PER_CTA, 0, ctx->stream>>>(data, guidance, paths, pitch, columns,
+                                                                            rows, labels);
     CK(cudaGetLastError());
 }
 
-void sgm_dispatch(chiaro_depth_ctx *ctx, int K, unsigned blocks, const float *data, const float *guidance,
-                  float *out, int columns, int rows, int labels, int family, int first, int reverse) {
+// Every direction's path costs in one launch, then their ordered sum (sgm.cuh).
+void launch_sgm(chiaro_depth_ctx *ctx, const float *data, const float *guidance, float *out, int columns, int rows,
+                int labels) {
+    const int K = (labels + 31) / 32;  // label sets per lane
+    const size_t total = (size_t)columns * rows * labels;
+    const size_t pitch = (total + 63) / 64 * 64;
+    float *paths = dbuf<float>(ctx, "sgm_paths", 8 * pitch);
     switch (K) {
-#define SGM_CASE(k)                                                                                              \
-    case k:                                                                                                      \
-        return sgm_pass<k>(ctx, blocks, data, guidance, out, columns, rows, labels, family, first, reverse);
+#define SGM_CASE(k)                                                         \
+    case k:                                                                 \
+        sgm_paths<k>(ctx, data, guidance, paths, pitch, columns, rows, labels); \
+        break;
         SGM_CASE(1) SGM_CASE(2) SGM_CASE(3) SGM_CASE(4) SGM_CASE(5) SGM_CASE(6) SGM_CASE(7) SGM_CASE(8)
 #undef SGM_CASE
         default: throw CudaError{cudaErrorInvalidValue, "labels exceed 256"};
     }
-}
-
-// One launch per direction, in the reference's summation order (sgm.cuh).
-void launch_sgm(chiaro_depth_ctx *ctx, const float *data, const float *guidance, float *out, int columns, int rows,
-                int labels) {
-    const int K = (labels + 31) / 32;  // warps per path
-    const int order[4] = {SGM_ROWS, SGM_COLUMNS, SGM_DOWN_RIGHT, SGM_DOWN_LEFT};
-    for (int pass = 0; pass < 8; ++pass) {
-        const int f = order[pass / 2];
-        sgm_dispatch(ctx, K, (unsigned)sgm_path_count(f, columns, rows), data, guidance, out, columns, rows, labels,
-                     f, pass == 0, pass % 2);
-    }
+    const unsigned blocks = (unsigned)std::min<size_t>(div_ceil(total, 256), (size_t)ctx->sm_count * 16);
+    sgm_sum_kernel<<<blocks, 256, 0, ctx->stream>>>(paths, pitch, total, out);
+    CK(cudaGetLastError());
 }
 
 // ---- the stage ------------------------------------------------------------------------
@@ -616,9 +614,9 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->events[6], s));
-    // quad planes 1 per target, geometry 2, cost 1, SGM 8, select 1, completion, direct 2, filters 6, stats 2,
+    // quad planes 1 per target, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
     // decisions 1 + 3 per target, map 1
-    ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 8 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
+    ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
     CK(cudaMemcpyAsync(&h_results, d_results, sizeof(Results), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ctx->timings[i], ctx->events[i], ctx->events[i + 1]));

@@ -53,7 +53,8 @@ def cpu():
 
 
 @pytest.mark.parametrize("columns,rows,labels", [(1, 1, 3), (5, 1, 4), (1, 7, 33), (13, 9, 65), (40, 31, 97),
-                                                 (31, 40, 129), (17, 23, 193), (9, 5, 256)])
+                                                 (31, 40, 129), (17, 23, 193), (9, 5, 256),
+                                                 (70, 3, 40), (2, 75, 129)])
 def test_sgm_bit_exact(gpu, cpu, columns, rows, labels):
     rng = np.random.default_rng(columns * 1000 + rows * 10 + labels)
     costs = rng.uniform(0, 2.25, columns * rows * labels).astype(np.float32)
