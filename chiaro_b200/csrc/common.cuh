@@ -179,18 +179,12 @@ CH_HD double exp_f64(double x) {
     return fma_d(scale, tmp, scale);
 }
 
-// floor(x) as an int and x - floor(x) for 0 <= x < 2^22, without the
-// conversion pipe: adding 2^23 rounds x to the nearest integer (its value is
-// in the low mantissa bits), and one compare corrects round-up to floor. All
-// steps are exact in that range.
+// floor(x) as an int and x - floor(x) for 0 <= x < 2^22 without a
+// float-to-int conversion: r = floor(x) is an integer below 2^22, so r + 2^23
+// is exact and holds r in its low mantissa bits; x - r is exact.
 CH_HD float floor_frac_small(float x, int &ix) {
-    const float magic = 8388608.0f;  // 2^23
-    float t = x + magic;
-    float r = t - magic;  // nearest integer to x
-    int i = (int)(f2u(t) - 0x4B000000u);
-    bool up = r > x;
-    ix = up ? i - 1 : i;
-    r = up ? r - 1.0f : r;
+    const float r = floorf(x);
+    ix = (int)(f2u(r + 8388608.0f) - 0x4B000000u);  // 2^23
     return x - r;
 }
 
