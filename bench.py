@@ -119,14 +119,29 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+def sgm_traffic():
+    """DRAM bytes of one SGM stage call on five_view from the committed ncu capture, or None."""
+    import re
+    f = ROOT / "profiles" / "sgm_five_view_dram.md"
+    if not f.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_call = (\d+)", f.read_text())
+    return int(m.group(1)) if m else None
+
+
 def stage_bytes(scene):
     """Algorithmic work per step: SGM compulsory bytes and SGM cells."""
     from chiaro_b200.depth import output_shape
     (cols, rows, step), (cc, cr, cs) = output_shape(scene.width, scene.height, scene.options)
     n, d = cc * cr, scene.options.planes + 1
+    targets = len(scene.cameras) - 1
+    taps = (2 * scene.options.patch_radius + 1) ** 2
     return {"coarse_nodes": n, "labels": d, "fine_nodes": cols * rows, "cells": n * d * 8,
             # read the data-cost volume once, write the aggregate once, guidance per direction
-            "sgm_bytes": n * d * 8 + 8 * n * 4}
+            "sgm_bytes": n * d * 8 + 8 * n * 4,
+            # cost build: N * D * V * (2r + 1)^2 taps at 16 FP32 FLOP per tap (3 lerps, 3 moments,
+            # coordinate and weight products)
+            "cost_taps": n * d * targets * taps, "cost_flop": 16 * n * d * targets * taps}
 
 
 def device_views(scene, torch, device):
@@ -258,6 +273,10 @@ def run_ours(args, rank, world, local):
     peaks = measured_peaks()
     sgm_s = stage_ms["sgm"] / 1e3
     achieved = work["sgm_bytes"] / sgm_s / 1e9
+    # FP32 peak of the SMs at the clock seen under load: 148 SMs x 128 lanes x 2 FLOP (FMA)
+    sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    cost_tflops = work["cost_flop"] / (stage_ms["cost_volume"] / 1e3) / 1e12
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
@@ -270,10 +289,17 @@ def run_ours(args, rank, world, local):
                    "parallelism": f"replicas x{world} (one capture per GPU, no collective)"},
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "sgm_only_gcells_s": round(work["cells"] / sgm_s / 1e9, 2),
-        "roofline": {"kernel": "SGM (8 direction launches, the metric's kernel)", "bound": "hbm",
+        "roofline": {"kernel": "SGM (sgm_paths_kernel + sgm_sum_kernel, the metric's kernel)", "bound": "hbm",
                      "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                     "frac": round(achieved / peaks["hbm_gbs"], 4),
+                     "traffic": sgm_traffic() if args.workload == "five_view" else None,
+                     "traffic_source": "profiles/sgm_five_view_dram.md (ncu dram__bytes_read + write, one call)",
                      "peak_source": peaks["source"], "algorithmic_bytes": work["sgm_bytes"]},
+        "compute_roofline": {"kernel": "cost_volume_kernel (build_cost_volume, the largest correlation kernel)",
+                             "bound": "fp32", "achieved": round(cost_tflops, 2), "peak": round(fp32_peak, 1),
+                             "unit": "TFLOP/s", "frac": round(cost_tflops / fp32_peak, 4),
+                             "flop_per_tap": 16, "taps": work["cost_taps"],
+                             "peak_source": f"148 SMs x 128 FP32 lanes x 2 FLOP at {sm_mhz:.0f} MHz"},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(1e3 * e2e_s / e2e_steps, 3),
                 "api": "chiaro_b200.depth.refine_multiview_depth (host buffers, pinned inputs)"},
