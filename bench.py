@@ -66,6 +66,23 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The maximum of `value` over all ranks (the slowest rank's time); `value` itself on one rank.
+    Every rank calls it at the same point (NCCL on the GPUs in the benchmark, gloo in the CPU tests)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, cells_per_step: int, steps: int, seconds: float) -> float:
+    """Whole-job Gcells/s: every rank processes its own replica of the workload (weak scaling)."""
+    return world * cells_per_step * steps / seconds / 1e9
+
+
 class ClockSampler:
     """nvidia-smi clock and throttle-reason samples during the timed region."""
 
@@ -234,11 +251,8 @@ def run_ours(args, rank, world, local):
         dist.barrier()
     total_ms = float(sum(durations))
     launches = ctx.launches()
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * work["cells"] * args.steps / (total_ms / 1e3) / 1e9
+    total_ms = max_over_ranks(total_ms, world, device)
+    value = whole_job_rate(world, work["cells"], args.steps, total_ms / 1e3)
     stage_ms = {k: statistics.median(s[k] for s in stages) for k in stages[0]}
 
     # end to end through the public API: pinned host inputs, host outputs
@@ -259,16 +273,12 @@ def run_ours(args, rank, world, local):
         result = refine_multiview_depth(inputs, scene.reference_index, alignments, scene.options, context=ctx)
         e2e.append(time.perf_counter() - t0)
         assert result is not None
-    e2e_s = float(sum(e2e))
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(float(sum(e2e)), world, device)
     targets = sum(1 for i in range(n) if i != scene.reference_index)
     h2d = sum(l.data.nbytes for l in scene.luminance) + sum(w.points.nbytes + w.confidence.nbytes
                                                             for w in scene.warps)
     d2h = M * (8 + 4 + 1) + targets * M * (8 + 4)
-    e2e_value = world * work["cells"] * e2e_steps / e2e_s / 1e9
+    e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
 
     peaks = measured_peaks()
     sgm_s = stage_ms["sgm"] / 1e3
