@@ -81,6 +81,16 @@ class CameraC(C.Structure):
     ]
 
 
+class VignettingC(C.Structure):
+    """VignettingMesh (calibration.rs:354-358)."""
+
+    _fields_ = [
+        ("columns", C.c_uint64),
+        ("rows", C.c_uint64),
+        ("gains", C.POINTER(C.c_float)),
+    ]
+
+
 class WarpC(C.Structure):
     """Warp (align.rs:34-45)."""
 

@@ -22,6 +22,7 @@
 #include "decisions.cuh"
 #include "direct.cuh"
 #include "filters.cuh"
+#include "luminance.cuh"
 #include "select.cuh"
 #include "sgm.cuh"
 
@@ -1069,6 +1070,75 @@ int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *gl
         download(ctx, reinterpret_cast<float2 *>(global), a.global, n);
         download(ctx, reinterpret_cast<float2 *>(point), a.point, n);
         CK(cudaStreamSynchronize(s));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+// ---- luminance_half (image.rs:401-428) -------------------------------------------------
+namespace {
+
+// Validation shared by both forms; the plane is (width / 2) x (height / 2).
+int luminance_args(const uint16_t *samples, uint64_t width, uint64_t height, const chiaro_vignetting *mesh,
+                   const float *out, bool device) {
+    if (!samples || !out || width > (1u << 30) || height > (1u << 30)) return CHIARO_ERR_ARGUMENT;
+    if (device && reinterpret_cast<uintptr_t>(samples) % 2 != 0) return CHIARO_ERR_ARGUMENT;
+    if (mesh && mesh->columns >= 2 && mesh->rows >= 2 && !mesh->gains) return CHIARO_ERR_ARGUMENT;
+    if (mesh && (mesh->columns > (1u << 20) || mesh->rows > (1u << 20))) return CHIARO_ERR_ARGUMENT;
+    return CHIARO_OK;
+}
+
+void launch_luminance(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64_t width, uint64_t height,
+                      float black_q6, float white_q6, VignettingRef mesh, float *out) {
+    const size_t n = (size_t)(width / 2) * (height / 2);
+    if (n == 0) return;
+    const unsigned blocks = (unsigned)std::min<size_t>(div_ceil(n, 256), (size_t)ctx->sm_count * 16);
+    luminance_half_kernel<<<blocks, 256, 0, ctx->stream>>>(samples, (int)width, (int)height, black_q6, white_q6,
+                                                          mesh, out);
+    CK(cudaGetLastError());
+}
+
+}  // namespace
+
+int chiaro_luminance_half_device(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64_t width, uint64_t height,
+                                 float black_q6, float white_q6, const chiaro_vignetting *mesh, float *out) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    if (int st = luminance_args(samples, width, height, mesh, out, true)) return st;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        VignettingRef m{nullptr, 0, 0};
+        if (mesh && mesh->columns >= 2 && mesh->rows >= 2)
+            m = VignettingRef{mesh->gains, (int)mesh->columns, (int)mesh->rows};
+        launch_luminance(ctx, samples, width, height, black_q6, white_q6, m, out);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_luminance_half(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64_t width, uint64_t height,
+                          float black_q6, float white_q6, const chiaro_vignetting *mesh, float *out) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    if (int st = luminance_args(samples, width, height, mesh, out, false)) return st;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        const size_t n_in = (size_t)width * height, n_out = (size_t)(width / 2) * (height / 2);
+        if (n_out == 0) return CHIARO_OK;
+        uint16_t *ds = dbuf<uint16_t>(ctx, "lum.samples", n_in);
+        float *dout = dbuf<float>(ctx, "lum.out", n_out);
+        upload(ctx, ds, samples, n_in);
+        VignettingRef m{nullptr, 0, 0};
+        if (mesh && mesh->columns >= 2 && mesh->rows >= 2) {
+            const size_t ng = (size_t)mesh->columns * mesh->rows;
+            float *dg = dbuf<float>(ctx, "lum.gains", ng);
+            upload(ctx, dg, mesh->gains, ng);
+            m = VignettingRef{dg, (int)mesh->columns, (int)mesh->rows};
+        }
+        launch_luminance(ctx, ds, width, height, black_q6, white_q6, m, dout);
+        download(ctx, out, dout, n_out);
+        CK(cudaStreamSynchronize(ctx->stream));
     } catch (const CudaError &e) {
         return fail(ctx, e);
     }

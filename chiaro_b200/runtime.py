@@ -37,6 +37,10 @@ SIGNATURES = {
     "chiaro_depth_last_timings": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int]),
     "chiaro_depth_last_launches": (C.c_int, [C.c_void_p]),
     "chiaro_depth_ctx_stream": (C.c_void_p, [C.c_void_p]),
+    "chiaro_luminance_half": (C.c_int, [C.c_void_p, P(C.c_uint16), C.c_uint64, C.c_uint64, C.c_float, C.c_float,
+                                        P(abi.VignettingC), P(C.c_float)]),
+    "chiaro_luminance_half_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_float,
+                                               C.c_float, P(abi.VignettingC), C.c_void_p]),
     "chiaro_sgm_aggregate": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_uint64, C.c_uint64, C.c_uint64,
                                        P(C.c_float)]),
     "chiaro_sgm_aggregate_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,

@@ -304,6 +304,32 @@ int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *gl
                                  const float *guidance, uint64_t columns,
                                  uint64_t rows, int consensus, int boundaries);
 
+/* ---- input plane --------------------------------------------------------- */
+
+/* VignettingMesh (calibration.rs:354-358): a columns x rows grid of flat-field
+ * gains over the sensor raster, row-major. columns or rows below 2 (or a NULL
+ * mesh) means flat field 1 (Mosaic::flat_field, image.rs:145-150). */
+typedef struct chiaro_vignetting {
+    uint64_t columns, rows;
+    const float *gains;
+} chiaro_vignetting;
+
+/* Mosaic::luminance_half (image.rs:401-428): the width x height u16 Q6 mosaic
+ * (row-major, calibration raster) becomes the (width / 2) x (height / 2) f32
+ * plane ln(1 + 1000 * linear), linear = max((mean of the 2x2 cell - black_q6) /
+ * max(white_q6 - black_q6, 1), 0) * flat_field(2i + 0.5, 2j + 0.5), ready to be
+ * a chiaro_view's luminance. Everything before the log is the reference's f32
+ * arithmetic bit for bit; the log is the correctly rounded one (f64 log rounded
+ * to f32), within 1 ulp of the host logf the reference calls. The _device
+ * form takes device pointers (samples, gains, out); the other
+ * takes host buffers and copies. */
+int chiaro_luminance_half(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64_t width,
+                          uint64_t height, float black_q6, float white_q6,
+                          const chiaro_vignetting *mesh, float *out);
+int chiaro_luminance_half_device(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64_t width,
+                                 uint64_t height, float black_q6, float white_q6,
+                                 const chiaro_vignetting *mesh, float *out);
+
 /* ---- allocation-free operator --------------------------------------------- */
 
 /* No counterpart in the reference: an allocation-free form of

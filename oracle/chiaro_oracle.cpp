@@ -1952,4 +1952,42 @@ void oracle_luminance_half(const uint16_t *samples, size_t width, size_t height,
     }
 }
 
+// VignettingMesh::gain (calibration.rs:362-379) at raster (x, y) of a width x height sensor.
+static float vignetting_gain(const float *gains, size_t columns, size_t rows, float x, float y, size_t width,
+                             size_t height) {
+    if (!gains || columns < 2 || rows < 2) return 1.0f;
+    float cmax = (float)(columns - 1), rmax = (float)(rows - 1);
+    float fx = fclamp(x / (float)width * cmax, 0.0f, cmax);
+    float fy = fclamp(y / (float)height * rmax, 0.0f, rmax);
+    size_t c0 = (size_t)std::floor(fx), r0 = (size_t)std::floor(fy);
+    size_t c1 = std::min(c0 + 1, columns - 1), r1 = std::min(r0 + 1, rows - 1);
+    float tx = fx - (float)c0, ty = fy - (float)r0;
+    auto g = [&](size_t c, size_t r) { return gains[r * columns + c]; };
+    float top = g(c0, r0) * (1.0f - tx) + g(c1, r0) * tx;
+    float bottom = g(c0, r1) * (1.0f - tx) + g(c1, r1) * tx;
+    return top * (1.0f - ty) + bottom * ty;
+}
+
+// luminance_half (image.rs:401-428) with Mosaic::flat_field (image.rs:145-150): the
+// plane, and (when `argument` is given) the log's argument 1 + 1000 * linear per pixel.
+void oracle_luminance_half_mesh(const uint16_t *samples, size_t width, size_t height, float black_q6,
+                                float white_q6, const float *gains, size_t columns, size_t rows, float *out,
+                                float *argument) {
+    size_t w = width / 2, h = height / 2;
+    float range = fmax_r(white_q6 - black_q6, 1.0f);
+    for (size_t j = 0; j < h; ++j) {
+        const uint16_t *row0 = samples + 2 * j * width;
+        const uint16_t *row1 = samples + (2 * j + 1) * width;
+        for (size_t i = 0; i < w; ++i) {
+            float sum = (float)row0[2 * i] + (float)row0[2 * i + 1] + (float)row1[2 * i] + (float)row1[2 * i + 1];
+            float flat = vignetting_gain(gains, columns, rows, 2.0f * (float)i + 0.5f, 2.0f * (float)j + 0.5f,
+                                         width, height);
+            float linear = fmax_r((sum * 0.25f - black_q6) / range, 0.0f) * flat;
+            float x = 1.0f + 1000.0f * linear;
+            if (argument) argument[j * w + i] = x;
+            out[j * w + i] = std::log(x);
+        }
+    }
+}
+
 }  // extern "C"
