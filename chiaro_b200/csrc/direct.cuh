@@ -317,17 +317,18 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
 // The wide-radius retry (depth.rs:803-846) for the listed nodes; a warp per
 // entry, persistent over the list. Its 225-tap positions are kept as f32 g,
 // which halves their shared memory and lets more warps stay resident.
-__global__ void __launch_bounds__(128) direct_wide_kernel(DirectParams p) {
+__global__ void __launch_bounds__(256) direct_wide_kernel(DirectParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ RefPatch patches[4];
+    __shared__ RefPatch patches[8];
     const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
     const int V = p.n_targets;
     const int taps = (2 * p.wide_radius + 1) * (2 * p.wide_radius + 1);
     DirectSlot<float2> d =
         carve_direct_slot<float2>(smem_raw + (size_t)slot * direct_slot_bytes<float2>(V, taps), V, taps);
     RefPatch &patch = patches[slot];
     const int count = *p.wide_count;
-    for (int e = blockIdx.x * 4 + slot; e < count; e += gridDim.x * 4) {
+    for (int e = blockIdx.x * warps + slot; e < count; e += gridDim.x * warps) {
         int4 entry = p.wide_list[e];
         const int node = entry.x, first = entry.y, last = entry.z;
         const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);

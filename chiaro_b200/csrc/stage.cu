@@ -499,14 +499,17 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         const int taps = (2 * direct_radius + 1) * (2 * direct_radius + 1);
         const int wide_taps = (2 * wide_radius + 1) * (2 * wide_radius + 1);
         const size_t slot = direct_slot_bytes<float2>(V, taps), wide_slot = direct_slot_bytes<float2>(V, wide_taps);
-        if (slot > 200 * 1024 || 4 * wide_slot > 200 * 1024)
+        if (slot > 200 * 1024 || wide_slot > 200 * 1024)
             throw CudaError{cudaErrorInvalidValue, "direct pass shared memory exceeds 200 KiB"};
         p.nodes_per_cta = warps_per_cta(direct_depth_kernel, slot, 8);
         direct_depth_kernel<<<blocks_for(M, p.nodes_per_cta), 32 * p.nodes_per_cta, p.nodes_per_cta * slot, s>>>(p);
         CK(cudaGetLastError());
+        const int wide_warps = warps_per_cta(direct_wide_kernel, wide_slot, 8);
         int wide_blocks = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wide_blocks, direct_wide_kernel, 128, 4 * wide_slot));
-        direct_wide_kernel<<<ctx->sm_count * std::max(1, wide_blocks), 128, 4 * wide_slot, s>>>(p);
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wide_blocks, direct_wide_kernel, 32 * wide_warps,
+                                                         wide_warps * wide_slot));
+        direct_wide_kernel<<<ctx->sm_count * std::max(1, wide_blocks), 32 * wide_warps, wide_warps * wide_slot,
+                             s>>>(p);
         CK(cudaGetLastError());
     }
     if (debug) {
