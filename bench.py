@@ -262,7 +262,10 @@ def run_ours(args, rank, world, local):
         pinned = torch.empty(inp.luminance.data.size, dtype=torch.float32, pin_memory=True).numpy()
         pinned[:] = inp.luminance.data.reshape(-1)
         inp.luminance.data = pinned.reshape(inp.luminance.height, inp.luminance.width)
-    refine_multiview_depth(inputs, scene.reference_index, scene.alignments(), scene.options, context=ctx)
+    result = None
+    for _ in range(max(args.warmup, 2)):  # steady state: the output pool holds two result sets
+        result = refine_multiview_depth(inputs, scene.reference_index, scene.alignments(), scene.options,
+                                        context=ctx)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()

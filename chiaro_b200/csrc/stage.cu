@@ -39,6 +39,8 @@ struct chiaro_depth_ctx {
     };
     std::map<std::string, Buffer> buffers;
     cudaEvent_t events[8] = {};
+    cudaStream_t copy_stream = nullptr;  // host transfers that overlap the stage's kernels
+    cudaEvent_t planes_ready = nullptr, map_ready = nullptr;
     float timings[7] = {};
     int launches = 0;  // this library's kernel launches in the last stage call
 };
@@ -221,6 +223,24 @@ struct StageOutputs {  // device pointers
     float *warp_confidence[MAX_VIEWS];
 };
 
+// Host transfers of the host-buffer entry point, issued inside the stage so that
+// they overlap its kernels: the luminance planes arrive on the copy stream while
+// the geometry kernels run, and the depth map leaves on the copy stream while
+// the per-target decisions run.
+struct HostTransfers {
+    struct Upload {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    };
+    std::vector<Upload> planes;
+    double *depth = nullptr;
+    float *confidence = nullptr;
+    uint8_t *provenance = nullptr;
+    float2 *points[MAX_VIEWS] = {};
+    float *warp_confidence[MAX_VIEWS] = {};
+};
+
 struct Results {  // read back once at the end
     unsigned long long tested, measured, regularized;
     unsigned long long target_counts[MAX_VIEWS][3];
@@ -322,7 +342,8 @@ void download_field(chiaro_depth_ctx *ctx, const Field &f, size_t n, uint8_t *ha
 // (device pointers inside), d_views: its device copy.
 void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_views, int reference,
                const chiaro_depth_options &o, const Grids &g, const StageOutputs &out, Results *d_results,
-               Results &h_results, const chiaro_depth_debug *debug, std::vector<int> &rewritten) {
+               Results &h_results, const chiaro_depth_debug *debug, std::vector<int> &rewritten,
+               const HostTransfers *host) {
     cudaStream_t s = ctx->stream;
     set_smem_limits();
     const int n_views = (int)h_views.size();
@@ -363,6 +384,19 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     CK(cudaMemsetAsync(d_results, 0, sizeof(Results), s));
 
     CK(cudaEventRecord(ctx->events[0], s));
+    // per (node, target) geometry of both grids: cameras and warps only, so it runs
+    // while the luminance planes are still arriving
+    GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
+    launch_geometry(ctx, d_views, reference, targets, g.coarse_columns, g.coarse_rows, g.coarse_step,
+                    coarse_geometry);
+    GeomRec *fine_geometry = dbuf<GeomRec>(ctx, "fine_geometry", M * std::max(V, 1));
+    launch_geometry(ctx, d_views, reference, targets, g.columns, g.rows, g.step, fine_geometry);
+    if (host && !host->planes.empty()) {
+        for (const auto &u : host->planes)
+            CK(cudaMemcpyAsync(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice, ctx->copy_stream));
+        CK(cudaEventRecord(ctx->planes_ready, ctx->copy_stream));
+        CK(cudaStreamWaitEvent(s, ctx->planes_ready, 0));
+    }
     // quad planes of the target luminance for the fast ZNCC path
     for (int t : targets) {
         const PlaneRef &lp = h_views[t].luma;
@@ -379,9 +413,6 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     float *guidance = dbuf<float>(ctx, "guidance", N);
     uint8_t *tested = dbuf<uint8_t>(ctx, "tested", N);
     CK(cudaMemsetAsync(tested, 0, N, s));  // the cost kernel only sets tested nodes
-    GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
-    launch_geometry(ctx, d_views, reference, targets, g.coarse_columns, g.coarse_rows, g.coarse_step,
-                    coarse_geometry);
     {
         CostParams p{};
         p.geometry = coarse_geometry;
@@ -461,8 +492,6 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     Field direct = field_bufs(ctx, "direct", M);
     float *fguidance = dbuf<float>(ctx, "fine_guidance", M);
     uint8_t *ftested = dbuf<uint8_t>(ctx, "fine_tested", M);
-    GeomRec *fine_geometry = dbuf<GeomRec>(ctx, "fine_geometry", M * std::max(V, 1));
-    launch_geometry(ctx, d_views, reference, targets, g.columns, g.rows, g.step, fine_geometry);
     {
         DirectParams p{};
         p.geometry = fine_geometry;
@@ -570,6 +599,10 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     }
     medians_kernel<<<1, 1, 0, s>>>(depth_sorted, imp_sorted, d_results);
     CK(cudaGetLastError());
+    // the depth map needs only the final field, so it is ready before the decisions
+    depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->map_ready, s));
     CK(cudaEventRecord(ctx->events[5], s));
     // ---- per-target decisions (depth.rs:420-547): all targets in one launch
     rewritten.clear();
@@ -615,14 +648,26 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
             rewritten.push_back(t);
         }
     }
-    depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
-    CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->events[6], s));
     // quad planes 1 per target, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
     // decisions 1 + 3 per target, map 1
     ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
+    if (host) {
+        // every kernel is queued: the depth map leaves on the copy stream while the
+        // decisions run (a pageable destination blocks this thread, not the GPU)
+        CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->map_ready, 0));
+        CK(cudaMemcpyAsync(host->depth, out.depth, M * sizeof(double), cudaMemcpyDeviceToHost, ctx->copy_stream));
+        CK(cudaMemcpyAsync(host->confidence, out.confidence, M * sizeof(float), cudaMemcpyDeviceToHost,
+                           ctx->copy_stream));
+        CK(cudaMemcpyAsync(host->provenance, out.provenance, M, cudaMemcpyDeviceToHost, ctx->copy_stream));
+        for (int t : rewritten) {
+            download(ctx, host->points[t], out.points[t], M);
+            download(ctx, host->warp_confidence[t], out.warp_confidence[t], M);
+        }
+    }
     CK(cudaMemcpyAsync(&h_results, d_results, sizeof(Results), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    CK(cudaStreamSynchronize(ctx->copy_stream));
     for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ctx->timings[i], ctx->events[i], ctx->events[i + 1]));
     CK(cudaEventElapsedTime(&ctx->timings[6], ctx->events[0], ctx->events[6]));
 }
@@ -716,6 +761,7 @@ int refine(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views, size
     try {
         CK(cudaSetDevice(ctx->device));
         std::vector<DevView> h_views(n_views);
+        HostTransfers host;
         for (size_t i = 0; i < n_views; ++i) {
             const chiaro_view &v = views[i];
             size_t luma_n = v.luma_width * v.luma_height, warp_n = v.warp.columns * v.warp.rows;
@@ -724,7 +770,7 @@ int refine(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views, size
             if (!device_pointers) {
                 float *dl = dbuf<float>(ctx, "luma" + std::to_string(i), luma_n);
                 float2 *dp = dbuf<float2>(ctx, "warp" + std::to_string(i), warp_n);
-                upload(ctx, dl, v.luminance, luma_n);
+                host.planes.push_back({dl, v.luminance, luma_n * sizeof(float)});  // sent inside the stage
                 upload(ctx, dp, reinterpret_cast<const float2 *>(v.warp.points), warp_n);
                 luma = dl;
                 pts = dp;
@@ -747,25 +793,23 @@ int refine(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views, size
             out.depth = dbuf<double>(ctx, "out.depth", M);
             out.confidence = dbuf<float>(ctx, "out.confidence", M);
             out.provenance = dbuf<uint8_t>(ctx, "out.provenance", M);
+            host.depth = out_map->depth;
+            host.confidence = out_map->confidence;
+            host.provenance = out_map->provenance;
             for (size_t t = 0; t < n_views; ++t) {
                 out.points[t] = dbuf<float2>(ctx, "out.points" + std::to_string(t), M);
                 out.warp_confidence[t] = dbuf<float>(ctx, "out.wconf" + std::to_string(t), M);
+                if (refined) {
+                    host.points[t] = reinterpret_cast<float2 *>(refined[t].points);
+                    host.warp_confidence[t] = refined[t].confidence;
+                }
             }
         }
         Results *d_results = dbuf<Results>(ctx, "results", 1);
         Results h_results{};
         std::vector<int> rewritten;
-        run_stage(ctx, h_views, d_views, (int)reference_index, o, g, out, d_results, h_results, debug, rewritten);
-        if (!device_pointers) {
-            download(ctx, out_map->depth, out.depth, M);
-            download(ctx, out_map->confidence, out.confidence, M);
-            download(ctx, out_map->provenance, out.provenance, M);
-            for (int t : rewritten) {
-                download(ctx, reinterpret_cast<float2 *>(refined[t].points), out.points[t], M);
-                download(ctx, refined[t].confidence, out.warp_confidence[t], M);
-            }
-            CK(cudaStreamSynchronize(ctx->stream));
-        }
+        run_stage(ctx, h_views, d_views, (int)reference_index, o, g, out, d_results, h_results, debug, rewritten,
+                  device_pointers ? nullptr : &host);
         out_map->columns = g.columns;
         out_map->rows = g.rows;
         out_map->step = g.step;
@@ -792,6 +836,17 @@ extern "C" {
 
 int chiaro_depth_abi_version(void) { return CHIARO_DEPTH_ABI_VERSION; }
 
+int chiaro_host_alloc(uint64_t bytes, void **out) {
+    if (!out) return CHIARO_ERR_ARGUMENT;
+    *out = nullptr;
+    if (bytes == 0) return CHIARO_OK;
+    return cudaHostAlloc(out, bytes, cudaHostAllocPortable) == cudaSuccess ? CHIARO_OK : CHIARO_ERR_CUDA;
+}
+
+void chiaro_host_free(void *ptr) {
+    if (ptr) cudaFreeHost(ptr);
+}
+
 int chiaro_depth_ctx_create(int device, chiaro_depth_ctx **out) {
     if (!out) return CHIARO_ERR_ARGUMENT;
     *out = nullptr;
@@ -802,6 +857,9 @@ int chiaro_depth_ctx_create(int device, chiaro_depth_ctx **out) {
         CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
         CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         for (auto &e : ctx->events) CK(cudaEventCreate(&e));
+        CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->planes_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->map_ready, cudaEventDisableTiming));
     } catch (const CudaError &e) {
         delete ctx;
         return CHIARO_ERR_CUDA;
@@ -816,8 +874,12 @@ void chiaro_depth_ctx_destroy(chiaro_depth_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto &kv : ctx->buffers)
         if (kv.second.ptr) cudaFree(kv.second.ptr);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (auto &e : ctx->events)
         if (e) cudaEventDestroy(e);
+    if (ctx->planes_ready) cudaEventDestroy(ctx->planes_ready);
+    if (ctx->map_ready) cudaEventDestroy(ctx->map_ready);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -286,7 +286,7 @@ def refine_multiview_depth(inputs: Sequence, reference_index: int, alignments: S
     ``debug`` may be a dict of numpy arrays named like the fields of
     ``chiaro_depth_debug``; the library fills them with stage results.
     """
-    from .runtime import default_context
+    from .runtime import default_context, pinned_pool
 
     if len(inputs) != len(alignments):
         return None
@@ -298,17 +298,23 @@ def refine_multiview_depth(inputs: Sequence, reference_index: int, alignments: S
     m = columns * rows
     n = len(inputs)
     views, keep = pack_views(inputs, alignments)
+    # outputs in page-locked host memory (a caching pool): the library copies into them at
+    # the full host-link rate and overlaps the depth map's copy with the decisions
+    pool = pinned_pool()
+    targets = [t for t in range(n) if t != reference_index and inputs[t].camera is not None
+               and alignments[t].report.accepted]
     refined = (WarpC * n)()
-    out_points = [np.empty(2 * m, dtype=np.float32) for _ in range(n)]
-    out_conf = [np.empty(m, dtype=np.float32) for _ in range(n)]
-    for i in range(n):
+    out_points, out_conf = [None] * n, [None] * n
+    for i in targets:
+        out_points[i] = pool.empty(2 * m, np.float32)
+        out_conf[i] = pool.empty(m, np.float32)
         refined[i].points = fptr(out_points[i])
         refined[i].confidence = fptr(out_conf[i])
         refined[i].capacity = m
     reports = (DepthReportC * n)()
-    depth = np.empty(m, dtype=np.float64)
-    confidence = np.empty(m, dtype=np.float32)
-    provenance = np.empty(m, dtype=np.uint8)
+    depth = pool.empty(m, np.float64)
+    confidence = pool.empty(m, np.float32)
+    provenance = pool.empty(m, np.uint8)
     dmap = DepthMapC()
     dmap.capacity = m
     dmap.depth = dptr(depth)

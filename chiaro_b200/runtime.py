@@ -6,8 +6,10 @@ stage has no CPU fallback.
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
 import threading
+import weakref
 from pathlib import Path
 from typing import Optional
 
@@ -37,6 +39,8 @@ SIGNATURES = {
     "chiaro_depth_last_timings": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int]),
     "chiaro_depth_last_launches": (C.c_int, [C.c_void_p]),
     "chiaro_depth_ctx_stream": (C.c_void_p, [C.c_void_p]),
+    "chiaro_host_alloc": (C.c_int, [C.c_uint64, P(C.c_void_p)]),
+    "chiaro_host_free": (None, [C.c_void_p]),
     "chiaro_luminance_half": (C.c_int, [C.c_void_p, P(C.c_uint16), C.c_uint64, C.c_uint64, C.c_float, C.c_float,
                                         P(abi.VignettingC), P(C.c_float)]),
     "chiaro_luminance_half_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_float,
@@ -162,6 +166,65 @@ class DepthContext:
         for name, arr in arrays.items():
             setattr(dbg, name, arr.ctypes.data_as(C.POINTER(abi.DEBUG_FIELD_TYPES[name])))
         return dbg
+
+
+class _PinnedBlock:
+    """One page-locked host buffer lent to numpy arrays; back to the pool when they are gone."""
+
+    def __init__(self, pool, ptr: int, nbytes: int, shape, dtype):
+        shape = (int(shape),) if np.isscalar(shape) else tuple(int(s) for s in shape)
+        self.__array_interface__ = {"data": (ptr, False), "shape": shape,
+                                    "typestr": np.dtype(dtype).str, "version": 3}
+        weakref.finalize(self, pool._release, ptr, nbytes)
+
+
+class PinnedPool:
+    """A caching pool of page-locked host buffers (chiaro_host_alloc), keyed by size.
+
+    ``empty(shape, dtype)`` returns a numpy array backed by pinned memory; when the
+    array and every view of it are garbage-collected, the buffer returns to the pool
+    for the next call, so a steady loop of stage calls pins its output memory once.
+    The return path takes no lock (a finalizer may run inside any allocation, the
+    pool's own included): it appends to a deque that ``empty`` drains.
+    """
+
+    def __init__(self, lib):
+        self.lib = lib
+        self.free = {}
+        self.returned = collections.deque()
+        self.lock = threading.Lock()
+
+    def empty(self, shape, dtype) -> np.ndarray:
+        nbytes = max(int(np.prod(shape)) * np.dtype(dtype).itemsize, 1)
+        ptr = None
+        with self.lock:
+            while self.returned:
+                size, p = self.returned.popleft()
+                self.free.setdefault(size, []).append(p)
+            stack = self.free.get(nbytes)
+            if stack:
+                ptr = stack.pop()
+        if ptr is None:
+            p = C.c_void_p()
+            if self.lib.chiaro_host_alloc(nbytes, C.byref(p)) != abi.OK or not p.value:
+                return np.empty(shape, dtype)  # pinning refused: pageable memory still works
+            ptr = p.value
+        return np.asarray(_PinnedBlock(self, ptr, nbytes, shape, dtype))
+
+    def _release(self, ptr: int, nbytes: int):
+        self.returned.append((nbytes, ptr))
+
+
+_pinned: Optional[PinnedPool] = None
+
+
+def pinned_pool() -> PinnedPool:
+    global _pinned
+    lib = load_library()  # takes _lock itself
+    with _lock:
+        if _pinned is None:
+            _pinned = PinnedPool(lib)
+    return _pinned
 
 
 def default_context(device: Optional[int] = None) -> DepthContext:

@@ -190,6 +190,16 @@ enum chiaro_node_warp {
 
 typedef struct chiaro_depth_ctx chiaro_depth_ctx;
 
+/* ---- pinned host memory ---------------------------------------------------- */
+
+/* No counterpart in the reference: page-locked host buffers for the inputs and
+ * outputs of the host-buffer entry points, which then move at the full
+ * host-link rate (about 50 GB/s here, against about 19 GB/s for pageable
+ * memory) and overlap the stage's kernels. Allocation is slow (it pins pages),
+ * so callers keep and reuse these buffers. */
+int chiaro_host_alloc(uint64_t bytes, void **out);
+void chiaro_host_free(void *ptr);
+
 /* ---- context ------------------------------------------------------------ */
 
 /* Create a context bound to CUDA device `device` with its own stream. One
