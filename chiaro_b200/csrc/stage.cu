@@ -25,6 +25,7 @@
 #include "luminance.cuh"
 #include "select.cuh"
 #include "sgm.cuh"
+#include "sgm_u16.cuh"
 
 using namespace chiaro;
 
@@ -211,6 +212,37 @@ void launch_sgm(chiaro_depth_ctx *ctx, const float *data, const float *guidance,
     }
     const unsigned blocks = (unsigned)std::min<size_t>(div_ceil(total, 256), (size_t)ctx->sm_count * 16);
     sgm_sum_kernel<<<blocks, 256, 0, ctx->stream>>>(paths, pitch, total, out);
+    CK(cudaGetLastError());
+}
+
+template <int K>
+void sgm_u16_paths(chiaro_depth_ctx *ctx, const unsigned *data, const float *guidance, unsigned *paths, size_t pitch,
+                   int columns, int rows, int labels) {
+    const unsigned blocks = (unsigned)div_ceil(sgm_total_paths(columns, rows), SGM_PATHS_PER_CTA);
+    sgm_u16_paths_kernel<K><<<blocks, 32 * SGM_PATHS_PER_CTA, 0, ctx->stream>>>(data, guidance, paths, pitch,
+                                                                                columns, rows, labels);
+    CK(cudaGetLastError());
+}
+
+// The quantised SGM (sgm_u16.cuh): quantise, every direction's path costs, sum and winner.
+void launch_sgm_u16(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, int columns, int rows,
+                    int labels, uint16_t *aggregate, uint16_t *best) {
+    const size_t nodes = (size_t)columns * rows, pairs = (size_t)(labels + 1) / 2;
+    const size_t words = nodes * pairs, pitch = (words + 63) / 64 * 64;
+    unsigned *quantised = dbuf<unsigned>(ctx, "sgm16.costs", words);
+    unsigned *paths = dbuf<unsigned>(ctx, "sgm16.paths", 8 * pitch);
+    const unsigned qblocks = (unsigned)std::min<size_t>(div_ceil(words, 256), (size_t)ctx->sm_count * 16);
+    sgm_quantise_kernel<<<qblocks, 256, 0, ctx->stream>>>(costs, (int)nodes, labels, quantised);
+    CK(cudaGetLastError());
+    switch ((int)((pairs + 31) / 32)) {
+        case 1: sgm_u16_paths<1>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
+        case 2: sgm_u16_paths<2>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
+        case 3: sgm_u16_paths<3>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
+        case 4: sgm_u16_paths<4>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
+        default: throw CudaError{cudaErrorInvalidValue, "labels exceed 256"};
+    }
+    sgm_u16_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, ctx->stream>>>(paths, pitch, (int)nodes,
+                                                                                       labels, aggregate, best);
     CK(cudaGetLastError());
 }
 
@@ -1135,6 +1167,45 @@ int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *gl
         download(ctx, reinterpret_cast<float2 *>(global), a.global, n);
         download(ctx, reinterpret_cast<float2 *>(point), a.point, n);
         CK(cudaStreamSynchronize(s));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_sgm_aggregate_u16_device(chiaro_depth_ctx *ctx, const float *costs, const float *guidance,
+                                    uint64_t columns, uint64_t rows, uint64_t labels, uint16_t *aggregate,
+                                    uint16_t *best) {
+    if (!ctx || !costs || !guidance || (!aggregate && !best) || columns < 1 || rows < 1 || labels < 1 ||
+        labels > MAX_LABELS || columns * rows > (1u << 30))
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        launch_sgm_u16(ctx, costs, guidance, (int)columns, (int)rows, (int)labels, aggregate, best);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_sgm_aggregate_u16(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, uint64_t columns,
+                             uint64_t rows, uint64_t labels, uint16_t *aggregate, uint16_t *best) {
+    if (!ctx || !costs || !guidance || (!aggregate && !best) || columns < 1 || rows < 1 || labels < 1 ||
+        labels > MAX_LABELS || columns * rows > (1u << 30))
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        size_t n = columns * rows, nl = n * labels;
+        float *dc = dbuf<float>(ctx, "op.costs", nl), *dg = dbuf<float>(ctx, "op.guidance", n);
+        uint16_t *da = aggregate ? dbuf<uint16_t>(ctx, "op.aggregate16", nl) : nullptr;
+        uint16_t *db = best ? dbuf<uint16_t>(ctx, "op.best16", n) : nullptr;
+        upload(ctx, dc, costs, nl);
+        upload(ctx, dg, guidance, n);
+        launch_sgm_u16(ctx, dc, dg, (int)columns, (int)rows, (int)labels, da, db);
+        download(ctx, aggregate, da, nl);
+        download(ctx, best, db, n);
+        CK(cudaStreamSynchronize(ctx->stream));
     } catch (const CudaError &e) {
         return fail(ctx, e);
     }

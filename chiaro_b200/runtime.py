@@ -39,6 +39,10 @@ SIGNATURES = {
     "chiaro_depth_last_timings": (C.c_int, [C.c_void_p, P(C.c_float), C.c_int]),
     "chiaro_depth_last_launches": (C.c_int, [C.c_void_p]),
     "chiaro_depth_ctx_stream": (C.c_void_p, [C.c_void_p]),
+    "chiaro_sgm_aggregate_u16": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_uint64, C.c_uint64,
+                                           C.c_uint64, P(C.c_uint16), P(C.c_uint16)]),
+    "chiaro_sgm_aggregate_u16_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
+                                                  C.c_uint64, C.c_void_p, C.c_void_p]),
     "chiaro_host_alloc": (C.c_int, [C.c_uint64, P(C.c_void_p)]),
     "chiaro_host_free": (None, [C.c_void_p]),
     "chiaro_luminance_half": (C.c_int, [C.c_void_p, P(C.c_uint16), C.c_uint64, C.c_uint64, C.c_float, C.c_float,

@@ -314,6 +314,25 @@ int chiaro_warp_decisions_filter(chiaro_depth_ctx *ctx, uint8_t *kind, float *gl
                                  const float *guidance, uint64_t columns,
                                  uint64_t rows, int consensus, int boundaries);
 
+/* ---- quantised SGM ---------------------------------------------------------- */
+
+/* No counterpart in the reference: the quantised performance mode of
+ * semi_global_costs (depth.rs:1279-1383). Costs (f32 [N][D], the stage's range
+ * [0, 2.25]; NaN counts as 2.25) become u16 fixed point at 2048 per unit, the
+ * edge penalties are the reference's f32 p1, p2 quantised the same way, and the
+ * 8-path recurrence and sum run in exact 16-bit integers on label pairs (a path
+ * cost is at most 5530, the sum at most 44240). Outputs, each optional: the
+ * u16 aggregate [N][D] and the winner over labels 1..D-1 per node (first
+ * minimum). Half the bytes of the f32 path per cell; the winner agrees with the
+ * f32 path's within one plane. labels <= 256. The _device form takes device
+ * pointers. */
+int chiaro_sgm_aggregate_u16(chiaro_depth_ctx *ctx, const float *costs, const float *guidance,
+                             uint64_t columns, uint64_t rows, uint64_t labels, uint16_t *aggregate,
+                             uint16_t *best);
+int chiaro_sgm_aggregate_u16_device(chiaro_depth_ctx *ctx, const float *costs,
+                                    const float *guidance, uint64_t columns, uint64_t rows,
+                                    uint64_t labels, uint16_t *aggregate, uint16_t *best);
+
 /* ---- input plane --------------------------------------------------------- */
 
 /* VignettingMesh (calibration.rs:354-358): a columns x rows grid of flat-field

@@ -1990,4 +1990,90 @@ void oracle_luminance_half_mesh(const uint16_t *samples, size_t width, size_t he
     }
 }
 
+// ---- quantised SGM (no counterpart in the reference) ------------------------------------
+// The project's quantised performance mode of semi_global_costs: costs in u16 fixed point
+// (Q = 2048 per cost unit; the stage's costs lie in [0, 2.25], so at most 4608), the edge
+// penalties of accumulate_path (depth.rs:1358-1361) computed in f32 as the reference does
+// and quantised the same way, the path recurrence (depth.rs:1363-1381) in exact integers,
+// the 8 path costs summed per cell (a path cost is at most 4608 + 922, the sum at most
+// 44240: no overflow), and the winner over labels 1..D-1 (the first minimum, as
+// select_depths picks it).
+static const float SGM_Q = 2048.0f;
+static const uint32_t SGM_COST_MAX_Q = 4608;  // 2.25 * Q
+
+static uint32_t quantise_sgm_cost(float c) {
+    if (!(c == c)) return SGM_COST_MAX_Q;  // NaN: the missing cost
+    float v = std::nearbyint(c * SGM_Q);
+    if (v <= 0.0f) return 0;
+    return v >= (float)SGM_COST_MAX_Q ? SGM_COST_MAX_Q : (uint32_t)v;
+}
+
+static uint32_t quantise_penalty(float p) { return (uint32_t)std::nearbyint(p * SGM_Q); }
+
+static void accumulate_path_u16(const uint32_t *data, const float *guidance, uint32_t *output, size_t labels,
+                                const std::vector<size_t> &path) {
+    const uint32_t big = 0xFFFF;
+    std::vector<uint32_t> previous(labels), current(labels);
+    for (size_t k = 0; k < path.size(); ++k) {
+        size_t node = path[k], offset = node * labels;
+        if (k == 0) {
+            for (size_t l = 0; l < labels; ++l) {
+                previous[l] = data[offset + l];
+                output[offset + l] += previous[l];
+            }
+            continue;
+        }
+        float edge = std::fabs(guidance[node] - guidance[path[k - 1]]);
+        float edge_scale = 1.0f / (1.0f + 4.0f * edge);
+        uint32_t p1 = quantise_penalty(0.06f * fmax_r(edge_scale, 0.35f));
+        uint32_t p2 = quantise_penalty(0.45f * fmax_r(edge_scale, 0.12f));
+        uint32_t minimum_previous = big;
+        for (size_t l = 0; l < labels; ++l) minimum_previous = std::min(minimum_previous, previous[l]);
+        for (size_t l = 0; l < labels; ++l) {
+            uint32_t lower = l > 0 ? previous[l - 1] + p1 : big;
+            uint32_t higher = l + 1 < labels ? previous[l + 1] + p1 : big;
+            uint32_t best = std::min(std::min(previous[l], lower), std::min(higher, minimum_previous + p2));
+            current[l] = data[offset + l] + best - minimum_previous;
+            output[offset + l] += current[l];
+        }
+        std::swap(previous, current);
+    }
+}
+
+void oracle_sgm_u16(const float *costs, const float *guidance, size_t columns, size_t rows, size_t labels,
+                    uint16_t *aggregate, uint16_t *best) {
+    size_t n = columns * rows;
+    std::vector<uint32_t> data(n * labels), output(n * labels, 0);
+    for (size_t i = 0; i < n * labels; ++i) data[i] = quantise_sgm_cost(costs[i]);
+    std::vector<size_t> forward, reverse;
+    auto both = [&](const std::vector<size_t> &path) {
+        accumulate_path_u16(data.data(), guidance, output.data(), labels, path);
+        reverse.assign(path.rbegin(), path.rend());
+        accumulate_path_u16(data.data(), guidance, output.data(), labels, reverse);
+    };
+    for (size_t row = 0; row < rows; ++row) {
+        forward.clear();
+        for (size_t column = 0; column < columns; ++column) forward.push_back(row * columns + column);
+        both(forward);
+    }
+    for (size_t column = 0; column < columns; ++column) {
+        forward.clear();
+        for (size_t row = 0; row < rows; ++row) forward.push_back(row * columns + column);
+        both(forward);
+    }
+    for (int mirrored = 0; mirrored < 2; ++mirrored)
+        for (const auto &path : diagonal_paths(columns, rows, mirrored != 0)) both(path);
+    for (size_t node = 0; node < n; ++node) {
+        const uint32_t *o = output.data() + node * labels;
+        if (aggregate)
+            for (size_t l = 0; l < labels; ++l) aggregate[node * labels + l] = (uint16_t)o[l];
+        if (best) {
+            size_t b = labels > 1 ? 1 : 0;
+            for (size_t l = 2; l < labels; ++l)
+                if (o[l] < o[b]) b = l;
+            best[node] = (uint16_t)b;
+        }
+    }
+}
+
 }  // extern "C"

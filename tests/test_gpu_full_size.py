@@ -154,3 +154,18 @@ def test_decisions_band(full):
         assert_bits(_rows(gpu, a + 2, b - 2, cols), kinds[2 * cols:(b - a - 2) * cols], f"decision kinds {t}")
         checked += 1
     assert checked == f["n"] - 1
+
+
+def test_quantised_sgm_whole_grid(full, gpu_ctx):
+    """The quantised SGM on the full-size cost volume: bit for bit against the integer
+    oracle, and its winner within one plane of the f32 path's on the tested nodes."""
+    from test_gpu_sgm_u16 import gpu_u16, oracle_u16
+    f, dbg = full, full["dbg"]
+    cc, cr, D = f["cc"], f["cr"], f["D"]
+    agg_g, best_g = gpu_u16(gpu_ctx, dbg["coarse_costs"], dbg["coarse_guidance"], cc, cr, D)
+    agg_o, best_o = oracle_u16(dbg["coarse_costs"], dbg["coarse_guidance"], cc, cr, D)
+    assert np.array_equal(agg_g, agg_o) and np.array_equal(best_g, best_o)
+    f32 = 1 + np.argmin(dbg["regularised"].reshape(-1, D)[:, 1:], axis=1)
+    tested = dbg["coarse_tested"] == 1
+    diff = np.abs(f32.astype(int) - best_g.astype(int))[tested]
+    assert (diff <= 1).mean() >= 0.995
