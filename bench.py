@@ -283,6 +283,8 @@ def run_ours(args, rank, world, local):
     d2h = M * (8 + 4 + 1) + targets * M * (8 + 4)
     e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
 
+    quantised = quantised_sgm(args, scene, work, ctx, torch, device, stream, flush)
+
     peaks = measured_peaks()
     sgm_s = stage_ms["sgm"] / 1e3
     achieved = work["sgm_bytes"] / sgm_s / 1e9
@@ -308,6 +310,9 @@ def run_ours(args, rank, world, local):
                      "traffic": sgm_traffic() if args.workload == "five_view" else None,
                      "traffic_source": "profiles/sgm_five_view_dram.md (ncu dram__bytes_read + write, one call)",
                      "peak_source": peaks["source"], "algorithmic_bytes": work["sgm_bytes"]},
+        "quantised_sgm": dict(quantised, roofline=dict(
+            quantised["roofline"], peak=peaks["hbm_gbs"],
+            frac=round(quantised["roofline"]["achieved"] / peaks["hbm_gbs"], 4))),
         "compute_roofline": {"kernel": "cost_volume_kernel (build_cost_volume, the largest correlation kernel)",
                              "bound": "fp32", "achieved": round(cost_tflops, 2), "peak": round(fp32_peak, 1),
                              "unit": "TFLOP/s", "frac": round(cost_tflops / fp32_peak, 4),
@@ -332,6 +337,62 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
     ctx.close()
     return line
+
+
+def quantised_sgm(args, scene, work, ctx, torch, device, stream, flush):
+    """The quantised u16 SGM (chiaro_sgm_aggregate_u16_device) against the f32 SGM on this
+    workload's own cost volume, both timed with CUDA events on the library's stream (L2
+    flushed before each step), and the agreement of their winners."""
+    import numpy as np
+
+    from chiaro_b200.depth import output_shape, refine_multiview_depth
+    (cols, rows, _), (cc, cr, _) = output_shape(scene.width, scene.height, scene.options)
+    N, D = cc * cr, scene.options.planes + 1
+    dbg = {k: np.zeros(n, t) for k, (n, t) in {"coarse_costs": (N * D, np.float32),
+                                                "coarse_guidance": (N, np.float32),
+                                                "regularised": (N * D, np.float32),
+                                                "coarse_tested": (N, np.uint8)}.items()}
+    refine_multiview_depth(scene.inputs(), scene.reference_index, scene.alignments(), scene.options, context=ctx,
+                           debug=dbg)
+    costs = torch.from_numpy(dbg["coarse_costs"]).to(device)
+    guidance = torch.from_numpy(dbg["coarse_guidance"]).to(device)
+    out32 = torch.empty(N * D, dtype=torch.float32, device=device)
+    best16 = torch.empty(N, dtype=torch.int16, device=device)
+    lib = ctx.lib
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        total = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / args.steps
+
+    f32_ms = timed(lambda: ctx.check(lib.chiaro_sgm_aggregate_device(
+        ctx.handle, costs.data_ptr(), guidance.data_ptr(), cc, cr, D, out32.data_ptr())))
+    u16_ms = timed(lambda: ctx.check(lib.chiaro_sgm_aggregate_u16_device(
+        ctx.handle, costs.data_ptr(), guidance.data_ptr(), cc, cr, D, None, best16.data_ptr())))
+    best = best16.cpu().numpy().view(np.uint16).astype(np.int64)
+    winner32 = 1 + np.argmin(dbg["regularised"].reshape(N, D)[:, 1:], axis=1)
+    tested = dbg["coarse_tested"] == 1
+    diff = np.abs(best - winner32)[tested]
+    u16_bytes = N * D * 4 + 8 * N * 4  # read u16 costs once, write the u16 aggregate once, guidance per direction
+    return {"kernel": "sgm_quantise + sgm_u16_paths + sgm_u16_select (chiaro_sgm_aggregate_u16_device)",
+            "ms": round(u16_ms, 4), "f32_sgm_ms": round(f32_ms, 4),
+            "gcells_s": round(work["cells"] / (u16_ms / 1e3) / 1e9, 2),
+            "winner_agreement": {"exact": round(float((diff == 0).mean()), 5),
+                                 "within_one_plane": round(float((diff <= 1).mean()), 5),
+                                 "tested_nodes": int(tested.sum())},
+            "roofline": {"bound": "hbm", "achieved": round(u16_bytes / (u16_ms / 1e3) / 1e9, 1), "unit": "GB/s",
+                         "algorithmic_bytes": u16_bytes}}
 
 
 def run_reference(args, rank, world):
