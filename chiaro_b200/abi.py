@@ -81,6 +81,23 @@ class CameraC(C.Structure):
     ]
 
 
+class SgmInstanceC(C.Structure):
+    """chiaro_sgm_instance: one SGM instance of a batch (device pointers)."""
+
+    _fields_ = [
+        ("costs", C.c_void_p),
+        ("guidance", C.c_void_p),
+        ("out", C.c_void_p),
+        ("columns", C.c_uint64),
+        ("rows", C.c_uint64),
+        ("labels", C.c_uint64),
+    ]
+
+
+BATCH_GRAPH = 1
+BATCH_AUTOTUNE = 2
+
+
 class VignettingC(C.Structure):
     """VignettingMesh (calibration.rs:354-358)."""
 

@@ -23,7 +23,7 @@ __host__ __device__ inline int sgm_path_count(int family, int columns, int rows)
 
 // Path p of a family in the reference's enumeration (depth.rs:1287-1338):
 // start node, step and length of its forward direction.
-__device__ inline void sgm_path(int family, int p, int columns, int rows, int &r0, int &c0, int &dr, int &dc,
+__host__ __device__ inline void sgm_path(int family, int p, int columns, int rows, int &r0, int &c0, int &dr, int &dc,
                                 int &len) {
     switch (family) {
         case SGM_ROWS: r0 = p; c0 = 0; dr = 0; dc = 1; len = columns; return;
@@ -73,7 +73,7 @@ __host__ __device__ inline unsigned sgm_total_paths(int columns, int rows) {
     return 2u * (unsigned)(rows + columns + 2 * (columns + rows - 1));
 }
 
-__device__ inline void sgm_path_of(int b, int columns, int rows, int &pass, int &path) {
+__host__ __device__ inline void sgm_path_of(int b, int columns, int rows, int &pass, int &path) {
     for (int family = 0; family < 4; ++family) {
         const int n = sgm_path_count(family, columns, rows);
         if (b < 2 * n) {
@@ -87,16 +87,14 @@ __device__ inline void sgm_path_of(int b, int columns, int rows, int &pass, int 
     path = 0;
 }
 
-// Path costs of every path of every direction; pass k writes paths + k * pitch.
+// Path `warp_path` of the launch's enumeration (sgm_path_of), walked by the
+// calling warp; pass k writes paths + k * pitch.
 template <int K>
-__global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_paths_kernel(const float *__restrict__ data,
-                                                                          const float *__restrict__ guidance,
-                                                                          float *__restrict__ paths, size_t pitch,
-                                                                          int columns, int rows, int labels) {
+__device__ __forceinline__ void sgm_walk_path(const float *__restrict__ data, const float *__restrict__ guidance,
+                                              float *__restrict__ paths, size_t pitch, int columns, int rows,
+                                              int labels, int warp_path) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
-    if (warp_path >= (int)sgm_total_paths(columns, rows)) return;  // whole warp
     int pass, path;
     sgm_path_of(warp_path, columns, rows, pass, path);
     int r0, c0, dr, dc, len;
@@ -179,6 +177,17 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_paths_kernel(const
             }
         }
     }
+}
+
+// Path costs of every path of every direction; pass k writes paths + k * pitch.
+template <int K>
+__global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_paths_kernel(const float *__restrict__ data,
+                                                                          const float *__restrict__ guidance,
+                                                                          float *__restrict__ paths, size_t pitch,
+                                                                          int columns, int rows, int labels) {
+    const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
+    if (warp_path >= (int)sgm_total_paths(columns, rows)) return;  // whole warp
+    sgm_walk_path<K>(data, guidance, paths, pitch, columns, rows, labels, warp_path);
 }
 
 // out = ((0 + L1) + L2) + ... + L8 per cell, the reference's order.

@@ -26,6 +26,7 @@
 #include "select.cuh"
 #include "sgm.cuh"
 #include "sgm_u16.cuh"
+#include "sgm_batch.cuh"
 
 using namespace chiaro;
 
@@ -42,6 +43,11 @@ struct chiaro_depth_ctx {
     cudaEvent_t events[8] = {};
     cudaStream_t copy_stream = nullptr;  // host transfers that overlap the stage's kernels
     cudaEvent_t planes_ready = nullptr, map_ready = nullptr;
+    // batched SGM: the last captured graph and the tuned warps per CTA per size bucket
+    uint64_t batch_key = 0;
+    cudaGraphExec_t batch_exec = nullptr;
+    std::map<uint64_t, int> batch_tuning;
+    int batch_warps = 0, batch_waves = 0, batch_replayed = 0;
     float timings[7] = {};
     int launches = 0;  // this library's kernel launches in the last stage call
 };
@@ -244,6 +250,230 @@ void launch_sgm_u16(chiaro_depth_ctx *ctx, const float *costs, const float *guid
     sgm_u16_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, ctx->stream>>>(paths, pitch, (int)nodes,
                                                                                        labels, aggregate, best);
     CK(cudaGetLastError());
+}
+
+// ---- batched SGM (sgm_batch.cuh) -------------------------------------------------------
+struct BatchWave {
+    size_t first, count;          // instances
+    size_t task_offset, n_tasks;  // tasks
+};
+
+struct BatchPlan {
+    std::vector<SgmInstance> descs;  // device path pointers filled in once the scratch is known
+    std::vector<size_t> scratch_offset;
+    std::vector<int2> tasks;
+    std::vector<BatchWave> waves;
+    size_t scratch_floats = 0;
+    int kmax = 1;
+    uint64_t key = 1469598103934665603ull;  // FNV-1a over the batch's description
+};
+
+void fnv(uint64_t &h, const void *data, size_t bytes) {
+    const unsigned char *c = static_cast<const unsigned char *>(data);
+    for (size_t i = 0; i < bytes; ++i) h = (h ^ c[i]) * 1099511628211ull;
+}
+
+// Waves under the scratch budget and each wave's tasks, longest path first
+// (a counting sort on the path length).
+int plan_batch(const chiaro_sgm_instance *in, size_t n, size_t budget_floats, BatchPlan &plan) {
+    size_t wave_floats = 0;
+    plan.waves.push_back({0, 0, 0, 0});
+    for (size_t i = 0; i < n; ++i) {
+        const chiaro_sgm_instance &x = in[i];
+        if (!x.costs || !x.guidance || !x.out || x.columns < 1 || x.rows < 1 || x.labels < 1 ||
+            x.labels > MAX_LABELS || x.columns * x.rows > (1u << 26))
+            return CHIARO_ERR_ARGUMENT;
+        SgmInstance d{};
+        d.costs = x.costs;
+        d.guidance = x.guidance;
+        d.out = x.out;
+        d.columns = (int)x.columns;
+        d.rows = (int)x.rows;
+        d.labels = (int)x.labels;
+        d.sets = (int)((x.labels + 31) / 32);
+        d.cells = (size_t)x.columns * x.rows * x.labels;
+        d.pitch = (d.cells + 63) / 64 * 64;
+        const size_t need = 8 * d.pitch;
+        if (need > budget_floats) return CHIARO_ERR_CAPACITY;
+        BatchWave &w = plan.waves.back();
+        if (w.count > 0 && wave_floats + need > budget_floats) {
+            plan.waves.push_back({i, 0, 0, 0});
+            wave_floats = 0;
+        }
+        plan.scratch_offset.push_back(wave_floats);
+        wave_floats += need;
+        plan.scratch_floats = std::max(plan.scratch_floats, wave_floats);
+        plan.waves.back().count += 1;
+        plan.kmax = std::max(plan.kmax, d.sets);
+        plan.descs.push_back(d);
+        fnv(plan.key, &x, sizeof(x));
+    }
+    for (BatchWave &w : plan.waves) {
+        int longest = 0;
+        for (size_t i = w.first; i < w.first + w.count; ++i)
+            longest = std::max({longest, plan.descs[i].columns, plan.descs[i].rows});
+        std::vector<std::vector<int2>> by_length(longest + 1);
+        for (size_t i = w.first; i < w.first + w.count; ++i) {
+            const SgmInstance &d = plan.descs[i];
+            const int paths = (int)sgm_total_paths(d.columns, d.rows);
+            for (int k = 0; k < paths; ++k) {
+                int pass, path, r0, c0, dr, dc, len;
+                sgm_path_of(k, d.columns, d.rows, pass, path);
+                sgm_path(pass >> 1, path, d.columns, d.rows, r0, c0, dr, dc, len);
+                by_length[len].push_back(make_int2((int)i, k));
+            }
+        }
+        w.task_offset = plan.tasks.size();
+        for (int len = longest; len >= 0; --len)
+            plan.tasks.insert(plan.tasks.end(), by_length[len].begin(), by_length[len].end());
+        w.n_tasks = plan.tasks.size() - w.task_offset;
+    }
+    return CHIARO_OK;
+}
+
+// Device copies of a plan: descriptors (path pointers into the scratch), tasks,
+// one task counter per wave and the error word.
+struct BatchDevice {
+    SgmInstance *descs;
+    int2 *tasks;
+    unsigned *counters;
+    int *error;
+    float *scratch;
+};
+
+template <int KMAX>
+int batch_blocks_per_sm(int warps) {
+    int blocks = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, sgm_batch_paths_kernel<KMAX>, 32 * warps, 0));
+    return std::max(blocks, 1);
+}
+
+template <int KMAX>
+void enqueue_batch_kmax(chiaro_depth_ctx *ctx, const BatchPlan &plan, const BatchDevice &dev, int warps,
+                        int blocks_per_sm) {
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemsetAsync(dev.error, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(dev.counters, 0, plan.waves.size() * sizeof(unsigned), s));
+    const unsigned sum_blocks = (unsigned)ctx->sm_count * 16;
+    for (size_t w = 0; w < plan.waves.size(); ++w) {
+        const BatchWave &wave = plan.waves[w];
+        if (wave.count == 0) continue;
+        sgm_batch_paths_kernel<KMAX><<<(unsigned)(ctx->sm_count * blocks_per_sm), 32 * warps, 0, s>>>(
+            dev.descs, dev.tasks + wave.task_offset, (unsigned)wave.n_tasks, dev.counters + w, dev.error);
+        CK(cudaGetLastError());
+        sgm_batch_sum_kernel<<<sum_blocks, 256, 0, s>>>(dev.descs + wave.first, (int)wave.count);
+        CK(cudaGetLastError());
+    }
+}
+
+// The launch's KMAX: the smallest of 2, 4 and 8 label sets that holds every instance.
+int batch_kmax(int kmax) { return kmax <= 2 ? 2 : (kmax <= 4 ? 4 : 8); }
+
+int batch_blocks(const BatchPlan &plan, int warps) {
+    switch (batch_kmax(plan.kmax)) {
+        case 2: return batch_blocks_per_sm<2>(warps);
+        case 4: return batch_blocks_per_sm<4>(warps);
+        default: return batch_blocks_per_sm<8>(warps);
+    }
+}
+
+void enqueue_batch(chiaro_depth_ctx *ctx, const BatchPlan &plan, const BatchDevice &dev, int warps) {
+    const int blocks = batch_blocks(plan, warps);
+    switch (batch_kmax(plan.kmax)) {
+        case 2: enqueue_batch_kmax<2>(ctx, plan, dev, warps, blocks); break;
+        case 4: enqueue_batch_kmax<4>(ctx, plan, dev, warps, blocks); break;
+        default: enqueue_batch_kmax<8>(ctx, plan, dev, warps, blocks); break;
+    }
+}
+
+// Size bucket of the autotuner: the launch's KMAX and log2 of the cells per direction.
+uint64_t batch_bucket(const BatchPlan &plan) {
+    size_t cells = 0;
+    for (const SgmInstance &d : plan.descs) cells += d.cells;
+    int log2 = 0;
+    while ((cells >> log2) > 1) ++log2;
+    return (uint64_t)batch_kmax(plan.kmax) | ((uint64_t)log2 << 8);
+}
+
+int run_batch(chiaro_depth_ctx *ctx, const chiaro_sgm_instance *in, size_t n, size_t scratch_bytes, int flags) {
+    uint64_t key = 1469598103934665603ull;
+    fnv(key, in, n * sizeof(chiaro_sgm_instance));
+    fnv(key, &scratch_bytes, sizeof(scratch_bytes));
+    fnv(key, &flags, sizeof(flags));
+    cudaStream_t s = ctx->stream;
+    ctx->batch_replayed = 0;
+    if ((flags & CHIARO_BATCH_GRAPH) && ctx->batch_exec && ctx->batch_key == key) {
+        CK(cudaGraphLaunch(ctx->batch_exec, s));
+        ctx->batch_replayed = 1;
+    } else {
+        ctx->batch_key = 0;  // any other batch may move the scratch: the cached graph is void
+        BatchPlan plan;
+        const size_t budget = scratch_bytes ? scratch_bytes : ((size_t)16 << 30);
+        if (int st = plan_batch(in, n, budget / sizeof(float), plan)) return st;
+        BatchDevice dev{};
+        dev.scratch = dbuf<float>(ctx, "batch.paths", std::max<size_t>(plan.scratch_floats, 1));
+        for (size_t i = 0; i < plan.descs.size(); ++i) plan.descs[i].paths = dev.scratch + plan.scratch_offset[i];
+        dev.descs = dbuf<SgmInstance>(ctx, "batch.descs", plan.descs.size());
+        dev.tasks = dbuf<int2>(ctx, "batch.tasks", std::max<size_t>(plan.tasks.size(), 1));
+        dev.counters = dbuf<unsigned>(ctx, "batch.counters", plan.waves.size());
+        dev.error = dbuf<int>(ctx, "batch.error", 1);
+        upload(ctx, dev.descs, plan.descs.data(), plan.descs.size());
+        upload(ctx, dev.tasks, plan.tasks.data(), plan.tasks.size());
+        const uint64_t bucket = batch_bucket(plan);
+        int warps = 4;
+        auto tuned = ctx->batch_tuning.find(bucket);
+        if (tuned != ctx->batch_tuning.end()) {
+            warps = tuned->second;
+        } else if (flags & CHIARO_BATCH_AUTOTUNE) {
+            float best_ms = 0.0f;
+            for (int candidate : {1, 2, 4, 8}) {
+                enqueue_batch(ctx, plan, dev, candidate);  // warm
+                CK(cudaEventRecord(ctx->events[0], s));
+                enqueue_batch(ctx, plan, dev, candidate);
+                CK(cudaEventRecord(ctx->events[1], s));
+                CK(cudaEventSynchronize(ctx->events[1]));
+                float ms = 0.0f;
+                CK(cudaEventElapsedTime(&ms, ctx->events[0], ctx->events[1]));
+                if (candidate == 1 || ms < best_ms) {
+                    best_ms = ms;
+                    warps = candidate;
+                }
+            }
+            ctx->batch_tuning[bucket] = warps;
+        }
+        ctx->batch_warps = warps;
+        ctx->batch_waves = (int)plan.waves.size();
+        if (flags & CHIARO_BATCH_GRAPH) {
+            batch_blocks(plan, warps);  // occupancy queried outside the capture
+            if (ctx->batch_exec) {
+                CK(cudaGraphExecDestroy(ctx->batch_exec));
+                ctx->batch_exec = nullptr;
+            }
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_batch(ctx, plan, dev, warps);
+            } catch (const CudaError &) {
+                cudaStreamEndCapture(s, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            CK(cudaStreamEndCapture(s, &graph));
+            cudaError_t e = cudaGraphInstantiate(&ctx->batch_exec, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(e);
+            CK(cudaGraphLaunch(ctx->batch_exec, s));
+            ctx->batch_key = key;
+        } else {
+            enqueue_batch(ctx, plan, dev, warps);
+        }
+    }
+    int error = 0;
+    int *d_error = dbuf<int>(ctx, "batch.error", 1);
+    CK(cudaMemcpyAsync(&error, d_error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (error) throw CudaError{cudaErrorInvalidValue, "batched SGM: an instance's label count exceeds the launch"};
+    return CHIARO_OK;
 }
 
 // ---- the stage ------------------------------------------------------------------------
@@ -909,6 +1139,7 @@ void chiaro_depth_ctx_destroy(chiaro_depth_ctx *ctx) {
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (auto &e : ctx->events)
         if (e) cudaEventDestroy(e);
+    if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
     if (ctx->planes_ready) cudaEventDestroy(ctx->planes_ready);
     if (ctx->map_ready) cudaEventDestroy(ctx->map_ready);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
@@ -1209,6 +1440,27 @@ int chiaro_sgm_aggregate_u16(chiaro_depth_ctx *ctx, const float *costs, const fl
     } catch (const CudaError &e) {
         return fail(ctx, e);
     }
+    return CHIARO_OK;
+}
+
+int chiaro_sgm_aggregate_batch_device(chiaro_depth_ctx *ctx, const chiaro_sgm_instance *instances,
+                                      uint64_t n_instances, uint64_t scratch_bytes, int flags) {
+    if (!ctx || (!instances && n_instances) || (flags & ~(CHIARO_BATCH_GRAPH | CHIARO_BATCH_AUTOTUNE)))
+        return CHIARO_ERR_ARGUMENT;
+    if (n_instances == 0) return CHIARO_OK;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        return run_batch(ctx, instances, (size_t)n_instances, (size_t)scratch_bytes, flags);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+}
+
+int chiaro_sgm_batch_report(const chiaro_depth_ctx *ctx, int *warps_per_cta, int *waves, int *replayed) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    if (warps_per_cta) *warps_per_cta = ctx->batch_warps;
+    if (waves) *waves = ctx->batch_waves;
+    if (replayed) *replayed = ctx->batch_replayed;
     return CHIARO_OK;
 }
 

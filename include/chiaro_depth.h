@@ -333,6 +333,41 @@ int chiaro_sgm_aggregate_u16_device(chiaro_depth_ctx *ctx, const float *costs,
                                     const float *guidance, uint64_t columns, uint64_t rows,
                                     uint64_t labels, uint16_t *aggregate, uint16_t *best);
 
+/* ---- batched SGM -------------------------------------------------------------- */
+
+/* One SGM instance of a batch: every array in device memory of the context's
+ * device. out receives semi_global_costs of (costs, guidance), bit-identical to
+ * chiaro_sgm_aggregate_device on the same instance. */
+typedef struct chiaro_sgm_instance {
+    const float *costs;     /* [columns * rows][labels] */
+    const float *guidance;  /* [columns * rows] */
+    float *out;             /* [columns * rows][labels] */
+    uint64_t columns, rows, labels;
+} chiaro_sgm_instance;
+
+enum {
+    CHIARO_BATCH_GRAPH = 1,    /* capture the batch in a CUDA graph; replay it while the batch is unchanged */
+    CHIARO_BATCH_AUTOTUNE = 2  /* time the launch shapes once per size bucket and keep the fastest */
+};
+
+/* No counterpart in the reference (which runs each grouping's SGM on its own):
+ * all reference/source groupings of a capture, or of many captures, as one
+ * batch of SGM instances of uneven sizes and label counts (labels <= 256). A
+ * persistent kernel walks every path of every direction of every instance from
+ * a work list (longest paths first), then one kernel forms each instance's
+ * ordered sum. Each instance needs 8 x its volume of path scratch; instances
+ * run in waves whose scratch fits in scratch_bytes (0: 16 GiB), and an
+ * instance larger than that returns CHIARO_ERR_CAPACITY. flags: see above. A
+ * captured graph refers to the context's scratch and the instances' pointers:
+ * it is replayed only while both are unchanged, and re-captured otherwise. */
+int chiaro_sgm_aggregate_batch_device(chiaro_depth_ctx *ctx, const chiaro_sgm_instance *instances,
+                                      uint64_t n_instances, uint64_t scratch_bytes, int flags);
+
+/* How the last batch ran: warps per CTA of the persistent kernel, number of
+ * waves, and whether a captured graph was replayed (1) rather than launched or
+ * captured (0). Any pointer may be NULL. */
+int chiaro_sgm_batch_report(const chiaro_depth_ctx *ctx, int *warps_per_cta, int *waves, int *replayed);
+
 /* ---- input plane --------------------------------------------------------- */
 
 /* VignettingMesh (calibration.rs:354-358): a columns x rows grid of flat-field
