@@ -284,6 +284,7 @@ def run_ours(args, rank, world, local):
     e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
 
     quantised = quantised_sgm(args, scene, work, ctx, torch, device, stream, flush)
+    batched = batched_sgm(args, ctx, torch, device, stream, flush)
 
     peaks = measured_peaks()
     sgm_s = stage_ms["sgm"] / 1e3
@@ -313,6 +314,8 @@ def run_ours(args, rank, world, local):
         "quantised_sgm": dict(quantised, roofline=dict(
             quantised["roofline"], peak=peaks["hbm_gbs"],
             frac=round(quantised["roofline"]["achieved"] / peaks["hbm_gbs"], 4))),
+        "batched_sgm": dict(batched, note="SGM of many instances of uneven sizes and label counts: "
+                            "per-instance calls (plain) against one persistent batch replayed from a CUDA graph"),
         "compute_roofline": {"kernel": "cost_volume_kernel (build_cost_volume, the largest correlation kernel)",
                              "bound": "fp32", "achieved": round(cost_tflops, 2), "peak": round(fp32_peak, 1),
                              "unit": "TFLOP/s", "frac": round(cost_tflops / fp32_peak, 4),
@@ -393,6 +396,79 @@ def quantised_sgm(args, scene, work, ctx, torch, device, stream, flush):
                                  "tested_nodes": int(tested.sum())},
             "roofline": {"bound": "hbm", "achieved": round(u16_bytes / (u16_ms / 1e3) / 1e9, 1), "unit": "GB/s",
                          "algorithmic_bytes": u16_bytes}}
+
+
+# Config 2: the reference/source groupings of one capture as SGM instances (raster W x H,
+# planes); coarse grid step 8. Config 4: 32 such captures.
+GROUPINGS = [(4160, 3120, 128), (4160, 3120, 192), (3120, 2340, 64), (3120, 2340, 128), (2080, 1560, 192),
+             (2080, 1560, 64), (2080, 1560, 128), (1560, 1170, 192), (1040, 780, 64), (1040, 780, 128)]
+
+
+def batched_sgm(args, ctx, torch, device, stream, flush):
+    """Configs 2 and 4: the SGM of many instances of uneven sizes and label counts, as plain
+    per-instance calls and as one batch (persistent work list, graph replay, autotuned),
+    both timed with CUDA events on the library's stream. Costs are seeded synthetic
+    volumes of each instance's shape (SGM time does not depend on the values)."""
+    from chiaro_b200 import abi
+    gen = torch.Generator(device=device)
+    gen.manual_seed(args.seed)
+    result = {}
+    for name, captures in (("config2", 1), ("config4", 32)):
+        shapes = []
+        for _ in range(captures):
+            for w, h, planes in GROUPINGS:
+                shapes.append((-(-w // 8) + 1, -(-h // 8) + 1, planes + 1))
+        tensors = []
+        arr = (abi.SgmInstanceC * len(shapes))()
+        for i, (c, r, d) in enumerate(shapes):
+            costs = torch.rand(c * r * d, generator=gen, device=device) * 2.25
+            guidance = torch.rand(c * r, generator=gen, device=device) * 7.0
+            out = torch.empty(c * r * d, device=device)
+            tensors += [costs, guidance, out]
+            arr[i] = abi.SgmInstanceC(costs.data_ptr(), guidance.data_ptr(), out.data_ptr(), c, r, d)
+        cells = sum(c * r * d for c, r, d in shapes) * 8
+        nbytes = sum(c * r * d * 8 + 8 * c * r * 4 for c, r, d in shapes)
+        lib = ctx.lib
+
+        def plain():
+            for i, (c, r, d) in enumerate(shapes):
+                ctx.check(lib.chiaro_sgm_aggregate_device(ctx.handle, arr[i].costs, arr[i].guidance, c, r, d,
+                                                          arr[i].out))
+
+        def batched():
+            ctx.check(lib.chiaro_sgm_aggregate_batch_device(ctx.handle, arr, len(shapes), 0,
+                                                            abi.BATCH_GRAPH | abi.BATCH_AUTOTUNE))
+
+        times = {}
+        for label, fn in (("plain", plain), ("batched", batched)):
+            for _ in range(max(args.warmup, 2)):
+                fn()
+            total = 0.0
+            steps = max(1, min(args.steps, 5))
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                fn()
+                with torch.cuda.stream(stream):
+                    e1.record(stream)
+                e1.synchronize()
+                total += e0.elapsed_time(e1)
+            times[label] = total / steps
+        w, waves, rep = C.c_int(), C.c_int(), C.c_int()
+        lib.chiaro_sgm_batch_report(ctx.handle, C.byref(w), C.byref(waves), C.byref(rep))
+        result[name] = {"instances": len(shapes), "sgm_cells": cells,
+                        "plain_ms": round(times["plain"], 3), "batched_ms": round(times["batched"], 3),
+                        "plain_gcells_s": round(cells / times["plain"] / 1e6, 2),
+                        "batched_gcells_s": round(cells / times["batched"] / 1e6, 2),
+                        "speedup": round(times["plain"] / times["batched"], 3),
+                        "warps_per_cta": w.value, "waves": waves.value, "graph_replayed": bool(rep.value),
+                        "hbm_achieved_gbs": round(nbytes / times["batched"] / 1e6, 1),
+                        "algorithmic_bytes": nbytes}
+        del tensors
+        torch.cuda.empty_cache()
+    return result
 
 
 def run_reference(args, rank, world):
