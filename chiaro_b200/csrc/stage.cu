@@ -27,6 +27,7 @@
 #include "sgm.cuh"
 #include "sgm_u16.cuh"
 #include "sgm_batch.cuh"
+#include "sgm_band.cuh"
 
 using namespace chiaro;
 
@@ -473,6 +474,78 @@ int run_batch(chiaro_depth_ctx *ctx, const chiaro_sgm_instance *in, size_t n, si
     CK(cudaMemcpyAsync(&error, d_error, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (error) throw CudaError{cudaErrorInvalidValue, "batched SGM: an instance's label count exceeds the launch"};
+    return CHIARO_OK;
+}
+
+// ---- banded SGM with windowed fallback (sgm_band.cuh) ----------------------------------
+int run_band(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, int columns, int rows, int labels,
+             const int *tile_offset, int tile, int band, int margin, int *winner, uint8_t *fallback) {
+    cudaStream_t s = ctx->stream;
+    const int tiles_x = (columns + tile - 1) / tile, tiles_y = (rows + tile - 1) / tile, tiles = tiles_x * tiles_y;
+    int *bad = dbuf<int>(ctx, "band.bad", 1);
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    band_check_kernel<<<(unsigned)div_ceil(tiles, 256), 256, 0, s>>>(tile_offset, tiles, labels, band, bad);
+    CK(cudaGetLastError());
+    int h_bad = 0;
+    CK(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h_bad) return CHIARO_ERR_ARGUMENT;
+    const BandGrid grid{tile_offset, tile, tiles_x, band};
+    const size_t nodes = (size_t)columns * rows, pitch = (nodes * band + 63) / 64 * 64;
+    float *paths = dbuf<float>(ctx, "band.paths", 8 * pitch);
+    CK(cudaMemsetAsync(fallback, 0, tiles, s));
+    sgm_band_paths_kernel<<<(unsigned)div_ceil(sgm_total_paths(columns, rows), SGM_PATHS_PER_CTA),
+                            32 * SGM_PATHS_PER_CTA, 0, s>>>(costs, guidance, grid, paths, pitch, columns, rows, labels);
+    CK(cudaGetLastError());
+    sgm_band_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, s>>>(paths, pitch, grid, columns, rows,
+                                                                               winner, fallback);
+    CK(cudaGetLastError());
+    std::vector<uint8_t> flags(tiles);
+    CK(cudaMemcpyAsync(flags.data(), fallback, tiles, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // windows of the tiles that fell back
+    std::vector<BandWindow> windows;
+    size_t cost_floats = 0, node_floats = 0;
+    for (int ty = 0; ty < tiles_y; ++ty)
+        for (int tx = 0; tx < tiles_x; ++tx) {
+            if (!flags[ty * tiles_x + tx]) continue;
+            BandWindow w{};
+            w.tc0 = tx * tile;
+            w.tr0 = ty * tile;
+            w.tc = std::min(columns, w.tc0 + tile) - w.tc0;
+            w.tr = std::min(rows, w.tr0 + tile) - w.tr0;
+            w.c0 = std::max(0, w.tc0 - margin);
+            w.r0 = std::max(0, w.tr0 - margin);
+            w.wc = std::min(columns, w.tc0 + tile + margin) - w.c0;
+            w.wr = std::min(rows, w.tr0 + tile + margin) - w.r0;
+            w.cost_offset = cost_floats;
+            w.node_offset = node_floats;
+            cost_floats += (size_t)w.wc * w.wr * labels;
+            node_floats += (size_t)w.wc * w.wr;
+            windows.push_back(w);
+        }
+    if (!windows.empty()) {
+        BandWindow *d_windows = dbuf<BandWindow>(ctx, "band.windows", windows.size());
+        float *wcosts = dbuf<float>(ctx, "band.wcosts", cost_floats);
+        float *wagg = dbuf<float>(ctx, "band.wagg", cost_floats);
+        float *wguid = dbuf<float>(ctx, "band.wguid", node_floats);
+        upload(ctx, d_windows, windows.data(), windows.size());
+        band_crop_kernel<<<dim3(64, (unsigned)windows.size()), 256, 0, s>>>(costs, guidance, columns, labels,
+                                                                             d_windows, wcosts, wguid);
+        CK(cudaGetLastError());
+        std::vector<chiaro_sgm_instance> instances(windows.size());
+        for (size_t i = 0; i < windows.size(); ++i) {
+            const BandWindow &w = windows[i];
+            instances[i] = chiaro_sgm_instance{wcosts + w.cost_offset, wguid + w.node_offset, wagg + w.cost_offset,
+                                               (uint64_t)w.wc, (uint64_t)w.wr, (uint64_t)labels};
+        }
+        if (int st = run_batch(ctx, instances.data(), instances.size(), 0, 0)) return st;
+        const int most = tile * tile;
+        band_window_winner_kernel<<<dim3((unsigned)div_ceil((size_t)most * 32, 256), (unsigned)windows.size()), 256,
+                                    0, s>>>(wagg, columns, labels, d_windows, winner);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(s));
     return CHIARO_OK;
 }
 
@@ -1461,6 +1534,59 @@ int chiaro_sgm_batch_report(const chiaro_depth_ctx *ctx, int *warps_per_cta, int
     if (warps_per_cta) *warps_per_cta = ctx->batch_warps;
     if (waves) *waves = ctx->batch_waves;
     if (replayed) *replayed = ctx->batch_replayed;
+    return CHIARO_OK;
+}
+
+static int band_args(const void *ctx, const float *costs, const float *guidance, uint64_t columns, uint64_t rows,
+                     uint64_t labels, const int32_t *offsets, uint64_t tile, uint64_t band, uint64_t margin,
+                     const int32_t *winner, const uint8_t *fallback) {
+    if (!ctx || !costs || !guidance || !offsets || !winner || !fallback || columns < 1 || rows < 1 || tile < 1 ||
+        tile > 1024 || band < 1 || band > 32 || labels < band + 1 || labels > MAX_LABELS || margin > 4096 ||
+        columns * rows > (1u << 26))
+        return CHIARO_ERR_ARGUMENT;
+    return CHIARO_OK;
+}
+
+int chiaro_sgm_banded_device(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, uint64_t columns,
+                             uint64_t rows, uint64_t labels, const int32_t *tile_offsets, uint64_t tile,
+                             uint64_t band, uint64_t margin, int32_t *winner, uint8_t *fallback) {
+    if (int st = band_args(ctx, costs, guidance, columns, rows, labels, tile_offsets, tile, band, margin, winner,
+                           fallback))
+        return st;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        return run_band(ctx, costs, guidance, (int)columns, (int)rows, (int)labels, tile_offsets, (int)tile,
+                        (int)band, (int)margin, winner, fallback);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+}
+
+int chiaro_sgm_banded(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, uint64_t columns,
+                      uint64_t rows, uint64_t labels, const int32_t *tile_offsets, uint64_t tile, uint64_t band,
+                      uint64_t margin, int32_t *winner, uint8_t *fallback) {
+    if (int st = band_args(ctx, costs, guidance, columns, rows, labels, tile_offsets, tile, band, margin, winner,
+                           fallback))
+        return st;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        const size_t n = columns * rows, nl = n * labels;
+        const size_t tiles = ((columns + tile - 1) / tile) * ((rows + tile - 1) / tile);
+        float *dc = dbuf<float>(ctx, "op.costs", nl), *dg = dbuf<float>(ctx, "op.guidance", n);
+        int *doff = dbuf<int>(ctx, "op.band_offsets", tiles), *dw = dbuf<int>(ctx, "op.band_winner", n);
+        uint8_t *df = dbuf<uint8_t>(ctx, "op.band_fallback", tiles);
+        upload(ctx, dc, costs, nl);
+        upload(ctx, dg, guidance, n);
+        upload(ctx, doff, tile_offsets, tiles);
+        int st = run_band(ctx, dc, dg, (int)columns, (int)rows, (int)labels, doff, (int)tile, (int)band, (int)margin,
+                          dw, df);
+        if (st) return st;
+        download(ctx, winner, dw, n);
+        download(ctx, fallback, df, tiles);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
     return CHIARO_OK;
 }
 

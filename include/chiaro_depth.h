@@ -368,6 +368,26 @@ int chiaro_sgm_aggregate_batch_device(chiaro_depth_ctx *ctx, const chiaro_sgm_in
  * captured (0). Any pointer may be NULL. */
 int chiaro_sgm_batch_report(const chiaro_depth_ctx *ctx, int *warps_per_cta, int *waves, int *replayed);
 
+/* ---- banded SGM ------------------------------------------------------------------ */
+
+/* No counterpart in the reference: the band-limited SGM of the learned-band
+ * design. The grid is cut into tiles of tile x tile nodes; tile t's nodes
+ * aggregate only the labels [tile_offsets[t], tile_offsets[t] + band)
+ * (1 <= offset <= labels - band, band <= 32; tiles row-major, ceil(columns /
+ * tile) per row) with the recurrence of semi_global_costs (depth.rs:1363-1381),
+ * the band shifting between tiles along each path. winner[node] is the label of
+ * the first minimum over the band. A tile whose winner sits on a band edge at
+ * any node falls back (fallback[t] = 1): the full-range SGM over the tile grown
+ * by `margin` nodes decides its nodes' winners (labels 1..labels-1). The _device
+ * form takes device pointers. */
+int chiaro_sgm_banded(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, uint64_t columns,
+                      uint64_t rows, uint64_t labels, const int32_t *tile_offsets, uint64_t tile,
+                      uint64_t band, uint64_t margin, int32_t *winner, uint8_t *fallback);
+int chiaro_sgm_banded_device(chiaro_depth_ctx *ctx, const float *costs, const float *guidance,
+                             uint64_t columns, uint64_t rows, uint64_t labels,
+                             const int32_t *tile_offsets, uint64_t tile, uint64_t band,
+                             uint64_t margin, int32_t *winner, uint8_t *fallback);
+
 /* ---- input plane --------------------------------------------------------- */
 
 /* VignettingMesh (calibration.rs:354-358): a columns x rows grid of flat-field

@@ -2076,4 +2076,126 @@ void oracle_sgm_u16(const float *costs, const float *guidance, size_t columns, s
     }
 }
 
+// ---- banded SGM with windowed full-range fallback (no counterpart in the reference) -----
+// The project's band-limited form of semi_global_costs (depth.rs:1279-1383): every node
+// of a tile (tile x tile coarse nodes) aggregates only the labels [O, O + band) of its
+// tile's offset O (1 <= O <= D - band: finite labels). Along a path the band may shift
+// between tiles: the previous node's value for label l is its slot l - O_prev when that
+// lies in its band, +inf otherwise, and the recurrence of accumulate_path
+// (depth.rs:1363-1381) is otherwise unchanged, the minimum taken over the previous band.
+// The 8 path costs are added per slot in the reference's order and the winner is the
+// first minimum over the band. A tile whose winner sits on a band edge (slot 0 or
+// band - 1) at any of its nodes falls back: the full-range SGM over the window of the
+// tile grown by `margin` nodes (clipped to the grid) decides its nodes' winners (over
+// labels 1..D-1, first minimum).
+static void accumulate_path_banded(const float *data, const float *guidance, const int *node_offset, float *output,
+                                   size_t labels, size_t band, const std::vector<size_t> &path) {
+    const float inf = std::numeric_limits<float>::infinity();
+    std::vector<float> previous(band), current(band);
+    for (size_t k = 0; k < path.size(); ++k) {
+        size_t node = path[k];
+        const float *c = data + node * labels + node_offset[node];
+        float *o = output + node * band;
+        if (k == 0) {
+            for (size_t j = 0; j < band; ++j) {
+                previous[j] = c[j];
+                o[j] += previous[j];
+            }
+            continue;
+        }
+        size_t prior = path[k - 1];
+        float edge = std::fabs(guidance[node] - guidance[prior]);
+        float edge_scale = 1.0f / (1.0f + 4.0f * edge);
+        float p1 = 0.06f * fmax_r(edge_scale, 0.35f);
+        float p2 = 0.45f * fmax_r(edge_scale, 0.12f);
+        float minimum_previous = inf;
+        for (size_t j = 0; j < band; ++j) minimum_previous = fmin_r(minimum_previous, previous[j]);
+        long delta = (long)node_offset[node] - (long)node_offset[prior];
+        for (size_t j = 0; j < band; ++j) {
+            long label = node_offset[node] + (long)j, s = (long)j + delta;
+            auto at = [&](long slot) { return slot >= 0 && slot < (long)band ? previous[slot] : inf; };
+            float same = at(s);
+            float lower = label > 0 ? at(s - 1) + p1 : inf;
+            float higher = label + 1 < (long)labels ? at(s + 1) + p1 : inf;
+            float jump = minimum_previous + p2;
+            current[j] = c[j] + fmin_r(fmin_r(fmin_r(same, lower), higher), jump) - minimum_previous;
+            o[j] += current[j];
+        }
+        std::swap(previous, current);
+    }
+}
+
+static void sgm_paths_generic(size_t columns, size_t rows, const std::function<void(const std::vector<size_t> &)> &walk) {
+    std::vector<size_t> forward, reverse;
+    auto both = [&](const std::vector<size_t> &path) {
+        walk(path);
+        reverse.assign(path.rbegin(), path.rend());
+        walk(reverse);
+    };
+    for (size_t row = 0; row < rows; ++row) {
+        forward.clear();
+        for (size_t column = 0; column < columns; ++column) forward.push_back(row * columns + column);
+        both(forward);
+    }
+    for (size_t column = 0; column < columns; ++column) {
+        forward.clear();
+        for (size_t row = 0; row < rows; ++row) forward.push_back(row * columns + column);
+        both(forward);
+    }
+    for (int mirrored = 0; mirrored < 2; ++mirrored)
+        for (const auto &path : diagonal_paths(columns, rows, mirrored != 0)) both(path);
+}
+
+// Winner labels of the banded SGM with fallback; fallback[t] = 1 for tiles that fell back.
+int oracle_sgm_banded(const float *costs, const float *guidance, size_t columns, size_t rows, size_t labels,
+                      const int *tile_offset, size_t tile, size_t band, size_t margin, int *winner,
+                      uint8_t *fallback) {
+    if (band < 1 || band > 32 || band + 1 > labels || tile < 1) return CHIARO_ERR_ARGUMENT;
+    size_t n = columns * rows, tiles_x = div_ceil(columns, tile), tiles_y = div_ceil(rows, tile);
+    std::vector<int> node_offset(n);
+    for (size_t r = 0; r < rows; ++r)
+        for (size_t c = 0; c < columns; ++c) {
+            int o = tile_offset[(r / tile) * tiles_x + c / tile];
+            if (o < 1 || o + band > labels) return CHIARO_ERR_ARGUMENT;
+            node_offset[r * columns + c] = o;
+        }
+    std::vector<float> output(n * band, 0.0f);
+    sgm_paths_generic(columns, rows, [&](const std::vector<size_t> &path) {
+        accumulate_path_banded(costs, guidance, node_offset.data(), output.data(), labels, band, path);
+    });
+    std::fill(fallback, fallback + tiles_x * tiles_y, 0);
+    for (size_t node = 0; node < n; ++node) {
+        const float *o = output.data() + node * band;
+        size_t best = 0;
+        for (size_t j = 1; j < band; ++j)
+            if (total_key_f32(o[j]) < total_key_f32(o[best])) best = j;
+        winner[node] = node_offset[node] + (int)best;
+        if (best == 0 || best + 1 == band) fallback[((node / columns) / tile) * tiles_x + (node % columns) / tile] = 1;
+    }
+    for (size_t ty = 0; ty < tiles_y; ++ty)
+        for (size_t tx = 0; tx < tiles_x; ++tx) {
+            if (!fallback[ty * tiles_x + tx]) continue;
+            size_t c0 = tx * tile > margin ? tx * tile - margin : 0, r0 = ty * tile > margin ? ty * tile - margin : 0;
+            size_t c1 = std::min(columns, (tx + 1) * tile + margin), r1 = std::min(rows, (ty + 1) * tile + margin);
+            size_t wc = c1 - c0, wr = r1 - r0;
+            std::vector<float> wcost(wc * wr * labels), wguid(wc * wr);
+            for (size_t r = 0; r < wr; ++r)
+                for (size_t c = 0; c < wc; ++c) {
+                    size_t src = (r0 + r) * columns + c0 + c;
+                    wguid[r * wc + c] = guidance[src];
+                    std::copy(costs + src * labels, costs + (src + 1) * labels, wcost.begin() + (r * wc + c) * labels);
+                }
+            auto agg = semi_global_costs(wcost.data(), wguid.data(), wc, wr, labels);
+            for (size_t r = ty * tile; r < std::min(rows, (ty + 1) * tile); ++r)
+                for (size_t c = tx * tile; c < std::min(columns, (tx + 1) * tile); ++c) {
+                    const float *o = agg.data() + ((r - r0) * wc + (c - c0)) * labels;
+                    size_t best = 1;
+                    for (size_t l = 2; l < labels; ++l)
+                        if (total_key_f32(o[l]) < total_key_f32(o[best])) best = l;
+                    winner[r * columns + c] = (int)best;
+                }
+        }
+    return CHIARO_OK;
+}
+
 }  // extern "C"
