@@ -28,6 +28,7 @@
 #include "sgm_u16.cuh"
 #include "sgm_batch.cuh"
 #include "sgm_band.cuh"
+#include "bandnet.cuh"
 
 using namespace chiaro;
 
@@ -547,6 +548,89 @@ int run_band(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, i
     }
     CK(cudaStreamSynchronize(s));
     return CHIARO_OK;
+}
+
+// ---- learned band network (bandnet.cuh) ----------------------------------------------
+struct NetState {
+    __nv_bfloat16 *w, *wt;             // packed weights and their transposed, mirrored copy
+    __nv_bfloat16 *act[NET_LAYERS + 1];  // act[0] = features, act[l + 1] = output of layer l
+    __nv_bfloat16 *grad_a, *grad_b;    // pre-activation gradients, ping-pong
+    float *y;                          // channel 0 of the last layer, fp32
+    long pixels;
+    int images, height, width;
+};
+
+NetState net_state(chiaro_depth_ctx *ctx, int images, int height, int width) {
+    NetState s{};
+    s.images = images;
+    s.height = height;
+    s.width = width;
+    s.pixels = (long)images * height * width;
+    const size_t act = (size_t)s.pixels * NET_CH;
+    s.w = dbuf<__nv_bfloat16>(ctx, "net.w", (size_t)NET_LAYERS * NET_W);
+    s.wt = dbuf<__nv_bfloat16>(ctx, "net.wt", (size_t)NET_LAYERS * NET_W);
+    for (int l = 0; l <= NET_LAYERS; ++l) s.act[l] = dbuf<__nv_bfloat16>(ctx, "net.act" + std::to_string(l), act);
+    s.grad_a = dbuf<__nv_bfloat16>(ctx, "net.grad_a", act);
+    s.grad_b = dbuf<__nv_bfloat16>(ctx, "net.grad_b", act);
+    s.y = dbuf<float>(ctx, "net.y", (size_t)s.pixels);
+    return s;
+}
+
+void net_features(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, const float *guidance, int labels) {
+    const int nodes = (int)s.pixels;
+    net_features_kernel<<<(unsigned)div_ceil((size_t)nodes, 256), 256, 0, ctx->stream>>>(costs, guidance, nodes,
+                                                                                          labels, s.act[0]);
+    CK(cudaGetLastError());
+}
+
+void net_forward(chiaro_depth_ctx *ctx, const NetState &s, const float *params) {
+    cudaStream_t st = ctx->stream;
+    net_pack_kernel<<<(unsigned)div_ceil((size_t)NET_LAYERS * NET_W, 256), 256, 0, st>>>(params, s.w, s.wt);
+    CK(cudaGetLastError());
+    const long tiles = (long)s.images * s.height * ((s.width + 15) / 16);
+    const unsigned blocks = (unsigned)div_ceil((size_t)tiles, 4);
+    for (int l = 0; l < NET_LAYERS; ++l) {
+        const bool last = l + 1 == NET_LAYERS;
+        net_conv_kernel<<<blocks, 128, 0, st>>>(s.act[l], s.images, s.height, s.width, s.w + (size_t)l * NET_W,
+                                                params + (size_t)l * (NET_W + NET_CH) + NET_W, last ? 0 : 1,
+                                                nullptr, s.act[l + 1], last ? s.y : nullptr);
+        CK(cudaGetLastError());
+    }
+}
+
+// One forward and backward over the batch: grads (fp32, the parameters' layout)
+// and the loss added into *loss_sum (device).
+void net_backward(chiaro_depth_ctx *ctx, const NetState &s, const float *params, const float *targets,
+                  const uint8_t *mask, float inverse_count, float *grads, float *loss_sum) {
+    cudaStream_t st = ctx->stream;
+    net_forward(ctx, s, params);
+    CK(cudaMemsetAsync(grads, 0, sizeof(float) * NET_PARAMS, st));
+    const unsigned eblocks = (unsigned)std::min<size_t>(div_ceil((size_t)s.pixels, 256), (size_t)ctx->sm_count * 8);
+    net_loss_kernel<<<eblocks, 256, 0, st>>>(s.y, targets, mask, s.pixels, inverse_count, 0.02f, s.grad_a, loss_sum);
+    CK(cudaGetLastError());
+    const long tiles = (long)s.images * s.height * ((s.width + 15) / 16);
+    const unsigned cblocks = (unsigned)div_ceil((size_t)tiles, 4);
+    const long chunks = (s.pixels + 16L * NET_WGRAD_STEPS - 1) / (16L * NET_WGRAD_STEPS);
+    const unsigned wblocks = (unsigned)div_ceil((size_t)chunks * NET_TAPS, 4);
+    __nv_bfloat16 *dpre = s.grad_a, *dnext = s.grad_b;
+    for (int l = NET_LAYERS - 1; l >= 0; --l) {
+        float *g = grads + (size_t)l * (NET_W + NET_CH);
+        net_wgrad_kernel<<<wblocks, 128, 0, st>>>(s.act[l], dpre, s.images, s.height, s.width, g);
+        net_bias_grad_kernel<<<(unsigned)ctx->sm_count * 4, 256, 0, st>>>(dpre, s.pixels, g + NET_W);
+        CK(cudaGetLastError());
+        if (l > 0) {  // gradient at the previous layer's output, masked by its ReLU
+            net_conv_kernel<<<cblocks, 128, 0, st>>>(dpre, s.images, s.height, s.width, s.wt + (size_t)l * NET_W,
+                                                     nullptr, 0, s.act[l], dnext, nullptr);
+            CK(cudaGetLastError());
+            std::swap(dpre, dnext);
+        }
+    }
+}
+
+// Normalised targets (label - 1) / (labels - 2) and the mask of scored nodes.
+__global__ void net_targets_kernel(const int *__restrict__ winners, long pixels, int labels, float *targets) {
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < pixels) targets[p] = (float)(winners[p] - 1) / (float)(labels - 2);
 }
 
 // ---- the stage ------------------------------------------------------------------------
@@ -1583,6 +1667,111 @@ int chiaro_sgm_banded(chiaro_depth_ctx *ctx, const float *costs, const float *gu
         if (st) return st;
         download(ctx, winner, dw, n);
         download(ctx, fallback, df, tiles);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+uint64_t chiaro_bandnet_parameter_count(void) { return NET_PARAMS; }
+
+static int bandnet_args(const void *ctx, uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels) {
+    if (!ctx || images < 1 || columns < 1 || rows < 1 || labels < 1 + NET_BINS + 2 || labels > MAX_LABELS ||
+        images * columns * rows > (1u << 26))
+        return CHIARO_ERR_ARGUMENT;
+    return CHIARO_OK;
+}
+
+// Batch setup shared by training and the gradient: features, targets, and
+// 1 / (number of scored nodes) from the mask.
+static float bandnet_batch(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, const float *guidance,
+                           const int32_t *winners, const uint8_t *mask, int labels, float **targets) {
+    net_features(ctx, s, costs, guidance, labels);
+    *targets = dbuf<float>(ctx, "net.targets", (size_t)s.pixels);
+    net_targets_kernel<<<(unsigned)div_ceil((size_t)s.pixels, 256), 256, 0, ctx->stream>>>(winners, s.pixels, labels,
+                                                                                           *targets);
+    CK(cudaGetLastError());
+    std::vector<uint8_t> h(s.pixels);
+    CK(cudaMemcpyAsync(h.data(), mask, s.pixels, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    size_t count = 0;
+    for (uint8_t m : h) count += m != 0;
+    return count ? 1.0f / (float)count : 0.0f;
+}
+
+int chiaro_bandnet_propose_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
+                                  const float *guidance, uint64_t columns, uint64_t rows, uint64_t labels,
+                                  uint64_t tile, uint64_t band, int32_t *tile_offsets, float *centres) {
+    if (bandnet_args(ctx, 1, columns, rows, labels) || !params || !costs || !guidance || !tile_offsets || tile < 1 ||
+        band < 1 || band > 32 || labels < band + 1)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        NetState s = net_state(ctx, 1, (int)rows, (int)columns);
+        net_features(ctx, s, costs, guidance, (int)labels);
+        net_forward(ctx, s, params);
+        const size_t tiles = ((columns + tile - 1) / tile) * ((rows + tile - 1) / tile);
+        net_tile_offsets_kernel<<<(unsigned)div_ceil(tiles, 128), 128, 0, ctx->stream>>>(
+            s.y, (int)columns, (int)rows, (int)labels, (int)tile, (int)band, tile_offsets);
+        CK(cudaGetLastError());
+        if (centres)
+            CK(cudaMemcpyAsync(centres, s.y, sizeof(float) * columns * rows, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_bandnet_gradient_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
+                                   const float *guidance, const int32_t *winners, const uint8_t *mask,
+                                   uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels, float *grads,
+                                   float *loss) {
+    if (bandnet_args(ctx, images, columns, rows, labels) || !params || !costs || !guidance || !winners || !mask ||
+        !grads || !loss)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        NetState s = net_state(ctx, (int)images, (int)rows, (int)columns);
+        float *targets = nullptr;
+        const float inverse = bandnet_batch(ctx, s, costs, guidance, winners, mask, (int)labels, &targets);
+        float *d_loss = dbuf<float>(ctx, "net.loss", 1);
+        CK(cudaMemsetAsync(d_loss, 0, sizeof(float), ctx->stream));
+        net_backward(ctx, s, params, targets, mask, inverse, grads, d_loss);
+        CK(cudaMemcpyAsync(loss, d_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_bandnet_train_device(chiaro_depth_ctx *ctx, float *params, float *adam_m, float *adam_v,
+                                uint64_t first_step, uint64_t steps, const float *costs, const float *guidance,
+                                const int32_t *winners, const uint8_t *mask, uint64_t images, uint64_t columns,
+                                uint64_t rows, uint64_t labels, float learning_rate, float *losses) {
+    if (bandnet_args(ctx, images, columns, rows, labels) || !params || !adam_m || !adam_v || !costs || !guidance ||
+        !winners || !mask || !(learning_rate > 0.0f) || steps > 100000)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        NetState s = net_state(ctx, (int)images, (int)rows, (int)columns);
+        float *targets = nullptr;
+        const float inverse = bandnet_batch(ctx, s, costs, guidance, winners, mask, (int)labels, &targets);
+        float *grads = dbuf<float>(ctx, "net.grads", NET_PARAMS);
+        float *d_losses = dbuf<float>(ctx, "net.losses", std::max<uint64_t>(steps, 1));
+        CK(cudaMemsetAsync(d_losses, 0, sizeof(float) * std::max<uint64_t>(steps, 1), ctx->stream));
+        const float beta1 = 0.9f, beta2 = 0.999f;
+        for (uint64_t k = 0; k < steps; ++k) {
+            net_backward(ctx, s, params, targets, mask, inverse, grads, d_losses + k);
+            const double t_step = (double)(first_step + k + 1);
+            net_adam_kernel<<<(unsigned)div_ceil((size_t)NET_PARAMS, 256), 256, 0, ctx->stream>>>(
+                params, grads, adam_m, adam_v, learning_rate, beta1, beta2, 1e-8f,
+                (float)(1.0 - std::pow((double)beta1, t_step)), (float)(1.0 - std::pow((double)beta2, t_step)));
+            CK(cudaGetLastError());
+        }
+        if (losses) CK(cudaMemcpyAsync(losses, d_losses, sizeof(float) * steps, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     } catch (const CudaError &e) {
         return fail(ctx, e);

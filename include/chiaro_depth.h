@@ -388,6 +388,45 @@ int chiaro_sgm_banded_device(chiaro_depth_ctx *ctx, const float *costs, const fl
                              const int32_t *tile_offsets, uint64_t tile, uint64_t band,
                              uint64_t margin, int32_t *winner, uint8_t *fallback);
 
+/* ---- learned band proposal ------------------------------------------------------- */
+
+/* No counterpart in the reference (which uses no learned model): the band
+ * proposal network of the banded SGM. Six 3x3 convolutions of 32 channels on
+ * the coarse grid (one pixel per node), bf16 tensor-core kernels with fp32
+ * accumulation. Inputs per node: the reference luminance (guidance) and 16
+ * cost-bin minima over the finite labels (labels >= 19). Parameters are
+ * chiaro_bandnet_parameter_count() fp32 values: per layer the weights
+ * [tap][co][ci] then the 32 biases. All arrays below are device memory; costs
+ * [images][nodes][labels], guidance [images][nodes], winners (the target
+ * labels, e.g. the full-range SGM's) and mask (1 for nodes to learn from)
+ * [images][nodes]. */
+uint64_t chiaro_bandnet_parameter_count(void);
+
+/* Band offsets per tile (as chiaro_sgm_banded takes them): the band centred on
+ * the mean predicted label of the tile's nodes, clamped to [1, labels - band];
+ * centres (optional, [nodes]) receives each node's normalised prediction. */
+int chiaro_bandnet_propose_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
+                                  const float *guidance, uint64_t columns, uint64_t rows,
+                                  uint64_t labels, uint64_t tile, uint64_t band,
+                                  int32_t *tile_offsets, float *centres);
+
+/* `steps` full-batch Adam steps (numbered from first_step + 1) of the Huber loss
+ * between the normalised prediction and (winner - 1) / (labels - 2) on the
+ * masked nodes; losses (host, optional) receives each step's loss. adam_m and
+ * adam_v hold the optimiser state (zero before the first step). */
+int chiaro_bandnet_train_device(chiaro_depth_ctx *ctx, float *params, float *adam_m, float *adam_v,
+                                uint64_t first_step, uint64_t steps, const float *costs,
+                                const float *guidance, const int32_t *winners, const uint8_t *mask,
+                                uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels,
+                                float learning_rate, float *losses);
+
+/* One forward and backward pass: the loss (host) and its gradient (device,
+ * the parameters' layout). */
+int chiaro_bandnet_gradient_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
+                                   const float *guidance, const int32_t *winners, const uint8_t *mask,
+                                   uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels,
+                                   float *grads, float *loss);
+
 /* ---- input plane --------------------------------------------------------- */
 
 /* VignettingMesh (calibration.rs:354-358): a columns x rows grid of flat-field

@@ -2198,4 +2198,120 @@ int oracle_sgm_banded(const float *costs, const float *guidance, size_t columns,
     return CHIARO_OK;
 }
 
+// ---- band proposal network, fp32 (no counterpart in the reference) -------------------------
+// The oracle of the learned band proposal: the same network in plain fp32 loops
+// (NHWC, 32 channels, zero padding, six 3x3 convolutions, ReLU after the first
+// five, Huber loss with delta 0.02 on channel 0 over the masked nodes, mean over
+// them) and its backward pass. Parameters: per layer [tap][co][ci] weights then
+// 32 biases.
+static const int NET_CH_O = 32, NET_LAYERS_O = 6, NET_W_O = 9 * 32 * 32;
+
+void oracle_bandnet_features(const float *costs, const float *guidance, size_t nodes, size_t labels, float *features) {
+    const int bins = 16, finite = (int)labels - 1;
+    for (size_t node = 0; node < nodes; ++node) {
+        const float *c = costs + node * labels;
+        float m[16], lowest = std::numeric_limits<float>::infinity();
+        for (int b = 0; b < bins; ++b) {
+            int l0 = 1 + b * finite / bins, l1 = 1 + (b + 1) * finite / bins;
+            m[b] = std::numeric_limits<float>::infinity();
+            for (int l = l0; l < l1; ++l) m[b] = std::fmin(m[b], c[l]);
+            lowest = std::fmin(lowest, m[b]);
+        }
+        float *f = features + node * NET_CH_O;
+        f[0] = guidance[node] * 0.125f;
+        for (int b = 0; b < bins; ++b) f[1 + b] = m[b] - lowest;
+        for (int k = 1 + bins; k < NET_CH_O; ++k) f[k] = 0.0f;
+    }
+}
+
+static void net_conv_o(const float *in, int images, int h, int w, const float *wt, const float *bias, float *out) {
+    for (int n = 0; n < images; ++n)
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x)
+                for (int co = 0; co < NET_CH_O; ++co) {
+                    double s = bias ? bias[co] : 0.0;
+                    for (int tap = 0; tap < 9; ++tap) {
+                        int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
+                        if (yy < 0 || yy >= h || xx < 0 || xx >= w) continue;
+                        const float *a = in + (((size_t)n * h + yy) * w + xx) * NET_CH_O;
+                        const float *k = wt + ((size_t)tap * NET_CH_O + co) * NET_CH_O;
+                        for (int ci = 0; ci < NET_CH_O; ++ci) s += (double)a[ci] * k[ci];
+                    }
+                    out[(((size_t)n * h + y) * w + x) * NET_CH_O + co] = (float)s;
+                }
+}
+
+// Loss and gradient of the network on a batch; y (optional) receives channel 0.
+void oracle_bandnet_loss_grad(const float *params, const float *features, const float *targets, const uint8_t *mask,
+                              size_t images, size_t height, size_t width, float *grads, float *loss, float *y) {
+    const int h = (int)height, w = (int)width, nimg = (int)images;
+    const size_t pixels = images * height * width, act_n = pixels * NET_CH_O;
+    std::vector<std::vector<float>> act(NET_LAYERS_O + 1, std::vector<float>(act_n));
+    std::copy(features, features + act_n, act[0].begin());
+    for (int l = 0; l < NET_LAYERS_O; ++l) {
+        const float *p = params + (size_t)l * (NET_W_O + NET_CH_O);
+        net_conv_o(act[l].data(), nimg, h, w, p, p + NET_W_O, act[l + 1].data());
+        if (l + 1 < NET_LAYERS_O)
+            for (float &v : act[l + 1]) v = std::fmax(v, 0.0f);
+    }
+    size_t count = 0;
+    for (size_t i = 0; i < pixels; ++i) count += mask[i] != 0;
+    const double inverse = count ? 1.0 / (double)count : 0.0;
+    const float delta = 0.02f;
+    std::vector<float> dpre(act_n, 0.0f), dnext(act_n);
+    double total = 0.0;
+    for (size_t i = 0; i < pixels; ++i) {
+        float yi = act[NET_LAYERS_O][i * NET_CH_O];
+        if (y) y[i] = yi;
+        if (!mask[i]) continue;
+        float e = yi - targets[i], a = std::fabs(e);
+        total += a <= delta ? 0.5 * e * e : delta * (a - 0.5 * delta);
+        dpre[i * NET_CH_O] = (float)((a <= delta ? e : std::copysign(delta, e)) * inverse);
+    }
+    *loss = (float)(total * inverse);
+    std::fill(grads, grads + (size_t)NET_LAYERS_O * (NET_W_O + NET_CH_O), 0.0f);
+    for (int l = NET_LAYERS_O - 1; l >= 0; --l) {
+        const float *p = params + (size_t)l * (NET_W_O + NET_CH_O);
+        float *g = grads + (size_t)l * (NET_W_O + NET_CH_O);
+        std::vector<double> dw(NET_W_O, 0.0), db(NET_CH_O, 0.0);
+        for (int n = 0; n < nimg; ++n)
+            for (int y0 = 0; y0 < h; ++y0)
+                for (int x0 = 0; x0 < w; ++x0) {
+                    const float *d = dpre.data() + (((size_t)n * h + y0) * w + x0) * NET_CH_O;
+                    for (int co = 0; co < NET_CH_O; ++co) db[co] += d[co];
+                    for (int tap = 0; tap < 9; ++tap) {
+                        int yy = y0 + tap / 3 - 1, xx = x0 + tap % 3 - 1;
+                        if (yy < 0 || yy >= h || xx < 0 || xx >= w) continue;
+                        const float *a = act[l].data() + (((size_t)n * h + yy) * w + xx) * NET_CH_O;
+                        for (int co = 0; co < NET_CH_O; ++co) {
+                            if (d[co] == 0.0f) continue;
+                            double *row = dw.data() + ((size_t)tap * NET_CH_O + co) * NET_CH_O;
+                            for (int ci = 0; ci < NET_CH_O; ++ci) row[ci] += (double)d[co] * a[ci];
+                        }
+                    }
+                }
+        for (int i = 0; i < NET_W_O; ++i) g[i] = (float)dw[i];
+        for (int co = 0; co < NET_CH_O; ++co) g[NET_W_O + co] = (float)db[co];
+        if (l == 0) break;
+        // gradient at layer l's input, masked by its ReLU (act[l] is layer l-1's output)
+        std::fill(dnext.begin(), dnext.end(), 0.0f);
+        for (int n = 0; n < nimg; ++n)
+            for (int y0 = 0; y0 < h; ++y0)
+                for (int x0 = 0; x0 < w; ++x0) {
+                    const float *d = dpre.data() + (((size_t)n * h + y0) * w + x0) * NET_CH_O;
+                    for (int tap = 0; tap < 9; ++tap) {
+                        int yy = y0 + tap / 3 - 1, xx = x0 + tap % 3 - 1;
+                        if (yy < 0 || yy >= h || xx < 0 || xx >= w) continue;
+                        float *o = dnext.data() + (((size_t)n * h + yy) * w + xx) * NET_CH_O;
+                        for (int co = 0; co < NET_CH_O; ++co) {
+                            if (d[co] == 0.0f) continue;
+                            const float *k = p + ((size_t)tap * NET_CH_O + co) * NET_CH_O;
+                            for (int ci = 0; ci < NET_CH_O; ++ci) o[ci] += d[co] * k[ci];
+                        }
+                    }
+                }
+        for (size_t i = 0; i < act_n; ++i) dpre[i] = act[l][i] > 0.0f ? dnext[i] : 0.0f;
+    }
+}
+
 }  // extern "C"

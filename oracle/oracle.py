@@ -100,6 +100,9 @@ def lib():
             "oracle_sgm_banded": (C.c_int, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, C.c_size_t,
                                              P(C.c_int), C.c_size_t, C.c_size_t, C.c_size_t, P(C.c_int),
                                              P(C.c_uint8)]),
+            "oracle_bandnet_features": (None, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_float)]),
+            "oracle_bandnet_loss_grad": (None, [P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_uint8), C.c_size_t,
+                                                C.c_size_t, C.c_size_t, P(C.c_float), P(C.c_float), P(C.c_float)]),
             "oracle_sgm_u16": (None, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, C.c_size_t,
                                       P(C.c_uint16), P(C.c_uint16)]),
             "oracle_luminance_half_mesh": (None, [P(C.c_uint16), C.c_size_t, C.c_size_t, C.c_float, C.c_float,

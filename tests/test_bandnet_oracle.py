@@ -1,0 +1,44 @@
+"""The fp32 oracle of the band proposal network (oracle_bandnet_loss_grad): its
+analytic gradient against central finite differences of its loss."""
+import ctypes as C
+
+import numpy as np
+
+from chiaro_b200.bandnet import init_params
+
+F = C.POINTER(C.c_float)
+
+
+def _loss_grad(lib, params, features, targets, mask, images, h, w):
+    grads = np.zeros_like(params)
+    loss = C.c_float()
+    lib.oracle_bandnet_loss_grad(params.ctypes.data_as(F), features.ctypes.data_as(F), targets.ctypes.data_as(F),
+                                 mask.ctypes.data_as(C.POINTER(C.c_uint8)), images, h, w, grads.ctypes.data_as(F),
+                                 C.byref(loss), None)
+    return float(loss.value), grads
+
+
+def test_oracle_gradient_matches_finite_differences(oracle_lib):
+    rng = np.random.default_rng(0)
+    images, h, w = 2, 5, 6
+    params = init_params(1)
+    params += rng.normal(0, 0.02, params.size).astype(np.float32)  # move off the initial zeros
+    features = rng.uniform(0, 1, (images, h, w, 32)).astype(np.float32)
+    features[..., 17:] = 0.0
+    targets = rng.uniform(0, 1, images * h * w).astype(np.float32)
+    mask = (rng.random(images * h * w) < 0.8).astype(np.uint8)
+    loss, grads = _loss_grad(oracle_lib, params, features, targets, mask, images, h, w)
+    assert loss > 0
+    big = np.argsort(-np.abs(grads))[:40]  # the largest entries: well above the finite-difference noise
+    checked = passed = 0
+    for i in big:
+        eps = 1e-3
+        p = params.copy()
+        p[i] += eps
+        lp, _ = _loss_grad(oracle_lib, p, features, targets, mask, images, h, w)
+        p[i] -= 2 * eps
+        lm, _ = _loss_grad(oracle_lib, p, features, targets, mask, images, h, w)
+        fd = (lp - lm) / (2 * eps)
+        checked += 1
+        passed += abs(fd - grads[i]) <= 0.05 * abs(grads[i]) + 1e-5
+    assert passed >= 0.9 * checked, (passed, checked)
