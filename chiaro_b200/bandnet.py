@@ -17,19 +17,22 @@ from typing import List, Optional
 
 import numpy as np
 
+from . import band as bandmod
+
 LAYERS, CH, TAPS = 6, 32, 9
+INPUTS = 19  # live input channels: guidance, 16 cost bins, the cost argmin and the minimum cost
 
 
 def init_params(seed: int = 0) -> np.ndarray:
     """He-initialised fp32 parameters in the library's layout (per layer [tap][co][ci] then 32 biases).
-    The first layer sees 17 live input channels; the last layer's channel 0 starts near the label range's middle."""
+    The first layer sees INPUTS live input channels; the last layer's channel 0 starts near the label range's middle."""
     rng = np.random.default_rng(seed)
     parts = []
     for layer in range(LAYERS):
-        fan_in = TAPS * (17 if layer == 0 else CH)
+        fan_in = TAPS * (INPUTS if layer == 0 else CH)
         w = rng.normal(0.0, np.sqrt(2.0 / fan_in), (TAPS, CH, CH)).astype(np.float32)
         if layer == 0:
-            w[:, :, 17:] = 0.0
+            w[:, :, INPUTS:] = 0.0
         b = np.zeros(CH, np.float32)
         if layer == LAYERS - 1:
             w *= 0.1
@@ -63,6 +66,45 @@ def samples_from_stage(scene, context=None) -> Sample:
                            context=context, debug=dbg)
     winners = (1 + np.argmin(dbg["regularised"].reshape(n, d)[:, 1:], axis=1)).astype(np.int32)
     return Sample(dbg["coarse_costs"], dbg["coarse_guidance"], winners, dbg["coarse_tested"], cc, cr, d)
+
+
+def tile_targets(sample: Sample, tile: int = 4, kind: str = "median") -> Sample:
+    """The band network's training targets: every node of a tile learns one label of the
+    tile's tested winners, their median (``kind="median"``: the band holds the tile's main
+    surface) or the middle of their range (``"midrange"``: a band centred there covers the
+    tile whenever the range fits in it); a tile with no tested node learns label 1, where
+    flat costs need no fallback."""
+    if kind not in ("median", "midrange"):
+        raise ValueError(f"unknown target kind {kind!r}")
+    columns, rows = sample.columns, sample.rows
+    tx, ty = bandmod.tiles_of(columns, rows, tile)
+    winners = sample.winners.reshape(rows, columns)
+    tested = sample.mask.reshape(rows, columns).astype(bool)
+    out = np.ones((rows, columns), np.int32)
+    for y in range(ty):
+        for x in range(tx):
+            block = (slice(y * tile, (y + 1) * tile), slice(x * tile, (x + 1) * tile))
+            w = winners[block][tested[block]]
+            if w.size:
+                out[block] = int(np.rint(np.median(w))) if kind == "median" else (int(w.min()) + int(w.max())) // 2
+    return Sample(sample.costs, sample.guidance, out.reshape(-1), np.ones(columns * rows, np.uint8), columns, rows,
+                  sample.labels)
+
+
+def wide_tile_fraction(sample: Sample, tile: int = 4, band: int = 24) -> float:
+    """The share of tiles whose tested full-range winners span more than band - 3 labels:
+    no band of ``band`` labels holds all of them off its edges, so every proposal method
+    falls back there or disagrees with the full-range SGM."""
+    tx, ty = bandmod.tiles_of(sample.columns, sample.rows, tile)
+    winners = sample.winners.reshape(sample.rows, sample.columns)
+    tested = sample.mask.reshape(sample.rows, sample.columns).astype(bool)
+    wide = 0
+    for y in range(ty):
+        for x in range(tx):
+            block = (slice(y * tile, (y + 1) * tile), slice(x * tile, (x + 1) * tile))
+            w = winners[block][tested[block]]
+            wide += int(w.size > 0 and int(w.max()) - int(w.min()) > band - 3)
+    return wide / (tx * ty)
 
 
 class BandNet:
@@ -121,3 +163,101 @@ class BandNet:
             self.ctx.handle, self.params.data_ptr(), costs.data_ptr(), guidance.data_ptr(), columns, rows, labels,
             tile, band, offsets.data_ptr(), centres.data_ptr() if centres is not None else None))
         return offsets
+
+
+def _render(name: str, seed: int, overrides: dict):
+    from . import scenes
+    return scenes.workload(name, seed=seed, cache=False, **overrides)
+
+
+def render_scenes(name: str, seeds, processes: Optional[int] = None, **overrides):
+    """Render seeded workloads in spawned worker processes (the renderer is numpy on the host;
+    spawned workers are safe after CUDA is initialised in this process). Where workers cannot
+    start (a caller whose main module cannot be re-imported), the scenes render here in turn."""
+    import multiprocessing as mp
+    import os
+    from concurrent.futures import ProcessPoolExecutor
+    from concurrent.futures.process import BrokenProcessPool
+    seeds = list(seeds)
+    processes = processes or max(1, min(len(seeds), os.cpu_count() or 1, 16))
+    if processes > 1:
+        try:
+            with ProcessPoolExecutor(processes, mp_context=mp.get_context("spawn")) as pool:
+                return list(pool.map(_render, [name] * len(seeds), seeds, [overrides] * len(seeds)))
+        except BrokenProcessPool:
+            pass
+    return [_render(name, s, overrides) for s in seeds]
+
+
+def band_winners(context, costs, guidance, columns: int, rows: int, labels: int, offsets, tile: int = 4,
+                 band: int = 24, margin: int = 16):
+    """chiaro_sgm_banded_device on device tensors: (winner labels, fallback flags per tile) as numpy."""
+    import torch
+    tx, ty = bandmod.tiles_of(columns, rows, tile)
+    if isinstance(offsets, np.ndarray):
+        offsets = torch.from_numpy(np.ascontiguousarray(offsets, np.int32)).to(costs.device)
+    winner = torch.empty(columns * rows, dtype=torch.int32, device=costs.device)
+    fallback = torch.empty(tx * ty, dtype=torch.uint8, device=costs.device)
+    context.check(context.lib.chiaro_sgm_banded_device(
+        context.handle, costs.data_ptr(), guidance.data_ptr(), columns, rows, labels, offsets.data_ptr(), tile, band,
+        margin, winner.data_ptr(), fallback.data_ptr()))
+    return winner.cpu().numpy(), fallback.cpu().numpy()
+
+
+@dataclass
+class BandScore:
+    """Winner agreement of a banded SGM with the full-range SGM, summed over images."""
+
+    nodes: int = 0
+    exact: int = 0
+    within_one: int = 0
+    tested: int = 0
+    tested_exact: int = 0
+    tested_within_one: int = 0
+    tiles: int = 0
+    fallback_tiles: int = 0
+    windows: int = 0
+
+    def add(self, winners: np.ndarray, fallback: np.ndarray, sample: Sample) -> None:
+        diff = np.abs(winners.astype(np.int64) - sample.winners)
+        tested = sample.mask.astype(bool)
+        self.nodes += diff.size
+        self.exact += int((diff == 0).sum())
+        self.within_one += int((diff <= 1).sum())
+        self.tested += int(tested.sum())
+        self.tested_exact += int((diff[tested] == 0).sum())
+        self.tested_within_one += int((diff[tested] <= 1).sum())
+        self.tiles += fallback.size
+        self.fallback_tiles += int(fallback.sum())
+
+    def summary(self) -> dict:
+        rate = lambda a, b: round(a / b, 5) if b else None
+        return {"within_one_plane": rate(self.tested_within_one, self.tested),
+                "exact": rate(self.tested_exact, self.tested),
+                "within_one_plane_all_nodes": rate(self.within_one, self.nodes),
+                "fallback_rate": rate(self.fallback_tiles, self.tiles),
+                "fallback_windows": self.windows, "tested_nodes": self.tested, "tiles": self.tiles}
+
+
+def evaluate(context, samples: List[Sample], nets: Optional[dict] = None, tile: int = 4, band: int = 24,
+             margin: int = 16) -> dict:
+    """Banded SGM with fallback against the full-range SGM's winners on each sample: with the
+    naive bands (the median cost argmin of each tile) and with each network of ``nets``
+    ({name: BandNet}). Agreement is over the tested nodes (those with a finite cost)."""
+    import torch
+    nets = nets or {}
+    device = torch.device("cuda", 0) if not nets else next(iter(nets.values())).device
+    scores = {"naive": BandScore(), **{name: BandScore() for name in nets}}
+    for s in samples:
+        costs = torch.from_numpy(s.costs).to(device)
+        guidance = torch.from_numpy(s.guidance).to(device)
+        proposals = {"naive": bandmod.naive_tile_offsets(s.costs, s.columns, s.rows, s.labels, tile, band)}
+        for name, net in nets.items():
+            proposals[name] = net.propose(costs, guidance, s.columns, s.rows, s.labels, tile, band)
+        for kind, offsets in proposals.items():
+            w, f = band_winners(context, costs, guidance, s.columns, s.rows, s.labels, offsets, tile, band, margin)
+            scores[kind].add(w, f, s)
+            windows = C.c_int()
+            context.check(context.lib.chiaro_sgm_banded_report(context.handle, C.byref(windows)))
+            scores[kind].windows += windows.value
+    return {k: v.summary() for k, v in scores.items()}

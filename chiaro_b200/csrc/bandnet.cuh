@@ -32,6 +32,7 @@ constexpr int NET_TAPS = 9;
 constexpr int NET_W = NET_TAPS * NET_CH * NET_CH;  // weights per layer
 constexpr int NET_PARAMS = NET_LAYERS * (NET_W + NET_CH);
 constexpr int NET_BINS = 16;    // cost-summary bins
+constexpr int NET_INPUTS = 1 + NET_BINS + 2;  // live input channels of layer 0
 
 __device__ __forceinline__ void mma_bf16_16816(float (&c)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
                                                unsigned b0, unsigned b1) {
@@ -55,8 +56,10 @@ __device__ __forceinline__ unsigned pack_raw(__nv_bfloat16 lo, __nv_bfloat16 hi)
     return (unsigned)__bfloat16_as_ushort(lo) | ((unsigned)__bfloat16_as_ushort(hi) << 16);
 }
 
-// Input features of one node: the reference luminance at the node (guidance / 8)
-// and, per bin of the finite labels, the bin's minimum cost minus the node's.
+// Input features of one node: the reference luminance at the node (guidance / 8);
+// per bin of the finite labels, the bin's minimum cost minus the node's; the
+// first cost argmin over the finite labels, as (argmin - 1) / (labels - 2); and
+// the node's minimum cost.
 __global__ void net_features_kernel(const float *__restrict__ costs, const float *__restrict__ guidance, int nodes,
                                     int labels, __nv_bfloat16 *__restrict__ features) {
     const int node = blockIdx.x * blockDim.x + threadIdx.x;
@@ -64,18 +67,27 @@ __global__ void net_features_kernel(const float *__restrict__ costs, const float
     const float *c = costs + (size_t)node * labels;
     float bins[NET_BINS];
     float lowest = INFINITY;
+    int argmin = 1;
     const int finite = labels - 1;
     for (int b = 0; b < NET_BINS; ++b) {
         const int l0 = 1 + b * finite / NET_BINS, l1 = 1 + (b + 1) * finite / NET_BINS;
         float m = INFINITY;
-        for (int l = l0; l < l1; ++l) m = fminf(m, c[l]);
+        for (int l = l0; l < l1; ++l) {
+            const float v = c[l];
+            if (v < lowest) {
+                lowest = v;
+                argmin = l;
+            }
+            m = fminf(m, v);
+        }
         bins[b] = m;
-        lowest = fminf(lowest, m);
     }
     __nv_bfloat16 *f = features + (size_t)node * NET_CH;
     f[0] = __float2bfloat16_rn(guidance[node] * 0.125f);
     for (int b = 0; b < NET_BINS; ++b) f[1 + b] = __float2bfloat16_rn(bins[b] - lowest);
-    for (int k = 1 + NET_BINS; k < NET_CH; ++k) f[k] = __float2bfloat16_rn(0.0f);
+    f[NET_INPUTS - 2] = __float2bfloat16_rn((float)(argmin - 1) / (float)(labels - 2));
+    f[NET_INPUTS - 1] = __float2bfloat16_rn(lowest);
+    for (int k = NET_INPUTS; k < NET_CH; ++k) f[k] = __float2bfloat16_rn(0.0f);
 }
 
 // out[p][co] = sum_{tap, ci} in[p + tap][ci] * w[tap][co][ci] + bias[co]; then ReLU

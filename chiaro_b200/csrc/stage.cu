@@ -50,6 +50,7 @@ struct chiaro_depth_ctx {
     cudaGraphExec_t batch_exec = nullptr;
     std::map<uint64_t, int> batch_tuning;
     int batch_warps = 0, batch_waves = 0, batch_replayed = 0;
+    int band_windows = 0;  // fallback windows of the last banded SGM
     float timings[7] = {};
     int launches = 0;  // this library's kernel launches in the last stage call
 };
@@ -499,51 +500,80 @@ int run_band(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, i
                             32 * SGM_PATHS_PER_CTA, 0, s>>>(costs, guidance, grid, paths, pitch, columns, rows, labels);
     CK(cudaGetLastError());
     sgm_band_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, s>>>(paths, pitch, grid, columns, rows,
-                                                                               winner, fallback);
+                                                                               labels, winner, fallback);
     CK(cudaGetLastError());
     std::vector<uint8_t> flags(tiles);
     CK(cudaMemcpyAsync(flags.data(), fallback, tiles, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    // windows of the tiles that fell back
+    // fallback tiles as greedy rectangles in raster order (widest run, then as many
+    // rows of it as are all flagged), each with its window of margin nodes around it
     std::vector<BandWindow> windows;
+    std::vector<uint8_t> taken(tiles, 0);
+    auto open = [&](int x, int y) { return flags[y * tiles_x + x] && !taken[y * tiles_x + x]; };
     size_t cost_floats = 0, node_floats = 0;
+    int most = 0;
     for (int ty = 0; ty < tiles_y; ++ty)
         for (int tx = 0; tx < tiles_x; ++tx) {
-            if (!flags[ty * tiles_x + tx]) continue;
-            BandWindow w{};
-            w.tc0 = tx * tile;
-            w.tr0 = ty * tile;
-            w.tc = std::min(columns, w.tc0 + tile) - w.tc0;
-            w.tr = std::min(rows, w.tr0 + tile) - w.tr0;
-            w.c0 = std::max(0, w.tc0 - margin);
-            w.r0 = std::max(0, w.tr0 - margin);
-            w.wc = std::min(columns, w.tc0 + tile + margin) - w.c0;
-            w.wr = std::min(rows, w.tr0 + tile + margin) - w.r0;
-            w.cost_offset = cost_floats;
-            w.node_offset = node_floats;
-            cost_floats += (size_t)w.wc * w.wr * labels;
-            node_floats += (size_t)w.wc * w.wr;
-            windows.push_back(w);
+            if (!open(tx, ty)) continue;
+            int w = 1, h = 1;
+            while (tx + w < tiles_x && open(tx + w, ty)) ++w;
+            for (bool grow = true; grow && ty + h < tiles_y;) {
+                for (int x = tx; x < tx + w; ++x) grow = grow && open(x, ty + h);
+                if (grow) ++h;
+            }
+            for (int y = ty; y < ty + h; ++y)
+                for (int x = tx; x < tx + w; ++x) taken[y * tiles_x + x] = 1;
+            BandWindow win{};
+            win.tc0 = tx * tile;
+            win.tr0 = ty * tile;
+            win.tc = std::min(columns, (tx + w) * tile) - win.tc0;
+            win.tr = std::min(rows, (ty + h) * tile) - win.tr0;
+            win.c0 = std::max(0, win.tc0 - margin);
+            win.r0 = std::max(0, win.tr0 - margin);
+            win.wc = std::min(columns, win.tc0 + win.tc + margin) - win.c0;
+            win.wr = std::min(rows, win.tr0 + win.tr + margin) - win.r0;
+            win.cost_offset = cost_floats;
+            win.node_offset = node_floats;
+            cost_floats += (size_t)win.wc * win.wr * labels;
+            node_floats += (size_t)win.wc * win.wr;
+            most = std::max(most, win.tc * win.tr);
+            windows.push_back(win);
         }
+    if (node_floats >= nodes) {
+        // the windows would cover at least the grid: one full-range SGM over the whole
+        // grid decides the fallback tiles' nodes instead
+        BandWindow whole{};
+        whole.wc = whole.tc = columns;
+        whole.wr = whole.tr = rows;
+        windows.assign(1, whole);
+        most = columns * rows;
+    }
+    ctx->band_windows = (int)windows.size();
     if (!windows.empty()) {
         BandWindow *d_windows = dbuf<BandWindow>(ctx, "band.windows", windows.size());
-        float *wcosts = dbuf<float>(ctx, "band.wcosts", cost_floats);
-        float *wagg = dbuf<float>(ctx, "band.wagg", cost_floats);
-        float *wguid = dbuf<float>(ctx, "band.wguid", node_floats);
         upload(ctx, d_windows, windows.data(), windows.size());
-        band_crop_kernel<<<dim3(64, (unsigned)windows.size()), 256, 0, s>>>(costs, guidance, columns, labels,
-                                                                             d_windows, wcosts, wguid);
-        CK(cudaGetLastError());
-        std::vector<chiaro_sgm_instance> instances(windows.size());
-        for (size_t i = 0; i < windows.size(); ++i) {
-            const BandWindow &w = windows[i];
-            instances[i] = chiaro_sgm_instance{wcosts + w.cost_offset, wguid + w.node_offset, wagg + w.cost_offset,
-                                               (uint64_t)w.wc, (uint64_t)w.wr, (uint64_t)labels};
+        float *wagg;
+        if (windows.size() == 1 && windows[0].wc == columns && windows[0].wr == rows) {
+            wagg = dbuf<float>(ctx, "band.wagg", nodes * labels);
+            launch_sgm(ctx, costs, guidance, wagg, columns, rows, labels);
+        } else {
+            float *wcosts = dbuf<float>(ctx, "band.wcosts", cost_floats);
+            float *wguid = dbuf<float>(ctx, "band.wguid", node_floats);
+            wagg = dbuf<float>(ctx, "band.wagg", cost_floats);
+            band_crop_kernel<<<dim3(64, (unsigned)windows.size()), 256, 0, s>>>(costs, guidance, columns, labels,
+                                                                                 d_windows, wcosts, wguid);
+            CK(cudaGetLastError());
+            std::vector<chiaro_sgm_instance> instances(windows.size());
+            for (size_t i = 0; i < windows.size(); ++i) {
+                const BandWindow &w = windows[i];
+                instances[i] = chiaro_sgm_instance{wcosts + w.cost_offset, wguid + w.node_offset,
+                                                   wagg + w.cost_offset, (uint64_t)w.wc, (uint64_t)w.wr,
+                                                   (uint64_t)labels};
+            }
+            if (int st = run_batch(ctx, instances.data(), instances.size(), 0, 0)) return st;
         }
-        if (int st = run_batch(ctx, instances.data(), instances.size(), 0, 0)) return st;
-        const int most = tile * tile;
         band_window_winner_kernel<<<dim3((unsigned)div_ceil((size_t)most * 32, 256), (unsigned)windows.size()), 256,
-                                    0, s>>>(wagg, columns, labels, d_windows, winner);
+                                    0, s>>>(wagg, columns, labels, d_windows, grid, fallback, winner);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(s));
@@ -1618,6 +1648,12 @@ int chiaro_sgm_batch_report(const chiaro_depth_ctx *ctx, int *warps_per_cta, int
     if (warps_per_cta) *warps_per_cta = ctx->batch_warps;
     if (waves) *waves = ctx->batch_waves;
     if (replayed) *replayed = ctx->batch_replayed;
+    return CHIARO_OK;
+}
+
+int chiaro_sgm_banded_report(const chiaro_depth_ctx *ctx, int *windows) {
+    if (!ctx || !windows) return CHIARO_ERR_ARGUMENT;
+    *windows = ctx->band_windows;
     return CHIARO_OK;
 }
 

@@ -377,9 +377,12 @@ int chiaro_sgm_batch_report(const chiaro_depth_ctx *ctx, int *warps_per_cta, int
  * tile) per row) with the recurrence of semi_global_costs (depth.rs:1363-1381),
  * the band shifting between tiles along each path. winner[node] is the label of
  * the first minimum over the band. A tile whose winner sits on a band edge at
- * any node falls back (fallback[t] = 1): the full-range SGM over the tile grown
- * by `margin` nodes decides its nodes' winners (labels 1..labels-1). The _device
- * form takes device pointers. */
+ * any node, with labels beyond that edge (not at label 1 or labels - 1), falls
+ * back (fallback[t] = 1). Fallback tiles are grouped into rectangles (in raster
+ * order: the widest run of fallback tiles, then as many rows of that run as are
+ * all fallback tiles); the full-range SGM over each rectangle grown by `margin`
+ * nodes decides its nodes' winners (labels 1..labels-1). The _device form takes
+ * device pointers. */
 int chiaro_sgm_banded(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, uint64_t columns,
                       uint64_t rows, uint64_t labels, const int32_t *tile_offsets, uint64_t tile,
                       uint64_t band, uint64_t margin, int32_t *winner, uint8_t *fallback);
@@ -388,13 +391,17 @@ int chiaro_sgm_banded_device(chiaro_depth_ctx *ctx, const float *costs, const fl
                              const int32_t *tile_offsets, uint64_t tile, uint64_t band,
                              uint64_t margin, int32_t *winner, uint8_t *fallback);
 
+/* The number of fallback windows (rectangles) of the last banded SGM. */
+int chiaro_sgm_banded_report(const chiaro_depth_ctx *ctx, int *windows);
+
 /* ---- learned band proposal ------------------------------------------------------- */
 
 /* No counterpart in the reference (which uses no learned model): the band
  * proposal network of the banded SGM. Six 3x3 convolutions of 32 channels on
  * the coarse grid (one pixel per node), bf16 tensor-core kernels with fp32
- * accumulation. Inputs per node: the reference luminance (guidance) and 16
- * cost-bin minima over the finite labels (labels >= 19). Parameters are
+ * accumulation. Inputs per node: the reference luminance (guidance), 16
+ * cost-bin minima over the finite labels (labels >= 19), the first cost argmin
+ * and the minimum cost. Parameters are
  * chiaro_bandnet_parameter_count() fp32 values: per layer the weights
  * [tap][co][ci] then the 32 biases. All arrays below are device memory; costs
  * [images][nodes][labels], guidance [images][nodes], winners (the target

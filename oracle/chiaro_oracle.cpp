@@ -2170,31 +2170,64 @@ int oracle_sgm_banded(const float *costs, const float *guidance, size_t columns,
         for (size_t j = 1; j < band; ++j)
             if (total_key_f32(o[j]) < total_key_f32(o[best])) best = j;
         winner[node] = node_offset[node] + (int)best;
-        if (best == 0 || best + 1 == band) fallback[((node / columns) / tile) * tiles_x + (node % columns) / tile] = 1;
+        // a band edge wins where labels lie beyond it (not at label 1 or D - 1)
+        const int offset = node_offset[node];
+        if ((best == 0 && offset > 1) || (best + 1 == band && (size_t)offset + band < labels))
+            fallback[((node / columns) / tile) * tiles_x + (node % columns) / tile] = 1;
     }
+    // fallback tiles as greedy rectangles in raster order (widest run, then as many
+    // rows of it as are all flagged), each rerun at full range in a window of margin
+    // nodes around it; where those windows would cover at least the grid, one
+    // full-range SGM over the whole grid decides every fallback tile instead
+    struct Rect { size_t n0c, n0r, n1c, n1r, c0, r0, c1, r1; };
+    std::vector<Rect> rects;
+    size_t window_nodes = 0;
+    std::vector<uint8_t> taken(tiles_x * tiles_y, 0);
+    auto open = [&](size_t x, size_t y) { return fallback[y * tiles_x + x] && !taken[y * tiles_x + x]; };
     for (size_t ty = 0; ty < tiles_y; ++ty)
         for (size_t tx = 0; tx < tiles_x; ++tx) {
-            if (!fallback[ty * tiles_x + tx]) continue;
-            size_t c0 = tx * tile > margin ? tx * tile - margin : 0, r0 = ty * tile > margin ? ty * tile - margin : 0;
-            size_t c1 = std::min(columns, (tx + 1) * tile + margin), r1 = std::min(rows, (ty + 1) * tile + margin);
-            size_t wc = c1 - c0, wr = r1 - r0;
-            std::vector<float> wcost(wc * wr * labels), wguid(wc * wr);
-            for (size_t r = 0; r < wr; ++r)
-                for (size_t c = 0; c < wc; ++c) {
-                    size_t src = (r0 + r) * columns + c0 + c;
-                    wguid[r * wc + c] = guidance[src];
-                    std::copy(costs + src * labels, costs + (src + 1) * labels, wcost.begin() + (r * wc + c) * labels);
-                }
-            auto agg = semi_global_costs(wcost.data(), wguid.data(), wc, wr, labels);
-            for (size_t r = ty * tile; r < std::min(rows, (ty + 1) * tile); ++r)
-                for (size_t c = tx * tile; c < std::min(columns, (tx + 1) * tile); ++c) {
-                    const float *o = agg.data() + ((r - r0) * wc + (c - c0)) * labels;
-                    size_t best = 1;
-                    for (size_t l = 2; l < labels; ++l)
-                        if (total_key_f32(o[l]) < total_key_f32(o[best])) best = l;
-                    winner[r * columns + c] = (int)best;
-                }
+            if (!open(tx, ty)) continue;
+            size_t w = 1, h = 1;
+            while (tx + w < tiles_x && open(tx + w, ty)) ++w;
+            for (bool grow = true; grow && ty + h < tiles_y;) {
+                for (size_t x = tx; x < tx + w; ++x) grow = grow && open(x, ty + h);
+                if (grow) ++h;
+            }
+            for (size_t y = ty; y < ty + h; ++y)
+                for (size_t x = tx; x < tx + w; ++x) taken[y * tiles_x + x] = 1;
+            Rect q;
+            q.n0c = tx * tile;
+            q.n0r = ty * tile;
+            q.n1c = std::min(columns, (tx + w) * tile);
+            q.n1r = std::min(rows, (ty + h) * tile);
+            q.c0 = q.n0c > margin ? q.n0c - margin : 0;
+            q.r0 = q.n0r > margin ? q.n0r - margin : 0;
+            q.c1 = std::min(columns, q.n1c + margin);
+            q.r1 = std::min(rows, q.n1r + margin);
+            window_nodes += (q.c1 - q.c0) * (q.r1 - q.r0);
+            rects.push_back(q);
         }
+    if (!rects.empty() && window_nodes >= n) rects.assign(1, Rect{0, 0, columns, rows, 0, 0, columns, rows});
+    for (const Rect &q : rects) {
+        const size_t wc = q.c1 - q.c0, wr = q.r1 - q.r0;
+        std::vector<float> wcost(wc * wr * labels), wguid(wc * wr);
+        for (size_t r = 0; r < wr; ++r)
+            for (size_t c = 0; c < wc; ++c) {
+                size_t src = (q.r0 + r) * columns + q.c0 + c;
+                wguid[r * wc + c] = guidance[src];
+                std::copy(costs + src * labels, costs + (src + 1) * labels, wcost.begin() + (r * wc + c) * labels);
+            }
+        auto agg = semi_global_costs(wcost.data(), wguid.data(), wc, wr, labels);
+        for (size_t r = q.n0r; r < q.n1r; ++r)
+            for (size_t c = q.n0c; c < q.n1c; ++c) {
+                if (!fallback[(r / tile) * tiles_x + c / tile]) continue;
+                const float *o = agg.data() + ((r - q.r0) * wc + (c - q.c0)) * labels;
+                size_t best = 1;
+                for (size_t l = 2; l < labels; ++l)
+                    if (total_key_f32(o[l]) < total_key_f32(o[best])) best = l;
+                winner[r * columns + c] = (int)best;
+            }
+    }
     return CHIARO_OK;
 }
 
@@ -2211,16 +2244,24 @@ void oracle_bandnet_features(const float *costs, const float *guidance, size_t n
     for (size_t node = 0; node < nodes; ++node) {
         const float *c = costs + node * labels;
         float m[16], lowest = std::numeric_limits<float>::infinity();
+        int argmin = 1;
         for (int b = 0; b < bins; ++b) {
             int l0 = 1 + b * finite / bins, l1 = 1 + (b + 1) * finite / bins;
             m[b] = std::numeric_limits<float>::infinity();
-            for (int l = l0; l < l1; ++l) m[b] = std::fmin(m[b], c[l]);
-            lowest = std::fmin(lowest, m[b]);
+            for (int l = l0; l < l1; ++l) {
+                if (c[l] < lowest) {
+                    lowest = c[l];
+                    argmin = l;
+                }
+                m[b] = std::fmin(m[b], c[l]);
+            }
         }
         float *f = features + node * NET_CH_O;
         f[0] = guidance[node] * 0.125f;
         for (int b = 0; b < bins; ++b) f[1 + b] = m[b] - lowest;
-        for (int k = 1 + bins; k < NET_CH_O; ++k) f[k] = 0.0f;
+        f[1 + bins] = (float)(argmin - 1) / (float)(labels - 2);
+        f[2 + bins] = lowest;
+        for (int k = 3 + bins; k < NET_CH_O; ++k) f[k] = 0.0f;
     }
 }
 

@@ -4,7 +4,7 @@ import ctypes as C
 
 import numpy as np
 
-from chiaro_b200.bandnet import init_params
+from chiaro_b200.bandnet import INPUTS, init_params
 
 F = C.POINTER(C.c_float)
 
@@ -24,7 +24,7 @@ def test_oracle_gradient_matches_finite_differences(oracle_lib):
     params = init_params(1)
     params += rng.normal(0, 0.02, params.size).astype(np.float32)  # move off the initial zeros
     features = rng.uniform(0, 1, (images, h, w, 32)).astype(np.float32)
-    features[..., 17:] = 0.0
+    features[..., INPUTS:] = 0.0
     targets = rng.uniform(0, 1, images * h * w).astype(np.float32)
     mask = (rng.random(images * h * w) < 0.8).astype(np.uint8)
     loss, grads = _loss_grad(oracle_lib, params, features, targets, mask, images, h, w)
@@ -42,3 +42,21 @@ def test_oracle_gradient_matches_finite_differences(oracle_lib):
         checked += 1
         passed += abs(fd - grads[i]) <= 0.05 * abs(grads[i]) + 1e-5
     assert passed >= 0.9 * checked, (passed, checked)
+
+
+def test_oracle_features_of_a_node(oracle_lib):
+    labels = 49  # 48 finite labels: 16 bins of 3
+    costs = np.full(labels, 1.5, np.float32)
+    costs[0] = 0.0  # label 0 is not a depth label and stays out of the summary
+    costs[[7, 20, 30]] = [0.4, 0.2, 0.2]
+    guidance = np.array([4.0], np.float32)
+    f = np.zeros(32, np.float32)
+    oracle_lib.oracle_bandnet_features(costs.ctypes.data_as(F), guidance.ctypes.data_as(F), 1, labels,
+                                       f.ctypes.data_as(F))
+    bins = np.full(16, 1.3, np.float32)
+    bins[2], bins[6], bins[9] = 0.2, 0.0, 0.0  # labels 7, 20 and 30 minus the minimum 0.2
+    assert f[0] == np.float32(0.5)
+    assert np.allclose(f[1:17], bins)
+    assert f[17] == np.float32(19 / 47)  # the first argmin (label 20), over labels 1..48
+    assert f[18] == np.float32(0.2)
+    assert not f[INPUTS:].any()

@@ -1,6 +1,6 @@
-"""The banded SGM with its windowed full-range fallback (chiaro_sgm_banded):
-winner labels and fallback tiles identical to the oracle's restatement
-(oracle_sgm_banded)."""
+"""The banded SGM with its full-range fallback (chiaro_sgm_banded), windowed and
+over the whole grid: winner labels and fallback tiles identical to the oracle's
+restatement (oracle_sgm_banded)."""
 import ctypes as C
 
 import numpy as np
@@ -41,7 +41,7 @@ def gpu_band(ctx, costs, guidance, columns, rows, labels, offsets, tile, band, m
 
 @pytest.mark.parametrize("columns,rows,labels,tile,band,margin", [
     (9, 7, 33, 4, 24, 4), (40, 31, 129, 4, 24, 8), (23, 45, 193, 3, 32, 16), (60, 2, 65, 5, 8, 0),
-    (1, 30, 40, 1, 1, 2), (17, 17, 97, 2, 16, 6)])
+    (1, 30, 40, 1, 1, 2), (17, 17, 97, 2, 16, 6), (64, 48, 97, 4, 31, 1), (50, 40, 65, 4, 24, 200)])
 def test_banded_sgm_matches_oracle(gpu_ctx, columns, rows, labels, tile, band, margin):
     rng = np.random.default_rng(columns * 97 + rows * 13 + labels + band)
     n = columns * rows
@@ -81,3 +81,29 @@ def test_banded_sgm_refuses_offsets_outside_the_labels(gpu_ctx):
     assert gpu_ctx.lib.chiaro_sgm_banded(gpu_ctx.handle, fptr(costs), fptr(guidance), 4, 4, 33,
                                          offsets.ctypes.data_as(I32), 4, 24, 2, winner.ctypes.data_as(I32),
                                          fallback.ctypes.data_as(U8)) == abi.ERR_ARGUMENT
+
+
+def test_few_fallback_tiles_take_windows(gpu_ctx):
+    """Costs with one clear minimum per node and bands centred on it, except a few tiles
+    whose band is far off: only those fall back, through windows of margin nodes (not the
+    whole grid), label for label as in the oracle."""
+    rng = np.random.default_rng(21)
+    columns, rows, labels, tile, band, margin = 57, 43, 97, 4, 24, 3
+    r, c = np.divmod(np.arange(columns * rows), columns)
+    best = (40 + 10 * np.sin(c / 9.0) + 8 * np.cos(r / 7.0)).astype(int)
+    costs = rng.uniform(0.8, 1.6, (columns * rows, labels)).astype(np.float32)
+    costs[np.arange(columns * rows), best] = 0.05
+    costs = costs.reshape(-1)
+    guidance = rng.uniform(0, 7, columns * rows).astype(np.float32)
+    tx, ty = bandmod.tiles_of(columns, rows, tile)
+    centres = np.array([np.median(best.reshape(rows, columns)[y * tile:(y + 1) * tile, x * tile:(x + 1) * tile])
+                        for y in range(ty) for x in range(tx)])
+    offsets = bandmod.centred_offsets(centres, labels, band)
+    far = rng.choice(tx * ty, 6, replace=False)
+    offsets[far] = np.where(offsets[far] > 40, 1, labels - band)
+    w_g, f_g = gpu_band(gpu_ctx, costs, guidance, columns, rows, labels, offsets, tile, band, margin)
+    windows = C.c_int()
+    gpu_ctx.check(gpu_ctx.lib.chiaro_sgm_banded_report(gpu_ctx.handle, C.byref(windows)))
+    w_o, f_o = oracle_band(costs, guidance, columns, rows, labels, offsets, tile, band, margin)
+    assert np.array_equal(f_g, f_o) and np.array_equal(w_g, w_o)
+    assert 0 < f_g.sum() < 20 and windows.value > 1
