@@ -56,6 +56,9 @@ def parse_args():
     p.add_argument("--band", type=int, default=0, help="coarse rows per CPU sample (0 = automatic)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (0 = --steps)")
+    p.add_argument("--band-train", type=int, default=24, help="1040x780 scenes the band network trains on")
+    p.add_argument("--band-eval", type=int, default=8, help="held-out 1040x780 scenes of the band evaluation")
+    p.add_argument("--no-learned-band", action="store_true")
     return p.parse_args()
 
 
@@ -285,6 +288,9 @@ def run_ours(args, rank, world, local):
 
     quantised = quantised_sgm(args, scene, work, ctx, torch, device, stream, flush)
     batched = batched_sgm(args, ctx, torch, device, stream, flush)
+    band = None
+    if world == 1 and not args.no_learned_band:
+        band = learned_band(args, scene, ctx, torch, device, stream, flush)
 
     peaks = measured_peaks()
     sgm_s = stage_ms["sgm"] / 1e3
@@ -316,6 +322,7 @@ def run_ours(args, rank, world, local):
             frac=round(quantised["roofline"]["achieved"] / peaks["hbm_gbs"], 4))),
         "batched_sgm": dict(batched, note="SGM of many instances of uneven sizes and label counts: "
                             "per-instance calls (plain) against one persistent batch replayed from a CUDA graph"),
+        **({"learned_band": band} if band else {}),
         "compute_roofline": {"kernel": "cost_volume_kernel (build_cost_volume, the largest correlation kernel)",
                              "bound": "fp32", "achieved": round(cost_tflops, 2), "peak": round(fp32_peak, 1),
                              "unit": "TFLOP/s", "frac": round(cost_tflops / fp32_peak, 4),
@@ -469,6 +476,104 @@ def batched_sgm(args, ctx, torch, device, stream, flush):
         del tensors
         torch.cuda.empty_cache()
     return result
+
+
+def learned_band(args, scene, ctx, torch, device, stream, flush):
+    """Config 3: the learned band proposal. Two networks (tile-median and tile-mid-range
+    targets) train on the GPU on seeded 1040x780 scenes with 192 planes, labelled by the
+    exact GPU stage's full-range SGM. On held-out scenes of that kind and on this workload's
+    own full-resolution scene, the banded SGM with full-range fallback is scored against the
+    full-range SGM (agreement within one plane over tested nodes, fallback rate) beside the
+    naive band (each tile's median cost argmin), and timed against the full-range SGM."""
+    import numpy as np
+
+    from chiaro_b200 import band as bandmod
+    from chiaro_b200 import bandnet
+    tile, width, margin = 4, 24, 8
+    t0 = time.perf_counter()
+    rendered = bandnet.render_scenes("band", list(range(1000, 1000 + args.band_train)) +
+                                     list(range(5000, 5000 + args.band_eval)))
+    render_s = time.perf_counter() - t0
+    samples = [bandnet.samples_from_stage(s, ctx) for s in rendered]
+    del rendered
+    train, held = samples[:args.band_train], samples[args.band_train:]
+    full = bandnet.samples_from_stage(scene, ctx)
+    nets, training = {}, {}
+    for kind in ("median", "midrange"):
+        net = bandnet.BandNet(ctx, seed=args.seed)
+        targets = [bandnet.tile_targets(s, tile, kind) for s in train]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        first = net.train(targets, 400, 2e-3)
+        last = net.train(targets, 200, 5e-4)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        nets[f"learned_{kind}"] = net
+        training[kind] = {"steps": 600, "images": len(targets), "ms": round(e0.elapsed_time(e1), 1),
+                          "loss_first": float(first[0]), "loss_last": float(last[-1])}
+    held_scores = bandnet.evaluate(ctx, held, nets, tile, width, margin)
+    full_scores = bandnet.evaluate(ctx, [full], nets, tile, width, margin)
+
+    # time on this workload's own cost volume: the full-range SGM against proposal + banded SGM + fallback
+    costs = torch.from_numpy(full.costs).to(device)
+    guidance = torch.from_numpy(full.guidance).to(device)
+    out = torch.empty_like(costs)
+    tx, ty = bandmod.tiles_of(full.columns, full.rows, tile)
+    winner = torch.empty(full.columns * full.rows, dtype=torch.int32, device=device)
+    fallback = torch.empty(tx * ty, dtype=torch.uint8, device=device)
+    lib = ctx.lib
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 2)):
+            fn()
+        total, steps = 0.0, max(1, min(args.steps, 5))
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return round(total / steps, 4)
+
+    def banded(net):
+        offsets = net.propose(costs, guidance, full.columns, full.rows, full.labels, tile, width)
+        ctx.check(lib.chiaro_sgm_banded_device(ctx.handle, costs.data_ptr(), guidance.data_ptr(), full.columns,
+                                               full.rows, full.labels, offsets.data_ptr(), tile, width, margin,
+                                               winner.data_ptr(), fallback.data_ptr()))
+
+    timing = {"full_range_sgm": timed(lambda: ctx.check(lib.chiaro_sgm_aggregate_device(
+        ctx.handle, costs.data_ptr(), guidance.data_ptr(), full.columns, full.rows, full.labels, out.data_ptr())))}
+    for name, net in nets.items():
+        timing[f"propose_{name}"] = timed(lambda: net.propose(costs, guidance, full.columns, full.rows, full.labels,
+                                                              tile, width))
+        timing[f"propose_banded_fallback_{name}"] = timed(lambda: banded(net))
+    # the banded SGM itself, with no tile falling back: every offset at label 1, every cost flat
+    flat = torch.full_like(costs, 2.25)
+    ones = torch.ones(tx * ty, dtype=torch.int32, device=device)
+    timing["banded_sgm_no_fallback"] = timed(lambda: ctx.check(lib.chiaro_sgm_banded_device(
+        ctx.handle, flat.data_ptr(), guidance.data_ptr(), full.columns, full.rows, full.labels, ones.data_ptr(), tile,
+        width, margin, winner.data_ptr(), fallback.data_ptr())))
+    assert int(fallback.sum()) == 0
+    del flat, costs, out
+    torch.cuda.empty_cache()
+    return {"tile_nodes": tile, "band_labels": width, "fallback_margin_nodes": margin,
+            "train": {"scenes": args.band_train, "workload": "1040x780, reference + 2 sources, 192 planes",
+                      "render_s": round(render_s, 1), **training},
+            "held_out_1040x780": dict(held_scores, scenes=args.band_eval,
+                                      wide_tile_fraction=round(float(np.mean(
+                                          [bandnet.wide_tile_fraction(s, tile, width) for s in held])), 4)),
+            "workload_full_resolution": dict(full_scores, labels=full.labels,
+                                             wide_tile_fraction=round(bandnet.wide_tile_fraction(full, tile,
+                                                                                                 width), 4)),
+            "timing_ms_full_resolution": timing,
+            "note": "agreement: banded winners within one plane of the full-range SGM's over tested coarse nodes; "
+                    "wide_tile_fraction: tiles whose full-range winners span more than band - 3 labels"}
 
 
 def run_reference(args, rank, world):

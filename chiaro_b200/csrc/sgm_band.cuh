@@ -33,15 +33,12 @@ __device__ __forceinline__ int band_offset_at(const BandGrid &b, int row, int co
     return __ldg(b.tile_offset + (row / b.tile) * b.tiles_x + column / b.tile);
 }
 
-constexpr int SGM_BAND_PREFETCH = 16;  // steps whose offset and costs are in flight (divides 32)
-
 // Banded path costs of every path of every direction; pass k writes paths + k * pitch ([N][band]).
-// A ring of SGM_BAND_PREFETCH steps holds each coming step's band offset and cost, loaded
-// that many steps ahead, so the walk waits on no load.
+// Each step loads its own costs: the kernel stays small enough (registers) for all paths of
+// a full-resolution grid to be resident at once, and the other warps hide the load.
 __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_band_paths_kernel(
     const float *__restrict__ data, const float *__restrict__ guidance, BandGrid grid, float *__restrict__ paths,
     size_t pitch, int columns, int rows, int labels) {
-    constexpr int P = SGM_BAND_PREFETCH;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
@@ -61,23 +58,13 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_band_paths_kernel(
     const long node_step = (long)dr * columns + dc;
     const long node0 = (long)r0 * columns + c0;
     float *wp = paths + (size_t)pass * pitch + (size_t)node0 * band + lane;
-    const long write_step = node_step * band;
     int offset = band_offset_at(grid, r0, c0);
     float prev = valid ? __ldg(data + (size_t)node0 * labels + offset + lane) : INFINITY;
     if (valid) *wp = prev;
-    // ring slot j holds step 1 + j, then every step s with (s - 1) % P == j
-    float ring[P];
-    int ring_offset[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-        const int s = 1 + j;
-        ring_offset[j] = s < len ? band_offset_at(grid, r0 + s * dr, c0 + s * dc) : 0;
-        ring[j] = valid && s < len ? __ldg(data + (size_t)(node0 + s * node_step) * labels + ring_offset[j] + lane)
-                                   : INFINITY;
-    }
     float p1s = 0.0f, p2s = 0.0f;
+    int offsets = 0;
     for (int base = 1; base < len; base += 32) {
-        {  // lane j: penalties of step base + j (depth.rs:1358-1361)
+        {  // lane j: offset and penalties of step base + j (depth.rs:1358-1361)
             const int s = base + lane;
             if (s < len) {
                 const float g = __ldg(guidance + node0 + s * node_step);
@@ -85,39 +72,29 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_band_paths_kernel(
                 const float edge_scale = __frcp_rn(1.0f + 4.0f * fabsf(g - g_prev));  // == 1 / x, correctly rounded
                 p1s = SGM_SMALL_PENALTY * fmaxf(edge_scale, 0.35f);
                 p2s = SGM_LARGE_PENALTY * fmaxf(edge_scale, 0.12f);
+                offsets = band_offset_at(grid, r0 + s * dr, c0 + s * dc);
             }
         }
-        for (int jj = 0; jj < 32; jj += P) {
-#pragma unroll
-            for (int j = 0; j < P; ++j) {
-                const int step = base + jj + j;
-                if (step >= len) break;  // uniform over the warp
-                const float cur = ring[j];
-                const int o = ring_offset[j];
-                const int ahead = step + P;
-                if (ahead < len) {
-                    const int oa = band_offset_at(grid, r0 + ahead * dr, c0 + ahead * dc);
-                    ring_offset[j] = oa;
-                    ring[j] = valid ? __ldg(data + (size_t)(node0 + ahead * node_step) * labels + oa + lane)
-                                    : INFINITY;
-                }
-                const float p1 = __shfl_sync(full, p1s, jj + j), p2 = __shfl_sync(full, p2s, jj + j);
-                const float minimum_previous = warp_min_f32(prev);
-                const int s = lane + (o - offset);  // this label's slot in the previous band
-                const float same = __shfl_sync(full, prev, s & 31);
-                const float below = __shfl_sync(full, prev, (s - 1) & 31);
-                const float above = __shfl_sync(full, prev, (s + 1) & 31);
-                const int label = o + lane;
-                const float same_v = s >= 0 && s < band ? same : INFINITY;
-                const float lower = label > 0 && s - 1 >= 0 && s - 1 < band ? below + p1 : INFINITY;
-                const float higher = label + 1 < labels && s + 1 >= 0 && s + 1 < band ? above + p1 : INFINITY;
-                const float jump = minimum_previous + p2;
-                const float v = cur + fminf(fminf(fminf(same_v, lower), higher), jump) - minimum_previous;
-                prev = valid ? v : INFINITY;
-                offset = o;
-                wp += write_step;
-                if (valid) *wp = v;
-            }
+        const int steps = min(32, len - base);
+        for (int j = 0; j < steps; ++j) {
+            const long node = node0 + (long)(base + j) * node_step;
+            const int o = __shfl_sync(full, offsets, j);
+            const float p1 = __shfl_sync(full, p1s, j), p2 = __shfl_sync(full, p2s, j);
+            const float cur = valid ? __ldg(data + (size_t)node * labels + o + lane) : INFINITY;
+            const float minimum_previous = warp_min_f32(prev);
+            const int s = lane + (o - offset);  // this label's slot in the previous band
+            const float same = __shfl_sync(full, prev, s & 31);
+            const float below = __shfl_sync(full, prev, (s - 1) & 31);
+            const float above = __shfl_sync(full, prev, (s + 1) & 31);
+            const int label = o + lane;
+            const float same_v = s >= 0 && s < band ? same : INFINITY;
+            const float lower = label > 0 && s - 1 >= 0 && s - 1 < band ? below + p1 : INFINITY;
+            const float higher = label + 1 < labels && s + 1 >= 0 && s + 1 < band ? above + p1 : INFINITY;
+            const float jump = minimum_previous + p2;
+            const float v = cur + fminf(fminf(fminf(same_v, lower), higher), jump) - minimum_previous;
+            prev = valid ? v : INFINITY;
+            offset = o;
+            if (valid) paths[(size_t)pass * pitch + (size_t)node * band + lane] = v;
         }
     }
 }

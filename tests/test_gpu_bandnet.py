@@ -84,3 +84,22 @@ def test_proposals_are_valid_band_offsets(gpu_ctx):
     b = net.propose(costs, guidance, 41, 30, 193, 4, 24).cpu().numpy()
     assert a.shape == (11 * 8,) and np.array_equal(a, b)
     assert a.min() >= 1 and a.max() <= 193 - 24
+
+
+def test_trained_network_against_the_naive_band(gpu_ctx):
+    """What training buys: the band network trained on the GPU (tile-median targets from
+    the exact stage's full-range SGM) against the naive band (each tile's median cost
+    argmin) on held-out 1040x780 scenes with 192 planes, the banded SGM with full-range
+    fallback scored against the full-range SGM over tested nodes."""
+    from chiaro_b200 import bandnet
+    scenes = bandnet.render_scenes("band", list(range(300, 316)) + list(range(900, 906)))
+    samples = [bandnet.samples_from_stage(s, gpu_ctx) for s in scenes]
+    train, held = samples[:16], samples[16:]
+    net = BandNet(gpu_ctx, seed=0)
+    targets = [bandnet.tile_targets(s, 4, "median") for s in train]
+    losses = np.concatenate([net.train(targets, 400, 2e-3), net.train(targets, 200, 5e-4)])
+    scores = bandnet.evaluate(gpu_ctx, held, {"learned": net}, 4, 24, 8)
+    print(scores)
+    assert losses[-1] < 0.2 * losses[0]
+    learned, naive = scores["learned"], scores["naive"]
+    assert learned["within_one_plane"] > naive["within_one_plane"]
