@@ -286,6 +286,7 @@ def run_ours(args, rank, world, local):
     d2h = M * (8 + 4 + 1) + targets * M * (8 + 4)
     e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
 
+    finest = finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap)
     quantised = quantised_sgm(args, scene, work, ctx, torch, device, stream, flush)
     batched = batched_sgm(args, ctx, torch, device, stream, flush)
     band = None
@@ -317,6 +318,7 @@ def run_ours(args, rank, world, local):
                      "traffic": sgm_traffic() if args.workload == "five_view" else None,
                      "traffic_source": "profiles/sgm_five_view_dram.md (ncu dram__bytes_read + write, one call)",
                      "peak_source": peaks["source"], "algorithmic_bytes": work["sgm_bytes"]},
+        "finest_coarse_grid": finest,
         "quantised_sgm": dict(quantised, roofline=dict(
             quantised["roofline"], peak=peaks["hbm_gbs"],
             frac=round(quantised["roofline"]["achieved"] / peaks["hbm_gbs"], 4))),
@@ -347,6 +349,43 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
     ctx.close()
     return line
+
+
+def finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap):
+    """The workload at grid_step 4: the coarse grid (cost volume and SGM) at the direct grid's
+    step, the finest the reference reaches (1041x781 nodes for 4160x3120, four times the
+    default's cells). Same inputs, device buffers and timing as the main leg."""
+    import dataclasses
+
+    options = dataclasses.replace(scene.options, grid_step=4)
+    work = stage_bytes(dataclasses.replace(scene, options=options))
+    opt = options.to_c()
+    lib = ctx.lib
+
+    def step():
+        ctx.check(lib.chiaro_refine_multiview_depth_device(ctx.handle, views, n, scene.reference_index,
+                                                           C.byref(opt), refined, reports, C.byref(dmap)))
+
+    for _ in range(max(args.warmup, 2)):
+        step()
+    steps = max(1, min(args.steps, 5))
+    total, stages = 0.0, []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        step()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+        stages.append(ctx.timings())
+    ms = total / steps
+    return {"grid_step": 4, "coarse_nodes": work["coarse_nodes"], "labels": work["labels"],
+            "sgm_cells_per_step": work["cells"], "ms_per_step": round(ms, 3),
+            "gcells_s": round(work["cells"] / (ms / 1e3) / 1e9, 3),
+            "stage_ms": {k: round(statistics.median(s[k] for s in stages), 4) for k in stages[0]}}
 
 
 def quantised_sgm(args, scene, work, ctx, torch, device, stream, flush):
@@ -480,9 +519,10 @@ def batched_sgm(args, ctx, torch, device, stream, flush):
 
 def learned_band(args, scene, ctx, torch, device, stream, flush):
     """Config 3: the learned band proposal. Two networks (tile-median and tile-mid-range
-    targets) train on the GPU on seeded 1040x780 scenes with 192 planes, labelled by the
-    exact GPU stage's full-range SGM. On held-out scenes of that kind and on this workload's
-    own full-resolution scene, the banded SGM with full-range fallback is scored against the
+    targets) train on the GPU on seeded 1040x780 five-view scenes with 192 planes, labelled
+    by the exact GPU stage's full-range SGM. On held-out scenes of that kind and on this
+    workload's own full-resolution scene at 192 planes, the banded SGM with full-range
+    fallback is scored against the
     full-range SGM (agreement within one plane over tested nodes, fallback rate) beside the
     naive band (each tile's median cost argmin), and timed against the full-range SGM."""
     import numpy as np
@@ -497,7 +537,9 @@ def learned_band(args, scene, ctx, torch, device, stream, flush):
     samples = [bandnet.samples_from_stage(s, ctx) for s in rendered]
     del rendered
     train, held = samples[:args.band_train], samples[args.band_train:]
-    full = bandnet.samples_from_stage(scene, ctx)
+    import dataclasses
+    full = bandnet.samples_from_stage(
+        dataclasses.replace(scene, options=dataclasses.replace(scene.options, planes=192)), ctx)
     nets, training = {}, {}
     for kind in ("median", "midrange"):
         net = bandnet.BandNet(ctx, seed=args.seed)
@@ -563,7 +605,8 @@ def learned_band(args, scene, ctx, torch, device, stream, flush):
     del flat, costs, out
     torch.cuda.empty_cache()
     return {"tile_nodes": tile, "band_labels": width, "fallback_margin_nodes": margin,
-            "train": {"scenes": args.band_train, "workload": "1040x780, reference + 2 sources, 192 planes",
+            "train": {"scenes": args.band_train,
+                      "workload": "five_view's structure at 1040x780 (reference + 4 sources), 192 planes",
                       "render_s": round(render_s, 1), **training},
             "held_out_1040x780": dict(held_scores, scenes=args.band_eval,
                                       wide_tile_fraction=round(float(np.mean(

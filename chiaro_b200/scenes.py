@@ -18,8 +18,9 @@ Named workloads:
     with its default of 2).
   * ``five_view``  – 4160x3120 reference + 4 sources at 20-60 mm baselines,
     12 planes + 3 spheres, 128 planes over 0.4-50 m, default options.
-  * ``band``       – 1040x780 reference + 2 sources, 8 planes + 2 spheres, 192 planes over
-    0.4-25 m: the learned band's training and evaluation scenes.
+  * ``band``       – five_view's structure at 1040x780 (reference + 4 sources, 12 planes +
+    3 spheres, 2-6 cm baselines) with 192 planes over 0.4-50 m: the learned band's
+    training and evaluation scenes.
   * ``small``      – reduced scenes for parity tests.
 """
 from __future__ import annotations
@@ -343,9 +344,9 @@ WORKLOADS: Dict[str, dict] = {
     "five_view": dict(width=4160, height=3120, n_sources=4, n_planes=12, n_spheres=3,
                       depth_range=(500.0, 20000.0), baseline_range=(20.0, 60.0), max_rotation_deg=0.5,
                       distortion=True, options=dict(planes=128, near_depth=400.0, far_depth=50000.0)),
-    "band": dict(width=1040, height=780, n_sources=2, n_planes=8, n_spheres=2, depth_range=(500.0, 15000.0),
-                 baseline_range=(20.0, 50.0), max_rotation_deg=0.3, distortion=True,
-                 options=dict(planes=192, near_depth=400.0, far_depth=25000.0)),
+    "band": dict(width=1040, height=780, n_sources=4, n_planes=12, n_spheres=3, depth_range=(500.0, 20000.0),
+                 baseline_range=(20.0, 60.0), max_rotation_deg=0.5, distortion=True,
+                 options=dict(planes=192, near_depth=400.0, far_depth=50000.0)),
     "small": dict(width=320, height=240, n_sources=2, n_planes=5, n_spheres=1, depth_range=(500.0, 8000.0),
                   baseline_range=(20.0, 40.0), max_rotation_deg=0.3, distortion=True,
                   options=dict(planes=24, near_depth=400.0, far_depth=20000.0)),

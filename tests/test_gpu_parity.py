@@ -204,6 +204,16 @@ def test_stage_with_completion_and_grid_step_bit_exact():
     _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
 
 
+def test_stage_at_the_finest_coarse_grid_bit_exact():
+    """grid_step 4: the coarse grid at the direct grid's step (the finest the reference
+    reaches, depth.rs:326-328), as in the five-view workload's step-4 configuration."""
+    sc = scenes.workload("small", seed=4)
+    opt = DepthOptions(**{**sc.options.__dict__, "grid_step": 4})
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc, options=opt)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+    assert (dmap.provenance == abi.MEASURED).sum() > 0.3 * dmap.provenance.size
+
+
 def test_stage_with_unaccepted_uncalibrated_and_partial_warps():
     sc = scenes.workload("tiny", seed=7, n_sources=3)
     inputs = sc.inputs()
