@@ -58,6 +58,8 @@ def parse_args():
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (0 = --steps)")
     p.add_argument("--band-train", type=int, default=24, help="1040x780 scenes the band network trains on")
     p.add_argument("--band-eval", type=int, default=8, help="held-out 1040x780 scenes of the band evaluation")
+    p.add_argument("--band-train-full", type=int, default=2,
+                   help="full-resolution five-view scenes added to the third band network's training")
     p.add_argument("--no-learned-band", action="store_true")
     return p.parse_args()
 
@@ -520,7 +522,8 @@ def batched_sgm(args, ctx, torch, device, stream, flush):
 def learned_band(args, scene, ctx, torch, device, stream, flush):
     """Config 3: the learned band proposal. Two networks (tile-median and tile-mid-range
     targets) train on the GPU on seeded 1040x780 five-view scenes with 192 planes, labelled
-    by the exact GPU stage's full-range SGM. On held-out scenes of that kind and on this
+    by the exact GPU stage's full-range SGM; a third (tile-median) also sees a few
+    full-resolution five-view scenes of other seeds. On held-out scenes of that kind and on this
     workload's own full-resolution scene at 192 planes, the banded SGM with full-range
     fallback is scored against the
     full-range SGM (agreement within one plane over tested nodes, fallback rate) beside the
@@ -540,21 +543,34 @@ def learned_band(args, scene, ctx, torch, device, stream, flush):
     import dataclasses
     full = bandnet.samples_from_stage(
         dataclasses.replace(scene, options=dataclasses.replace(scene.options, planes=192)), ctx)
+    t0 = time.perf_counter()
+    full_train = [bandnet.samples_from_stage(s, ctx) for s in bandnet.render_scenes(
+        "five_view", range(7000, 7000 + args.band_train_full), options=dict(planes=192))]
+    render_s += time.perf_counter() - t0
     nets, training = {}, {}
-    for kind in ("median", "midrange"):
+    for kind, mixed in (("median", False), ("midrange", False), ("median", True)):
         net = bandnet.BandNet(ctx, seed=args.seed)
         targets = [bandnet.tile_targets(s, tile, kind) for s in train]
+        full_targets = [bandnet.tile_targets(s, tile, kind) for s in full_train] if mixed else []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             e0.record(stream)
-        first = net.train(targets, 400, 2e-3)
-        last = net.train(targets, 200, 5e-4)
+        losses = []
+        for lr, rounds in ((2e-3, 10), (5e-4, 5)):  # 40 steps per round, a third of them full resolution
+            for _ in range(rounds):
+                if full_targets:
+                    losses.append(net.train(targets, 27, lr))
+                    losses.append(net.train(full_targets, 13, lr))
+                else:
+                    losses.append(net.train(targets, 40, lr))
         with torch.cuda.stream(stream):
             e1.record(stream)
         e1.synchronize()
-        nets[f"learned_{kind}"] = net
-        training[kind] = {"steps": 600, "images": len(targets), "ms": round(e0.elapsed_time(e1), 1),
-                          "loss_first": float(first[0]), "loss_last": float(last[-1])}
+        name = f"learned_{kind}" + ("_with_full_resolution" if mixed else "")
+        nets[name] = net
+        training[name] = {"steps": 600, "images": len(targets) + len(full_targets),
+                          "ms": round(e0.elapsed_time(e1), 1), "loss_first": float(losses[0][0]),
+                          "loss_last": float(losses[-1][-1])}
     held_scores = bandnet.evaluate(ctx, held, nets, tile, width, margin)
     full_scores = bandnet.evaluate(ctx, [full], nets, tile, width, margin)
 
@@ -605,7 +621,7 @@ def learned_band(args, scene, ctx, torch, device, stream, flush):
     del flat, costs, out
     torch.cuda.empty_cache()
     return {"tile_nodes": tile, "band_labels": width, "fallback_margin_nodes": margin,
-            "train": {"scenes": args.band_train,
+            "train": {"scenes": args.band_train, "full_resolution_scenes": args.band_train_full,
                       "workload": "five_view's structure at 1040x780 (reference + 4 sources), 192 planes",
                       "render_s": round(render_s, 1), **training},
             "held_out_1040x780": dict(held_scores, scenes=args.band_eval,
