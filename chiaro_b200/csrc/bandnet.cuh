@@ -11,8 +11,9 @@
 // The convolutions are implicit GEMMs on the tensor cores with mma.sync
 // m16n8k16 (bf16 in, fp32 accumulate): a warp owns 16 consecutive pixels of a
 // row and all 32 output channels (four n8 tiles), and walks K = 9 taps x 32
-// input channels in 18 steps, gathering each A fragment straight from the NHWC
-// input (zero outside the image) as 32-bit pairs of channels. The data gradient
+// input channels in 18 steps, its A fragments read by ldmatrix from the window of
+// input rows it staged in shared memory (zero outside the image) and its B
+// fragments from the layer's weights staged there once per CTA. The data gradient
 // is the same kernel with the weights transposed and the taps mirrored, its
 // epilogue masking by the previous layer's ReLU. The weight gradient is a GEMM
 // over pixels (M = co, N = ci, K = pixels) per tap, accumulated in fp32 with
@@ -43,17 +44,9 @@ __device__ __forceinline__ void mma_bf16_16816(float (&c)[4], unsigned a0, unsig
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ unsigned ld_pair(const __nv_bfloat16 *p) {
-    return *reinterpret_cast<const unsigned *>(p);
-}
-
 __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<const unsigned *>(&v);
-}
-
-__device__ __forceinline__ unsigned pack_raw(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (unsigned)__bfloat16_as_ushort(lo) | ((unsigned)__bfloat16_as_ushort(hi) << 16);
 }
 
 // Input features of one node: the reference luminance at the node (guidance / 8);
@@ -90,65 +83,106 @@ __global__ void net_features_kernel(const float *__restrict__ costs, const float
     for (int k = NET_INPUTS; k < NET_CH; ++k) f[k] = __float2bfloat16_rn(0.0f);
 }
 
+// Shared-memory rows of the convolution: 32 bf16 channels padded to 40 (80 bytes), so
+// the eight 16-byte rows an ldmatrix reads fall in distinct banks.
+constexpr int NET_SROW = 40;
+constexpr int NET_WIN = 3 * 18;  // a warp's input window: rows y - 1 .. y + 1, pixels x0 - 1 .. x0 + 16
+constexpr int NET_CONV_WARPS = 4;
+constexpr size_t NET_CONV_SMEM =
+    (size_t)(NET_TAPS * NET_CH + NET_CONV_WARPS * NET_WIN) * NET_SROW * sizeof(__nv_bfloat16);
+
+__device__ __forceinline__ void ldmatrix_x4(unsigned (&r)[4], const __nv_bfloat16 *p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
 // out[p][co] = sum_{tap, ci} in[p + tap][ci] * w[tap][co][ci] + bias[co]; then ReLU
 // (relu), or the mask of a previous activation (mask: zero where mask <= 0). out_f32,
-// when given, receives channel 0 in fp32.
-__global__ void __launch_bounds__(128) net_conv_kernel(const __nv_bfloat16 *__restrict__ in, int images, int height,
-                                                       int width, const __nv_bfloat16 *__restrict__ w,
-                                                       const float *__restrict__ bias, int relu,
-                                                       const __nv_bfloat16 *__restrict__ mask,
-                                                       __nv_bfloat16 *__restrict__ out, float *__restrict__ out_f32) {
-    const int lane = threadIdx.x & 31;
+// when given, receives channel 0 in fp32. Persistent CTAs of four warps: the layer's
+// weights are staged in shared memory once per CTA; each warp stages its tile's 3 x 18
+// pixel window (zero outside the image) with 16-byte loads and feeds the MMAs through
+// ldmatrix. The k order (tap, then channel halves) is fixed, so the sums do not depend
+// on the staging.
+__global__ void __launch_bounds__(32 * NET_CONV_WARPS) net_conv_kernel(
+    const __nv_bfloat16 *__restrict__ in, int images, int height, int width, const __nv_bfloat16 *__restrict__ w,
+    const float *__restrict__ bias, int relu, const __nv_bfloat16 *__restrict__ mask, __nv_bfloat16 *__restrict__ out,
+    float *__restrict__ out_f32) {
+    extern __shared__ __align__(16) __nv_bfloat16 net_smem[];
+    __nv_bfloat16 *wsm = net_smem;                                     // [tap][co][NET_SROW]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __nv_bfloat16 *win = net_smem + (NET_TAPS * NET_CH + warp * NET_WIN) * NET_SROW;  // [3][18][NET_SROW]
     const int group = lane >> 2, tig = lane & 3;
+    // the weights, 16 bytes (8 channels) at a time
+    for (int c = threadIdx.x; c < NET_TAPS * NET_CH * 4; c += blockDim.x) {
+        const int row = c >> 2, part = c & 3;
+        *reinterpret_cast<uint4 *>(wsm + row * NET_SROW + part * 8) =
+            *reinterpret_cast<const uint4 *>(w + (size_t)row * NET_CH + part * 8);
+    }
+    __syncthreads();
     const int segments = (width + 15) / 16;
-    const long tile = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (tile >= (long)images * height * segments) return;  // whole warp
-    const int n = (int)(tile / ((long)height * segments));
-    const int rest = (int)(tile - (long)n * height * segments);
-    const int y = rest / segments, x0 = (rest - y * segments) * 16;
-    const __nv_bfloat16 *image = in + (size_t)n * height * width * NET_CH;
-    float acc[4][4] = {};
-    for (int tap = 0; tap < NET_TAPS; ++tap) {
-        const int yy = y + tap / 3 - 1, dx = tap % 3 - 1;
-        const bool row_in = yy >= 0 && yy < height;
-        const int xa = x0 + group + dx, xb = xa + 8;
-        const bool in_a = row_in && xa >= 0 && xa < width, in_b = row_in && xb >= 0 && xb < width;
-        const __nv_bfloat16 *pa = image + ((size_t)(row_in ? yy : 0) * width + (in_a ? xa : 0)) * NET_CH;
-        const __nv_bfloat16 *pb = image + ((size_t)(row_in ? yy : 0) * width + (in_b ? xb : 0)) * NET_CH;
+    const long tiles = (long)images * height * segments;
+    // ldmatrix row addresses of this lane: matrix j = lane / 8, row lane % 8
+    const int mj = lane >> 3, mr = lane & 7;
+    for (long base = (long)blockIdx.x * NET_CONV_WARPS; base < tiles; base += (long)gridDim.x * NET_CONV_WARPS) {
+        const long tile = base + warp;
+        if (tile >= tiles) break;  // whole warp; no block barrier follows
+        const int n = (int)(tile / ((long)height * segments));
+        const int rest = (int)(tile - (long)n * height * segments);
+        const int y = rest / segments, x0 = (rest - y * segments) * 16;
+        const __nv_bfloat16 *image = in + (size_t)n * height * width * NET_CH;
+        __syncwarp();  // the previous tile's reads of the window are done
+        for (int c = lane; c < NET_WIN * 4; c += 32) {
+            const int px = c >> 2, part = c & 3;
+            const int r = px / 18, xx = x0 - 1 + px % 18, yy = y - 1 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (yy >= 0 && yy < height && xx >= 0 && xx < width)
+                v = *reinterpret_cast<const uint4 *>(image + ((size_t)yy * width + xx) * NET_CH + part * 8);
+            *reinterpret_cast<uint4 *>(win + px * NET_SROW + part * 8) = v;
+        }
+        __syncwarp();
+        float acc[4][4] = {};
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int ci = half * 16 + tig * 2;
-            const unsigned a0 = in_a ? ld_pair(pa + ci) : 0u, a1 = in_b ? ld_pair(pb + ci) : 0u;
-            const unsigned a2 = in_a ? ld_pair(pa + ci + 8) : 0u, a3 = in_b ? ld_pair(pb + ci + 8) : 0u;
+        for (int tap = 0; tap < NET_TAPS; ++tap) {
+            const int r = tap / 3, dx = tap % 3;  // window row and pixel shift
 #pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const __nv_bfloat16 *wp = w + ((size_t)tap * NET_CH + nt * 8 + group) * NET_CH + ci;
-                mma_bf16_16816(acc[nt], a0, a1, a2, a3, ld_pair(wp), ld_pair(wp + 8));
+            for (int half = 0; half < 2; ++half) {
+                unsigned a[4];
+                ldmatrix_x4(a, win + (r * 18 + dx + (mj & 1) * 8 + mr) * NET_SROW + half * 16 + (mj >> 1) * 8);
+#pragma unroll
+                for (int np = 0; np < 2; ++np) {
+                    unsigned b[4];  // b0, b1 of n-tile 2 np, then of n-tile 2 np + 1
+                    ldmatrix_x4(b, wsm + (tap * NET_CH + (2 * np + (mj >> 1)) * 8 + mr) * NET_SROW + half * 16 +
+                                       (mj & 1) * 8);
+                    mma_bf16_16816(acc[2 * np], a[0], a[1], a[2], a[3], b[0], b[1]);
+                    mma_bf16_16816(acc[2 * np + 1], a[0], a[1], a[2], a[3], b[2], b[3]);
+                }
             }
         }
-    }
-    // epilogue: rows group (pixel x0 + group) and group + 8, columns co = nt * 8 + 2 tig + (0, 1)
+        // epilogue: rows group (pixel x0 + group) and group + 8, columns co = nt * 8 + 2 tig + (0, 1)
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        const int x = x0 + group + 8 * half;
-        if (x >= width) continue;
-        const size_t p = ((size_t)n * height + y) * width + x;
+        for (int hh = 0; hh < 2; ++hh) {
+            const int x = x0 + group + 8 * hh;
+            if (x >= width) continue;
+            const size_t p = ((size_t)n * height + y) * width + x;
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            const int co = nt * 8 + tig * 2;
-            float v0 = acc[nt][2 * half] + (bias ? bias[co] : 0.0f);
-            float v1 = acc[nt][2 * half + 1] + (bias ? bias[co + 1] : 0.0f);
-            if (relu) {
-                v0 = fmaxf(v0, 0.0f);
-                v1 = fmaxf(v1, 0.0f);
+            for (int nt = 0; nt < 4; ++nt) {
+                const int co = nt * 8 + tig * 2;
+                float v0 = acc[nt][2 * hh] + (bias ? bias[co] : 0.0f);
+                float v1 = acc[nt][2 * hh + 1] + (bias ? bias[co + 1] : 0.0f);
+                if (relu) {
+                    v0 = fmaxf(v0, 0.0f);
+                    v1 = fmaxf(v1, 0.0f);
+                }
+                if (mask) {
+                    const __nv_bfloat16 *m = mask + p * NET_CH + co;
+                    if (!(__bfloat162float(m[0]) > 0.0f)) v0 = 0.0f;
+                    if (!(__bfloat162float(m[1]) > 0.0f)) v1 = 0.0f;
+                }
+                *reinterpret_cast<unsigned *>(out + p * NET_CH + co) = pack_bf16(v0, v1);
+                if (out_f32 && co == 0) out_f32[p] = v0;
             }
-            if (mask) {
-                const __nv_bfloat16 *m = mask + p * NET_CH + co;
-                if (!(__bfloat162float(m[0]) > 0.0f)) v0 = 0.0f;
-                if (!(__bfloat162float(m[1]) > 0.0f)) v1 = 0.0f;
-            }
-            *reinterpret_cast<unsigned *>(out + p * NET_CH + co) = pack_bf16(v0, v1);
-            if (out_f32 && co == 0) out_f32[p] = v0;
         }
     }
 }
@@ -158,54 +192,71 @@ __global__ void __launch_bounds__(128) net_conv_kernel(const __nv_bfloat16 *__re
 // NET_WGRAD_STEPS pixels); pixels are the flattened (image, y, x) index.
 constexpr int NET_WGRAD_STEPS = 16;
 
-__device__ __forceinline__ __nv_bfloat16 net_at(const __nv_bfloat16 *act, long q, int dy, int dx, int height,
-                                                int width, long total, int ch) {
-    if (q >= total) return __float2bfloat16_rn(0.0f);
-    const long hw = (long)height * width;
-    const long n = q / hw;
-    const int rem = (int)(q - n * hw), y = rem / width + dy, x = rem % width + dx;
-    if (y < 0 || y >= height || x < 0 || x >= width) return __float2bfloat16_rn(0.0f);
-    return act[((n * hw) + (long)y * width + x) * NET_CH + ch];
+__device__ __forceinline__ void ldmatrix_x4_trans(unsigned (&r)[4], const __nv_bfloat16 *p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
 }
 
+// Per step, two lanes stage one of the 16 pixels: its gradient row dpre[q][*] and its
+// tap neighbour's input row in[q + tap][*] (zero outside the image or past the last
+// pixel), 16 bytes at a time, into shared rows of NET_SROW; ldmatrix.trans then reads
+// both as k-major (pixel) fragments.
 __global__ void __launch_bounds__(128) net_wgrad_kernel(const __nv_bfloat16 *__restrict__ in,
                                                         const __nv_bfloat16 *__restrict__ dpre, int images,
                                                         int height, int width, float *__restrict__ dw) {
-    const int lane = threadIdx.x & 31;
+    __shared__ __align__(16) __nv_bfloat16 stage[4][2][16 * NET_SROW];  // [warp][dpre, in][pixel][channel]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int group = lane >> 2, tig = lane & 3;
     const long total = (long)images * height * width;
     const long chunk_pixels = 16L * NET_WGRAD_STEPS;
     const long chunks = (total + chunk_pixels - 1) / chunk_pixels;
-    const long job = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (job >= chunks * NET_TAPS) return;  // whole warp
+    const long job = (long)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (job >= chunks * NET_TAPS) return;  // whole warp; no block barrier follows
     const int tap = (int)(job % NET_TAPS);
     const long q0 = (job / NET_TAPS) * chunk_pixels;
     const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+    __nv_bfloat16 *ds = stage[warp][0], *xs = stage[warp][1];
+    const long hw = (long)height * width;
+    const int mj = lane >> 3, mr = lane & 7;
+    const int pixel = lane >> 1, part = (lane & 1) * 2;  // this lane's staged pixel and 16-byte parts
     float acc[2][4][4] = {};
     for (int step = 0; step < NET_WGRAD_STEPS; ++step) {
-        const long qa = q0 + step * 16 + tig * 2;  // k = 2 tig, 2 tig + 1; then + 8
+        const long q = q0 + step * 16 + pixel;
+        uint4 d0 = make_uint4(0u, 0u, 0u, 0u), d1 = d0, x0 = d0, x1 = d0;
+        if (q < total) {
+            const __nv_bfloat16 *dp = dpre + q * NET_CH + part * 8;
+            d0 = *reinterpret_cast<const uint4 *>(dp);
+            d1 = *reinterpret_cast<const uint4 *>(dp + 8);
+            const long n = q / hw;
+            const int rem = (int)(q - n * hw), y = rem / width + dy, x = rem % width + dx;
+            if (y >= 0 && y < height && x >= 0 && x < width) {
+                const __nv_bfloat16 *xp = in + ((n * hw) + (long)y * width + x) * NET_CH + part * 8;
+                x0 = *reinterpret_cast<const uint4 *>(xp);
+                x1 = *reinterpret_cast<const uint4 *>(xp + 8);
+            }
+        }
+        __syncwarp();  // the previous step's fragments are read
+        *reinterpret_cast<uint4 *>(ds + pixel * NET_SROW + part * 8) = d0;
+        *reinterpret_cast<uint4 *>(ds + pixel * NET_SROW + part * 8 + 8) = d1;
+        *reinterpret_cast<uint4 *>(xs + pixel * NET_SROW + part * 8) = x0;
+        *reinterpret_cast<uint4 *>(xs + pixel * NET_SROW + part * 8 + 8) = x1;
+        __syncwarp();
+        // A (co x pixels) of m-tile mt: matrices (pixels 0-7 | 8-15) x (co m0 | m0 + 8), a0..a3
         unsigned a[2][4];
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt) {
-            const int co = mt * 16 + group;
-            a[mt][0] = pack_raw(net_at(dpre, qa, 0, 0, height, width, total, co),
-                                net_at(dpre, qa + 1, 0, 0, height, width, total, co));
-            a[mt][1] = pack_raw(net_at(dpre, qa, 0, 0, height, width, total, co + 8),
-                                net_at(dpre, qa + 1, 0, 0, height, width, total, co + 8));
-            a[mt][2] = pack_raw(net_at(dpre, qa + 8, 0, 0, height, width, total, co),
-                                net_at(dpre, qa + 9, 0, 0, height, width, total, co));
-            a[mt][3] = pack_raw(net_at(dpre, qa + 8, 0, 0, height, width, total, co + 8),
-                                net_at(dpre, qa + 9, 0, 0, height, width, total, co + 8));
-        }
+        for (int mt = 0; mt < 2; ++mt)
+            ldmatrix_x4_trans(a[mt], ds + ((mj >> 1) * 8 + mr) * NET_SROW + mt * 16 + (mj & 1) * 8);
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            const int ci = nt * 8 + group;
-            const unsigned b0 = pack_raw(net_at(in, qa, dy, dx, height, width, total, ci),
-                                         net_at(in, qa + 1, dy, dx, height, width, total, ci));
-            const unsigned b1 = pack_raw(net_at(in, qa + 8, dy, dx, height, width, total, ci),
-                                         net_at(in, qa + 9, dy, dx, height, width, total, ci));
+        for (int np = 0; np < 2; ++np) {
+            unsigned b[4];  // b0, b1 of n-tile 2 np, then of 2 np + 1 (pixels 0-7 | 8-15)
+            ldmatrix_x4_trans(b, xs + ((mj & 1) * 8 + mr) * NET_SROW + (2 * np + (mj >> 1)) * 8);
 #pragma unroll
-            for (int mt = 0; mt < 2; ++mt) mma_bf16_16816(acc[mt][nt], a[mt][0], a[mt][1], a[mt][2], a[mt][3], b0, b1);
+            for (int mt = 0; mt < 2; ++mt) {
+                mma_bf16_16816(acc[mt][2 * np], a[mt][0], a[mt][1], a[mt][2], a[mt][3], b[0], b[1]);
+                mma_bf16_16816(acc[mt][2 * np + 1], a[mt][0], a[mt][1], a[mt][2], a[mt][3], b[2], b[3]);
+            }
         }
     }
     // C rows: co = mt * 16 + group (+ 8); columns: ci = nt * 8 + 2 tig (+ 1)

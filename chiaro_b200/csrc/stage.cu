@@ -613,15 +613,21 @@ void net_features(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, 
     CK(cudaGetLastError());
 }
 
+// Persistent grid of the convolution: as many CTAs as are resident at once (shared memory
+// allows five per SM), or fewer when there are fewer tiles.
+unsigned net_conv_blocks(chiaro_depth_ctx *ctx, long tiles) {
+    return (unsigned)std::min<size_t>(div_ceil((size_t)tiles, NET_CONV_WARPS), (size_t)ctx->sm_count * 5);
+}
+
 void net_forward(chiaro_depth_ctx *ctx, const NetState &s, const float *params) {
     cudaStream_t st = ctx->stream;
     net_pack_kernel<<<(unsigned)div_ceil((size_t)NET_LAYERS * NET_W, 256), 256, 0, st>>>(params, s.w, s.wt);
     CK(cudaGetLastError());
     const long tiles = (long)s.images * s.height * ((s.width + 15) / 16);
-    const unsigned blocks = (unsigned)div_ceil((size_t)tiles, 4);
+    const unsigned blocks = net_conv_blocks(ctx, tiles);
     for (int l = 0; l < NET_LAYERS; ++l) {
         const bool last = l + 1 == NET_LAYERS;
-        net_conv_kernel<<<blocks, 128, 0, st>>>(s.act[l], s.images, s.height, s.width, s.w + (size_t)l * NET_W,
+        net_conv_kernel<<<blocks, 32 * NET_CONV_WARPS, NET_CONV_SMEM, st>>>(s.act[l], s.images, s.height, s.width, s.w + (size_t)l * NET_W,
                                                 params + (size_t)l * (NET_W + NET_CH) + NET_W, last ? 0 : 1,
                                                 nullptr, s.act[l + 1], last ? s.y : nullptr);
         CK(cudaGetLastError());
@@ -639,7 +645,7 @@ void net_backward(chiaro_depth_ctx *ctx, const NetState &s, const float *params,
     net_loss_kernel<<<eblocks, 256, 0, st>>>(s.y, targets, mask, s.pixels, inverse_count, 0.02f, s.grad_a, loss_sum);
     CK(cudaGetLastError());
     const long tiles = (long)s.images * s.height * ((s.width + 15) / 16);
-    const unsigned cblocks = (unsigned)div_ceil((size_t)tiles, 4);
+    const unsigned cblocks = net_conv_blocks(ctx, tiles);
     const long chunks = (s.pixels + 16L * NET_WGRAD_STEPS - 1) / (16L * NET_WGRAD_STEPS);
     const unsigned wblocks = (unsigned)div_ceil((size_t)chunks * NET_TAPS, 4);
     __nv_bfloat16 *dpre = s.grad_a, *dnext = s.grad_b;
@@ -649,7 +655,7 @@ void net_backward(chiaro_depth_ctx *ctx, const NetState &s, const float *params,
         net_bias_grad_kernel<<<(unsigned)ctx->sm_count * 4, 256, 0, st>>>(dpre, s.pixels, g + NET_W);
         CK(cudaGetLastError());
         if (l > 0) {  // gradient at the previous layer's output, masked by its ReLU
-            net_conv_kernel<<<cblocks, 128, 0, st>>>(dpre, s.images, s.height, s.width, s.wt + (size_t)l * NET_W,
+            net_conv_kernel<<<cblocks, 32 * NET_CONV_WARPS, NET_CONV_SMEM, st>>>(dpre, s.images, s.height, s.width, s.wt + (size_t)l * NET_W,
                                                      nullptr, 0, s.act[l], dnext, nullptr);
             CK(cudaGetLastError());
             std::swap(dpre, dnext);
