@@ -52,35 +52,53 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
 // Input features of one node: the reference luminance at the node (guidance / 8);
 // per bin of the finite labels, the bin's minimum cost minus the node's; the
 // first cost argmin over the finite labels, as (argmin - 1) / (labels - 2); and
-// the node's minimum cost.
+// the node's minimum cost. A warp per node: lanes read consecutive labels, the
+// minima are reduced by shuffles (a minimum does not depend on its order) and the
+// argmin is the smallest label holding the minimum; lane k writes channel k.
 __global__ void net_features_kernel(const float *__restrict__ costs, const float *__restrict__ guidance, int nodes,
                                     int labels, __nv_bfloat16 *__restrict__ features) {
-    const int node = blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= nodes) return;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int node = (int)(((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (node >= nodes) return;  // whole warp
     const float *c = costs + (size_t)node * labels;
-    float bins[NET_BINS];
-    float lowest = INFINITY;
-    int argmin = 1;
     const int finite = labels - 1;
-    for (int b = 0; b < NET_BINS; ++b) {
-        const int l0 = 1 + b * finite / NET_BINS, l1 = 1 + (b + 1) * finite / NET_BINS;
-        float m = INFINITY;
-        for (int l = l0; l < l1; ++l) {
-            const float v = c[l];
-            if (v < lowest) {
-                lowest = v;
-                argmin = l;
-            }
-            m = fminf(m, v);
+    float bins[NET_BINS];
+#pragma unroll
+    for (int b = 0; b < NET_BINS; ++b) bins[b] = INFINITY;
+    float lowest = INFINITY;
+    int argmin = labels;
+    for (int l = 1 + lane; l < labels; l += 32) {
+        const float v = __ldcs(c + l);
+        const int bin = (NET_BINS * l + finite - 1) / finite - 1;  // l0(bin) <= l < l0(bin + 1)
+#pragma unroll
+        for (int b = 0; b < NET_BINS; ++b)
+            if (b == bin) bins[b] = fminf(bins[b], v);
+        if (v < lowest) {  // a lane's labels rise, so this keeps its first minimum
+            lowest = v;
+            argmin = l;
         }
-        bins[b] = m;
     }
-    __nv_bfloat16 *f = features + (size_t)node * NET_CH;
-    f[0] = __float2bfloat16_rn(guidance[node] * 0.125f);
-    for (int b = 0; b < NET_BINS; ++b) f[1 + b] = __float2bfloat16_rn(bins[b] - lowest);
-    f[NET_INPUTS - 2] = __float2bfloat16_rn((float)(argmin - 1) / (float)(labels - 2));
-    f[NET_INPUTS - 1] = __float2bfloat16_rn(lowest);
-    for (int k = NET_INPUTS; k < NET_CH; ++k) f[k] = __float2bfloat16_rn(0.0f);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_xor_sync(full, lowest, off);
+        const int oa = __shfl_xor_sync(full, argmin, off);
+        if (ov < lowest || (ov == lowest && oa < argmin)) {
+            lowest = ov;
+            argmin = oa;
+        }
+#pragma unroll
+        for (int b = 0; b < NET_BINS; ++b) bins[b] = fminf(bins[b], __shfl_xor_sync(full, bins[b], off));
+    }
+    if (argmin == labels) argmin = 1;  // no finite label at all: the first
+    float value = 0.0f;
+    if (lane == 0) value = guidance[node] * 0.125f;
+#pragma unroll
+    for (int b = 0; b < NET_BINS; ++b)
+        if (lane == 1 + b) value = bins[b] - lowest;
+    if (lane == NET_INPUTS - 2) value = (float)(argmin - 1) / (float)(labels - 2);
+    if (lane == NET_INPUTS - 1) value = lowest;
+    features[(size_t)node * NET_CH + lane] = __float2bfloat16_rn(value);
 }
 
 // Shared-memory rows of the convolution: 32 bf16 channels padded to 40 (80 bytes), so

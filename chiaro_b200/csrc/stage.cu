@@ -608,8 +608,8 @@ NetState net_state(chiaro_depth_ctx *ctx, int images, int height, int width) {
 
 void net_features(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, const float *guidance, int labels) {
     const int nodes = (int)s.pixels;
-    net_features_kernel<<<(unsigned)div_ceil((size_t)nodes, 256), 256, 0, ctx->stream>>>(costs, guidance, nodes,
-                                                                                          labels, s.act[0]);
+    net_features_kernel<<<(unsigned)div_ceil((size_t)nodes * 32, 256), 256, 0, ctx->stream>>>(costs, guidance, nodes,
+                                                                                               labels, s.act[0]);
     CK(cudaGetLastError());
 }
 
