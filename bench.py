@@ -289,6 +289,7 @@ def run_ours(args, rank, world, local):
     e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
 
     finest = finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap)
+    resolution = resolution_warp(args, scene, ctx)
     quantised = quantised_sgm(args, scene, work, ctx, torch, device, stream, flush)
     batched = batched_sgm(args, ctx, torch, device, stream, flush)
     band = None
@@ -321,6 +322,7 @@ def run_ours(args, rank, world, local):
                      "traffic_source": "profiles/sgm_five_view_dram.md (ncu dram__bytes_read + write, one call)",
                      "peak_source": peaks["source"], "algorithmic_bytes": work["sgm_bytes"]},
         "finest_coarse_grid": finest,
+        "resolution_warp": resolution,
         "quantised_sgm": dict(quantised, roofline=dict(
             quantised["roofline"], peak=peaks["hbm_gbs"],
             frac=round(quantised["roofline"]["achieved"] / peaks["hbm_gbs"], 4))),
@@ -346,11 +348,47 @@ def run_ours(args, rank, world, local):
                                 "kind": "port", "sample": r["sample"],
                                 "estimated_stage_s": round(r["total_seconds"], 2),
                                 "stage_s": {k: round(v, 3) for k, v in r["stage_seconds"].items()}}
+        # refine_resolution_warp of every target through the oracle, one host thread as the reference runs it
+        from oracle import oracle as oracle_module
+        ref = scene.luminance[scene.reference_index]
+        t0 = time.perf_counter()
+        for t in range(len(scene.cameras)):
+            if t != scene.reference_index:
+                oracle_module.refine_resolution_warp(ref, scene.luminance[t], scene.warps[t], scene.width,
+                                                     scene.height)
+        cpu_ms = (time.perf_counter() - t0) * 1e3 / max(1, len(scene.cameras) - 1)
+        line["resolution_warp"]["cpu_oracle_ms_per_target"] = round(cpu_ms, 1)
+        line["resolution_warp"]["cpu_oracle_threads"] = 1
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
     return line
+
+
+def resolution_warp(args, scene, ctx):
+    """refine_resolution_warp of every target of the workload against the reference module
+    (chiaro_refine_resolution_warp: host planes and warps in and out, transfers included),
+    wall-clock per call after warm-up, with the bit-exact result's report."""
+    from chiaro_b200.resolution import refine_resolution_warp
+    ref = scene.luminance[scene.reference_index]
+    targets = [t for t in range(len(scene.cameras)) if t != scene.reference_index]
+    result = None
+    for _ in range(max(args.warmup, 2)):
+        for t in targets:
+            result = refine_resolution_warp(ref, scene.luminance[t], scene.warps[t], scene.width, scene.height,
+                                            context=ctx)
+    steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for t in targets:
+            result = refine_resolution_warp(ref, scene.luminance[t], scene.warps[t], scene.width, scene.height,
+                                            context=ctx)
+    ms = (time.perf_counter() - t0) * 1e3 / (steps * len(targets))
+    return {"api": "chiaro_b200.resolution.refine_resolution_warp (host planes and warps)",
+            "plane": [ref.width, ref.height], "control_grid": [result.warp.columns, result.warp.rows],
+            "ms_per_target": round(ms, 3), "targets": len(targets),
+            "last_report": {k: round(v, 4) for k, v in vars(result.report).items()}}
 
 
 def finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap):

@@ -108,6 +108,17 @@ class VignettingC(C.Structure):
     ]
 
 
+class ResolutionReportC(C.Structure):
+    """ResolutionAlignmentReport (resolution.rs:88-100)."""
+
+    _fields_ = [
+        ("verified_fraction", C.c_float),
+        ("supported_fraction", C.c_float),
+        ("median_correction_px", C.c_float),
+        ("mean_confidence", C.c_float),
+    ]
+
+
 class WarpC(C.Structure):
     """Warp (align.rs:34-45)."""
 

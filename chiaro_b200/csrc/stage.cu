@@ -29,6 +29,7 @@
 #include "sgm_batch.cuh"
 #include "sgm_band.cuh"
 #include "bandnet.cuh"
+#include "resolution.cuh"
 
 using namespace chiaro;
 
@@ -577,6 +578,205 @@ int run_band(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, i
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(s));
+    return CHIARO_OK;
+}
+
+// ---- refine_resolution_warp (resolution.cuh; resolution.rs:232-439) -----------------
+namespace resolution_host {
+
+WarpRef host_warp(const chiaro_warp &w) {
+    return WarpRef{reinterpret_cast<const float2 *>(w.points), (int)w.step, (int)w.columns, (int)w.rows};
+}
+
+// Rust's f32::clamp: NaN passes through.
+float clamp_rust(float x, float lo, float hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+
+// Warp::confidence (align.rs:113-131).
+float warp_confidence(const chiaro_warp &w, float x, float y) {
+    const float fx = x / (float)w.step, fy = y / (float)w.step;
+    if (fx < 0.0f || fy < 0.0f || !w.confidence) return 0.0f;
+    const int c0 = sat_index(floorf(fx), (int)w.columns - 1), r0 = sat_index(floorf(fy), (int)w.rows - 1);
+    const int c1 = std::min(c0 + 1, (int)w.columns - 1), r1 = std::min(r0 + 1, (int)w.rows - 1);
+    const float tx = fx - (float)c0, ty = fy - (float)r0;
+    auto value = [&](int c, int r) { return w.confidence[(size_t)r * w.columns + c]; };
+    const float top = value(c0, r0) * (1.0f - tx) + value(c1, r0) * tx;
+    const float bottom = value(c0, r1) * (1.0f - tx) + value(c1, r1) * tx;
+    return clamp_rust(top * (1.0f - ty) + bottom * ty, 0.0f, 1.0f);
+}
+
+// Warp::magnification (align.rs:133-145); false for None.
+bool warp_magnification(const chiaro_warp &w, float x, float y, float &out) {
+    const WarpRef r = host_warp(w);
+    const float h = (float)w.step;
+    float ax, ay, bx, by, cx, cy;
+    if (!warp_map(r, x, y, ax, ay) || !warp_map(r, x + h, y, bx, by) || !warp_map(r, x, y + h, cx, cy)) return false;
+    const float dx = std::sqrt((bx - ax) * (bx - ax) + (by - ay) * (by - ay)) / h;
+    const float dy = std::sqrt((cx - ax) * (cx - ax) + (cy - ay) * (cy - ay)) / h;
+    out = std::fmax(std::sqrt(dx * dy), 1.0e-6f);
+    return true;
+}
+
+bool total_less(float a, float b) { return total_key(a) < total_key(b); }
+
+float smoothstep(float v) {
+    v = clamp_rust(v, 0.0f, 1.0f);
+    return v * v * (3.0f - 2.0f * v);
+}
+
+struct Correction {
+    bool some;
+    float x, y;
+};
+
+}  // namespace resolution_host
+
+// The device half (render, patch searches) and the host half (the control grid's
+// median filter, hole completion and report) of refine_resolution_warp. The planes
+// are device pointers; the warps and the report are host memory.
+int run_resolution(chiaro_depth_ctx *ctx, const float *d_reference, int reference_width, int reference_height,
+                   const float *d_target, int target_width, int target_height, const chiaro_warp &base, int width,
+                   int height, chiaro_warp &out, chiaro_resolution_report &report) {
+    using namespace resolution_host;
+    cudaStream_t s = ctx->stream;
+    const int columns = (width + RES_WARP_STEP - 1) / RES_WARP_STEP + 1;
+    const int rows = (height + RES_WARP_STEP - 1) / RES_WARP_STEP + 1;
+    const size_t n_nodes = (size_t)columns * rows;
+    out.step = RES_WARP_STEP;
+    out.columns = (uint64_t)columns;
+    out.rows = (uint64_t)rows;
+    if (out.capacity < n_nodes) return CHIARO_ERR_CAPACITY;
+    // resolution.rs:239-253
+    float magnification = 1.0f;
+    if (!warp_magnification(base, (float)width * 0.5f, (float)height * 0.5f, magnification)) magnification = 1.0f;
+    magnification = clamp_rust(magnification, 0.5f, 4.0f);
+    const int radius = magnification > 1.35f ? RES_MAGNIFIED_RADIUS : RES_RADIUS;
+    // base warp on the device
+    const size_t base_nodes = (size_t)base.columns * base.rows;
+    float2 *d_points = dbuf<float2>(ctx, "res.base", std::max<size_t>(base_nodes, 1));
+    if (base_nodes) upload(ctx, d_points, reinterpret_cast<const float2 *>(base.points), base_nodes);
+    const WarpRef dbase{d_points, (int)base.step, (int)base.columns, (int)base.rows};
+    const size_t plane = (size_t)reference_width * reference_height;
+    float *rendered = dbuf<float>(ctx, "res.rendered", std::max<size_t>(plane, 1));
+    if (plane)
+        resolution_render_kernel<<<(unsigned)std::min<size_t>(div_ceil(plane, 256), (size_t)ctx->sm_count * 16), 256,
+                                   0, s>>>(PlaneRef{d_target, target_width, target_height}, dbase, magnification,
+                                           reference_width, reference_height, rendered);
+    CK(cudaGetLastError());
+    ResolutionNode *d_nodes = dbuf<ResolutionNode>(ctx, "res.nodes", n_nodes);
+    resolution_match_kernel<<<(unsigned)div_ceil(n_nodes * 32, 256), 256, 0, s>>>(
+        PlaneRef{d_reference, reference_width, reference_height}, PlaneRef{rendered, reference_width, reference_height},
+        columns, rows, width, height, radius, d_nodes);
+    CK(cudaGetLastError());
+    std::vector<ResolutionNode> measured(n_nodes);
+    CK(cudaMemcpyAsync(measured.data(), d_nodes, n_nodes * sizeof(ResolutionNode), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+
+    // resolution.rs:307-361: neighbourhood medians of the measured shifts
+    const WarpRef hbase = host_warp(base);
+    std::vector<float> confidence(n_nodes);
+    std::vector<Correction> grid(n_nodes);
+    std::vector<float> corrections;
+    float confidence_sum = 0.0f;
+    float *points = out.points;
+    for (int row = 0; row < rows; ++row)
+        for (int column = 0; column < columns; ++column) {
+            const float rx = (float)(column * RES_WARP_STEP), ry = (float)(row * RES_WARP_STEP);
+            const size_t index = (size_t)row * columns + column;
+            bool refined = false;
+            float qx = 0.0f, qy = 0.0f, local = 0.0f, median_x = 0.0f, median_y = 0.0f;
+            if (measured[index].measured) {
+                std::vector<float> xs, ys;
+                for (int nr = std::max(row - 1, 0); nr <= std::min(row + 1, rows - 1); ++nr)
+                    for (int nc = std::max(column - 1, 0); nc <= std::min(column + 1, columns - 1); ++nc) {
+                        const ResolutionNode &m = measured[(size_t)nr * columns + nc];
+                        if (m.measured) {
+                            xs.push_back(m.shift_x);
+                            ys.push_back(m.shift_y);
+                        }
+                    }
+                if (xs.size() >= 3) {
+                    std::sort(xs.begin(), xs.end(), total_less);
+                    std::sort(ys.begin(), ys.end(), total_less);
+                    median_x = xs[xs.size() / 2];
+                    median_y = ys[ys.size() / 2];
+                    const ResolutionNode &c = measured[index];
+                    if (!(std::hypot(c.shift_x - median_x, c.shift_y - median_y) > 1.5f) &&
+                        warp_map(hbase, rx + median_x, ry + median_y, qx, qy)) {
+                        const float score_confidence = smoothstep((c.score - RES_MINIMUM_SCORE) / 0.20f);
+                        local = score_confidence * warp_confidence(base, rx, ry);
+                        refined = true;
+                    }
+                }
+            }
+            if (refined) {
+                points[2 * index] = qx;
+                points[2 * index + 1] = qy;
+                confidence[index] = local;
+                grid[index] = Correction{true, median_x, median_y};
+                corrections.push_back(std::hypot(median_x, median_y));
+                confidence_sum += local;
+            } else {
+                float bx = NAN, by = NAN;
+                if (!warp_map(hbase, rx, ry, bx, by)) bx = by = NAN;
+                points[2 * index] = bx;
+                points[2 * index + 1] = by;
+                confidence[index] = 0.0f;
+                grid[index] = Correction{false, 0.0f, 0.0f};
+            }
+        }
+    // resolution.rs:362-415: two passes completing short holes in a coherent correction field
+    for (int pass = 0; pass < 2; ++pass) {
+        const std::vector<Correction> grid_snapshot = grid;
+        const std::vector<float> confidence_snapshot = confidence;
+        for (int row = 0; row < rows; ++row)
+            for (int column = 0; column < columns; ++column) {
+                const size_t index = (size_t)row * columns + column;
+                if (grid_snapshot[index].some) continue;
+                std::vector<float> xs, ys;
+                float neighbour_confidence = 0.0f;
+                for (int nr = std::max(row - 1, 0); nr <= std::min(row + 1, rows - 1); ++nr)
+                    for (int nc = std::max(column - 1, 0); nc <= std::min(column + 1, columns - 1); ++nc) {
+                        const size_t neighbour = (size_t)nr * columns + nc;
+                        if (grid_snapshot[neighbour].some) {
+                            xs.push_back(grid_snapshot[neighbour].x);
+                            ys.push_back(grid_snapshot[neighbour].y);
+                            neighbour_confidence += confidence_snapshot[neighbour];
+                        }
+                    }
+                if (xs.size() < 3) continue;
+                std::vector<float> sx = xs, sy = ys;
+                std::sort(sx.begin(), sx.end(), total_less);
+                std::sort(sy.begin(), sy.end(), total_less);
+                const float cx = sx[sx.size() / 2], cy = sy[sy.size() / 2];
+                // coherence over the sorted lists, pairing the k-th sorted x with the k-th sorted y
+                bool coherent = true;
+                for (size_t k = 0; k < sx.size() && coherent; ++k)
+                    coherent = std::hypot(sx[k] - cx, sy[k] - cy) <= 1.5f;
+                if (!coherent) continue;
+                const float rx = (float)(column * RES_WARP_STEP), ry = (float)(row * RES_WARP_STEP);
+                float qx, qy;
+                if (warp_map(hbase, rx + cx, ry + cy, qx, qy)) {
+                    points[2 * index] = qx;
+                    points[2 * index + 1] = qy;
+                    confidence[index] = 0.45f * neighbour_confidence / (float)xs.size();
+                    grid[index] = Correction{true, cx, cy};
+                }
+            }
+    }
+    std::sort(corrections.begin(), corrections.end(), total_less);
+    const size_t verified = corrections.size();
+    size_t supported = 0;
+    for (float c : confidence) supported += c > 0.0f;
+    if (out.confidence) std::copy(confidence.begin(), confidence.end(), out.confidence);
+    const float cells = (float)std::max<size_t>(n_nodes, 1);
+    report.verified_fraction = (float)verified / cells;
+    report.supported_fraction = (float)supported / cells;
+    report.median_correction_px = verified ? corrections[verified / 2] : 0.0f;
+    report.mean_confidence = confidence_sum / (float)std::max<size_t>(verified, 1);
     return CHIARO_OK;
 }
 
@@ -1888,6 +2088,30 @@ int chiaro_luminance_half(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64
         return fail(ctx, e);
     }
     return CHIARO_OK;
+}
+
+int chiaro_refine_resolution_warp(chiaro_depth_ctx *ctx, const float *reference, uint64_t reference_width,
+                                  uint64_t reference_height, const float *target, uint64_t target_width,
+                                  uint64_t target_height, const chiaro_warp *base, uint64_t width, uint64_t height,
+                                  chiaro_warp *out, chiaro_resolution_report *report) {
+    if (!ctx || !reference || !target || !base || !base->points || !out || !out->points || !report)
+        return CHIARO_ERR_ARGUMENT;
+    if (base->step == 0 || base->columns == 0 || base->rows == 0 || reference_width > INT32_MAX ||
+        reference_height > INT32_MAX || target_width > INT32_MAX || target_height > INT32_MAX ||
+        width > INT32_MAX / 2 || height > INT32_MAX / 2)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        const size_t nr = (size_t)reference_width * reference_height, nt = (size_t)target_width * target_height;
+        float *dr = dbuf<float>(ctx, "res.reference", std::max<size_t>(nr, 1));
+        float *dt = dbuf<float>(ctx, "res.target", std::max<size_t>(nt, 1));
+        if (nr) upload(ctx, dr, reference, nr);
+        if (nt) upload(ctx, dt, target, nt);
+        return run_resolution(ctx, dr, (int)reference_width, (int)reference_height, dt, (int)target_width,
+                              (int)target_height, *base, (int)width, (int)height, *out, *report);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
 }
 
 }  // extern "C"

@@ -47,6 +47,9 @@ SIGNATURES = {
                                                     C.c_int]),
     "chiaro_sgm_batch_report": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int)]),
     "chiaro_sgm_banded_report": (C.c_int, [C.c_void_p, P(C.c_int)]),
+    "chiaro_refine_resolution_warp": (C.c_int, [C.c_void_p, P(C.c_float), C.c_uint64, C.c_uint64, P(C.c_float),
+                                                C.c_uint64, C.c_uint64, P(abi.WarpC), C.c_uint64, C.c_uint64,
+                                                P(abi.WarpC), P(abi.ResolutionReportC)]),
     "chiaro_sgm_banded": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_uint64, C.c_uint64, C.c_uint64,
                                     P(C.c_int32), C.c_uint64, C.c_uint64, C.c_uint64, P(C.c_int32), P(C.c_uint8)]),
     "chiaro_sgm_banded_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,

@@ -460,6 +460,34 @@ int chiaro_luminance_half_device(chiaro_depth_ctx *ctx, const uint16_t *samples,
                                  uint64_t height, float black_q6, float white_q6,
                                  const chiaro_vignetting *mesh, float *out);
 
+/* ---- resolution-domain local warp refinement ------------------------------------ */
+
+/* ResolutionAlignmentReport (crates/chiaro-fusion/src/resolution.rs:88-100). */
+typedef struct chiaro_resolution_report {
+    float verified_fraction;     /* control nodes with a coherent, verified match  */
+    float supported_fraction;    /* verified or completed from coherent neighbours */
+    float median_correction_px;  /* median verified correction, reference pixels   */
+    float mean_confidence;       /* mean confidence of the verified nodes          */
+} chiaro_resolution_report;
+
+/* Replaces refine_resolution_warp (crates/chiaro-fusion/src/resolution.rs:232-439),
+ * called per target module at pipeline.rs:1185 and chiaro-stack/src/fusion.rs:384.
+ * reference and target are half-resolution luminance planes (Plane, row-major f32,
+ * host memory); base is the target's warp from the reference raster (width x
+ * height) into the target raster (host memory). The target is resampled to the
+ * reference plane through base (a Gaussian footprint when base magnifies it more
+ * than 1.15x), a 12 x 12 patch is matched around every node of a 32 px grid (radius
+ * 2, or 5 when base magnifies more than 1.35x), and the matches are median-filtered
+ * and completed over the grid. out (host memory) receives the refined warp: step 32,
+ * columns = ceil(width / 32) + 1, rows = ceil(height / 32) + 1 (set on return, also
+ * when out->capacity is too small, which returns CHIARO_ERR_CAPACITY); points and
+ * confidence of columns * rows nodes (confidence may be NULL). Bit-identical to the
+ * reference's result. */
+int chiaro_refine_resolution_warp(chiaro_depth_ctx *ctx, const float *reference, uint64_t reference_width,
+                                  uint64_t reference_height, const float *target, uint64_t target_width,
+                                  uint64_t target_height, const chiaro_warp *base, uint64_t width,
+                                  uint64_t height, chiaro_warp *out, chiaro_resolution_report *report);
+
 /* ---- allocation-free operator --------------------------------------------- */
 
 /* No counterpart in the reference: an allocation-free form of

@@ -2356,3 +2356,313 @@ void oracle_bandnet_loss_grad(const float *params, const float *features, const 
 }
 
 }  // extern "C"
+
+// ---- resolution.rs: refine_resolution_warp (232-439) and image.rs: match_patch (531-640) ----
+
+namespace {
+
+float clamp_rust_o(float x, float lo, float hi) {  // f32::clamp: NaN passes through
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+
+struct PatchMatchO {
+    float shift[2];
+    float score;
+};
+
+// image.rs:531-640
+std::optional<PatchMatchO> match_patch_o(const Plane &reference, const Plane &target, size_t rx, size_t ry,
+                                         size_t size, size_t radius) {
+    if (rx + size > reference.width || ry + size > reference.height || rx < radius || ry < radius ||
+        rx + size + radius > target.width || ry + size + radius > target.height || rx + size > target.width ||
+        ry + size > target.height)
+        return std::nullopt;
+    const float n = (float)(size * size);
+    std::vector<float> ref_values;
+    for (size_t y = ry; y < ry + size; ++y)
+        for (size_t x = rx; x < rx + size; ++x) ref_values.push_back(reference.at(x, y));
+    float total = -0.0f;  // f32 Sum starts at -0.0
+    for (float v : ref_values) total += v;
+    const float ref_mean = total / n;
+    float squares = -0.0f;
+    for (float v : ref_values) squares += (v - ref_mean) * (v - ref_mean);  // powi(2)
+    const float ref_std = std::sqrt(squares / n);
+    if (ref_std < 1e-4f) return std::nullopt;
+    std::vector<float> ref_centered;
+    for (float v : ref_values) ref_centered.push_back(v - ref_mean);
+    const size_t span = 2 * radius + 1;
+    std::vector<float> scores(span * span, -std::numeric_limits<float>::infinity());
+    for (size_t dy = 0; dy < span; ++dy)
+        for (size_t dx = 0; dx < span; ++dx) {
+            const size_t tx = rx + dx - radius, ty = ry + dy - radius;
+            float sum = 0.0f, sum_sq = 0.0f, cross = 0.0f;
+            for (size_t y = 0; y < size; ++y)
+                for (size_t x = 0; x < size; ++x) {
+                    const float t = target.at(tx + x, ty + y), r = ref_centered[y * size + x];
+                    sum += t;
+                    sum_sq += t * t;
+                    cross += t * r;
+                }
+            const float mean = sum / n;
+            const float var = fmax_r(sum_sq / n - mean * mean, 0.0f);
+            if (var < 1e-8f) continue;
+            const float covariance = cross / n;
+            scores[dy * span + dx] = covariance / (std::sqrt(var) * ref_std);
+        }
+    size_t best = 0;  // Iterator::max_by(total_cmp): the last maximum
+    for (size_t i = 1; i < scores.size(); ++i)
+        if (!(total_key_f32(scores[i]) < total_key_f32(scores[best]))) best = i;
+    const float score = scores[best];
+    if (!std::isfinite(score)) return std::nullopt;
+    const size_t bx = best % span, by = best / span;
+    auto refine = [](float minus, float center, float plus) {
+        const float denominator = minus - 2.0f * center + plus;
+        if (std::fabs(denominator) < 1e-9f) return 0.0f;
+        return clamp_rust_o(0.5f * (minus - plus) / denominator, -0.5f, 0.5f);
+    };
+    const float sub_x =
+        bx > 0 && bx + 1 < span ? refine(scores[by * span + bx - 1], score, scores[by * span + bx + 1]) : 0.0f;
+    const float sub_y =
+        by > 0 && by + 1 < span ? refine(scores[(by - 1) * span + bx], score, scores[(by + 1) * span + bx]) : 0.0f;
+    PatchMatchO m;
+    m.shift[0] = (float)bx - (float)radius + sub_x;
+    m.shift[1] = (float)by - (float)radius + sub_y;
+    m.score = score;
+    return m;
+}
+
+// resolution.rs:441-465
+std::optional<float> sample_at_reference_bandwidth_o(const Plane &target, float x, float y, float magnification) {
+    if (magnification <= 1.15f) return target.sample(x, y);
+    const float sigma = fmax_r(0.42f * magnification, 0.55f);
+    const long radius = (long)clamp_rust_o(std::ceil(2.0f * sigma), 1.0f, 4.0f);
+    float sum = 0.0f, weight = 0.0f;
+    for (long dy = -radius; dy <= radius; ++dy)
+        for (long dx = -radius; dx <= radius; ++dx) {
+            const float distance_squared = (float)(dx * dx + dy * dy);
+            const float kernel = std::exp(-0.5f * distance_squared / (sigma * sigma));  // libm expf
+            if (auto value = target.sample(x + (float)dx, y + (float)dy)) {
+                sum += kernel * *value;
+                weight += kernel;
+            }
+        }
+    if (!(weight > 1.0e-8f)) return std::nullopt;
+    return sum / weight;
+}
+
+// Warp::confidence (align.rs:113-131)
+float warp_confidence_o(const chiaro_warp &w, float x, float y) {
+    const float fx = x / (float)w.step, fy = y / (float)w.step;
+    if (fx < 0.0f || fy < 0.0f || !w.confidence) return 0.0f;
+    const size_t c0 = std::min(sat_usize(std::floor(fx)), (size_t)w.columns - 1);
+    const size_t r0 = std::min(sat_usize(std::floor(fy)), (size_t)w.rows - 1);
+    const size_t c1 = std::min(c0 + 1, (size_t)w.columns - 1), r1 = std::min(r0 + 1, (size_t)w.rows - 1);
+    const float tx = fx - (float)c0, ty = fy - (float)r0;
+    auto value = [&](size_t c, size_t r) { return w.confidence[r * w.columns + c]; };
+    const float top = value(c0, r0) * (1.0f - tx) + value(c1, r0) * tx;
+    const float bottom = value(c0, r1) * (1.0f - tx) + value(c1, r1) * tx;
+    return clamp_rust_o(top * (1.0f - ty) + bottom * ty, 0.0f, 1.0f);
+}
+
+bool total_less_o(float a, float b) { return total_key_f32(a) < total_key_f32(b); }
+
+}  // namespace
+
+// match_patch (image.rs:531-640); returns 0 for None.
+extern "C" int oracle_match_patch(const float *reference, size_t reference_width, size_t reference_height, const float *target,
+                       size_t target_width, size_t target_height, size_t rx, size_t ry, size_t size, size_t radius,
+                       float *shift, float *score) {
+    Plane r, t;
+    r.width = reference_width;
+    r.height = reference_height;
+    r.data = reference;
+    t.width = target_width;
+    t.height = target_height;
+    t.data = target;
+    auto m = match_patch_o(r, t, rx, ry, size, radius);
+    if (!m) return 0;
+    shift[0] = m->shift[0];
+    shift[1] = m->shift[1];
+    *score = m->score;
+    return 1;
+}
+
+// refine_resolution_warp (resolution.rs:232-439). out->points / out->confidence hold
+// columns * rows nodes; report = (verified, supported, median correction, mean confidence).
+extern "C" int oracle_refine_resolution_warp(const float *reference_data, size_t reference_width, size_t reference_height,
+                                  const float *target_data, size_t target_width, size_t target_height,
+                                  const chiaro_warp *base_c, size_t width, size_t height, chiaro_warp *out,
+                                  float *report) {
+    constexpr size_t STEP = 32, PATCH = 12, RADIUS = 2, MAGNIFIED_RADIUS = 5;
+    constexpr float MINIMUM_SCORE = 0.72f;
+    Plane reference, target;
+    reference.width = reference_width;
+    reference.height = reference_height;
+    reference.data = reference_data;
+    target.width = target_width;
+    target.height = target_height;
+    target.data = target_data;
+    Warp base;
+    base.step = (size_t)base_c->step;
+    base.columns = (size_t)base_c->columns;
+    base.rows = (size_t)base_c->rows;
+    base.points = base_c->points;
+    // resolution.rs:239-253
+    float magnification = 1.0f;
+    if (!oracle_warp_magnification(base_c, (float)width * 0.5f, (float)height * 0.5f, &magnification))
+        magnification = 1.0f;
+    magnification = clamp_rust_o(magnification, 0.5f, 4.0f);
+    const size_t match_radius = magnification > 1.35f ? MAGNIFIED_RADIUS : RADIUS;
+    // resolution.rs:255-271
+    std::vector<float> rendered_data(reference.width * reference.height);
+    for (size_t y = 0; y < reference.height; ++y)
+        for (size_t x = 0; x < reference.width; ++x) {
+            const float rx = (float)x * 2.0f + 0.5f, ry = (float)y * 2.0f + 0.5f;
+            float value = std::numeric_limits<float>::quiet_NaN();
+            if (auto q = base.map(rx, ry))
+                if (auto v = sample_at_reference_bandwidth_o(target, ((*q)[0] + 0.5f) * 0.5f - 0.5f,
+                                                             ((*q)[1] + 0.5f) * 0.5f - 0.5f, magnification))
+                    value = *v;
+            rendered_data[y * reference.width + x] = value;
+        }
+    Plane rendered;
+    rendered.width = reference.width;
+    rendered.height = reference.height;
+    rendered.data = rendered_data.data();
+    // resolution.rs:273-305
+    const size_t columns = div_ceil(width, STEP) + 1, rows = div_ceil(height, STEP) + 1;
+    out->step = STEP;
+    out->columns = columns;
+    out->rows = rows;
+    if (out->capacity < columns * rows) return CHIARO_ERR_CAPACITY;
+    struct Measured {
+        bool some;
+        float shift[2];
+        float score;
+    };
+    std::vector<Measured> measured(columns * rows, Measured{false, {0, 0}, 0});
+    for (size_t row = 0; row < rows; ++row)
+        for (size_t column = 0; column < columns; ++column) {
+            const float rx = (float)(column * STEP), ry = (float)(row * STEP);
+            if (rx >= (float)width || ry >= (float)height) continue;
+            const long plane_x = (long)std::round((rx - 0.5f) * 0.5f), plane_y = (long)std::round((ry - 0.5f) * 0.5f);
+            const long x = plane_x - (long)PATCH / 2, y = plane_y - (long)PATCH / 2;
+            if (x < (long)match_radius || y < (long)match_radius ||
+                x + (long)PATCH + (long)match_radius > (long)reference.width ||
+                y + (long)PATCH + (long)match_radius > (long)reference.height)
+                continue;
+            // rendered_window_is_covered (resolution.rs:467-484)
+            bool covered = true;
+            for (size_t yy = (size_t)y - match_radius; yy < (size_t)y + PATCH + match_radius && covered; ++yy)
+                for (size_t xx = (size_t)x - match_radius; xx < (size_t)x + PATCH + match_radius && covered; ++xx)
+                    covered = std::isfinite(rendered.at(xx, yy));
+            if (!covered) continue;
+            auto found = match_patch_o(reference, rendered, (size_t)x, (size_t)y, PATCH, match_radius);
+            if (found && found->score >= MINIMUM_SCORE)
+                measured[row * columns + column] =
+                    Measured{true, {found->shift[0] * 2.0f, found->shift[1] * 2.0f}, found->score};
+        }
+    // resolution.rs:307-361
+    struct Correction {
+        bool some;
+        float v[2];
+    };
+    std::vector<float> confidence(columns * rows);
+    std::vector<Correction> grid(columns * rows);
+    std::vector<float> corrections;
+    float confidence_sum = 0.0f;
+    for (size_t row = 0; row < rows; ++row)
+        for (size_t column = 0; column < columns; ++column) {
+            const float rx = (float)(column * STEP), ry = (float)(row * STEP);
+            const size_t index = row * columns + column;
+            std::optional<std::pair<F2, std::pair<float, F2>>> refined;
+            if (measured[index].some) {
+                std::vector<float> xs, ys;
+                for (size_t nr = row > 0 ? row - 1 : 0; nr <= std::min(row + 1, rows - 1); ++nr)
+                    for (size_t nc = column > 0 ? column - 1 : 0; nc <= std::min(column + 1, columns - 1); ++nc)
+                        if (measured[nr * columns + nc].some) {
+                            xs.push_back(measured[nr * columns + nc].shift[0]);
+                            ys.push_back(measured[nr * columns + nc].shift[1]);
+                        }
+                if (xs.size() >= 3) {
+                    std::stable_sort(xs.begin(), xs.end(), total_less_o);
+                    std::stable_sort(ys.begin(), ys.end(), total_less_o);
+                    const F2 median = {xs[xs.size() / 2], ys[ys.size() / 2]};
+                    const Measured &c = measured[index];
+                    if (!(std::hypot(c.shift[0] - median[0], c.shift[1] - median[1]) > 1.5f))
+                        if (auto q = base.map(rx + median[0], ry + median[1])) {
+                            const float v = clamp_rust_o((c.score - MINIMUM_SCORE) / 0.20f, 0.0f, 1.0f);
+                            const float score_confidence = v * v * (3.0f - 2.0f * v);  // smoothstep
+                            const float base_confidence = warp_confidence_o(*base_c, rx, ry);
+                            refined = std::make_pair(*q, std::make_pair(score_confidence * base_confidence, median));
+                        }
+                }
+            }
+            if (refined) {
+                out->points[2 * index] = refined->first[0];
+                out->points[2 * index + 1] = refined->first[1];
+                confidence[index] = refined->second.first;
+                grid[index] = Correction{true, {refined->second.second[0], refined->second.second[1]}};
+                corrections.push_back(std::hypot(refined->second.second[0], refined->second.second[1]));
+                confidence_sum += refined->second.first;
+            } else {
+                auto q = base.map(rx, ry);
+                out->points[2 * index] = q ? (*q)[0] : std::numeric_limits<float>::quiet_NaN();
+                out->points[2 * index + 1] = q ? (*q)[1] : std::numeric_limits<float>::quiet_NaN();
+                confidence[index] = 0.0f;
+                grid[index] = Correction{false, {0, 0}};
+            }
+        }
+    // resolution.rs:362-415
+    for (int pass = 0; pass < 2; ++pass) {
+        const auto grid_snapshot = grid;
+        const auto confidence_snapshot = confidence;
+        for (size_t row = 0; row < rows; ++row)
+            for (size_t column = 0; column < columns; ++column) {
+                const size_t index = row * columns + column;
+                if (grid_snapshot[index].some) continue;
+                std::vector<float> xs, ys;
+                float neighbour_sum = 0.0f;
+                for (size_t nr = row > 0 ? row - 1 : 0; nr <= std::min(row + 1, rows - 1); ++nr)
+                    for (size_t nc = column > 0 ? column - 1 : 0; nc <= std::min(column + 1, columns - 1); ++nc) {
+                        const size_t neighbour = nr * columns + nc;
+                        if (grid_snapshot[neighbour].some) {
+                            xs.push_back(grid_snapshot[neighbour].v[0]);
+                            ys.push_back(grid_snapshot[neighbour].v[1]);
+                            neighbour_sum += confidence_snapshot[neighbour];
+                        }
+                    }
+                if (xs.size() < 3) continue;
+                std::stable_sort(xs.begin(), xs.end(), total_less_o);
+                std::stable_sort(ys.begin(), ys.end(), total_less_o);
+                const F2 correction = {xs[xs.size() / 2], ys[ys.size() / 2]};
+                bool coherent = true;
+                for (size_t k = 0; k < xs.size(); ++k)
+                    if (!(std::hypot(xs[k] - correction[0], ys[k] - correction[1]) <= 1.5f)) {
+                        coherent = false;
+                        break;
+                    }
+                if (!coherent) continue;
+                const float rx = (float)(column * STEP), ry = (float)(row * STEP);
+                if (auto q = base.map(rx + correction[0], ry + correction[1])) {
+                    out->points[2 * index] = (*q)[0];
+                    out->points[2 * index + 1] = (*q)[1];
+                    confidence[index] = 0.45f * neighbour_sum / (float)xs.size();
+                    grid[index] = Correction{true, {correction[0], correction[1]}};
+                }
+            }
+    }
+    std::stable_sort(corrections.begin(), corrections.end(), total_less_o);
+    const size_t verified = corrections.size();
+    size_t supported = 0;
+    for (float c : confidence) supported += c > 0.0f;
+    if (out->confidence) std::copy(confidence.begin(), confidence.end(), out->confidence);
+    const float cells = (float)std::max<size_t>(columns * rows, 1);
+    report[0] = (float)verified / cells;
+    report[1] = (float)supported / cells;
+    report[2] = verified ? corrections[verified / 2] : 0.0f;
+    report[3] = confidence_sum / (float)std::max<size_t>(verified, 1);
+    return CHIARO_OK;
+}

@@ -80,6 +80,12 @@ def lib():
             "oracle_map_from": (C.c_int, [P(CameraC), P(CameraC), P(C.c_double), C.c_double, P(C.c_double)]),
             "oracle_warp_map": (C.c_int, [P(WarpC), C.c_float, C.c_float, P(C.c_float)]),
             "oracle_warp_magnification": (C.c_int, [P(WarpC), C.c_float, C.c_float, P(C.c_float)]),
+            "oracle_match_patch": (C.c_int, [P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_float), C.c_size_t,
+                                             C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                                             P(C.c_float), P(C.c_float)]),
+            "oracle_refine_resolution_warp": (C.c_int, [P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_float),
+                                                        C.c_size_t, C.c_size_t, P(WarpC), C.c_size_t, C.c_size_t,
+                                                        P(WarpC), P(C.c_float)]),
             "oracle_plane_sample": (C.c_float, [P(C.c_float), C.c_size_t, C.c_size_t, C.c_float, C.c_float,
                                                 P(C.c_int)]),
             "oracle_score_one_view": (C.c_int, [P(ViewC), C.c_size_t, C.c_size_t, C.c_size_t, C.c_double,
@@ -194,3 +200,25 @@ def semi_global_costs(costs: np.ndarray, guidance: np.ndarray, columns: int, row
 
 def threads_default() -> int:
     return os.cpu_count() or 1
+
+
+def refine_resolution_warp(reference, target, base, width: int, height: int):
+    """oracle_refine_resolution_warp (resolution.rs:232-439) on chiaro_b200's Plane and Warp
+    types; returns a chiaro_b200.resolution.ResolutionWarp."""
+    from chiaro_b200.align import Warp
+    from chiaro_b200.resolution import WARP_STEP, ResolutionAlignmentReport, ResolutionWarp, warp_c
+    F = C.POINTER(C.c_float)
+    columns, rows = -(-width // WARP_STEP) + 1, -(-height // WARP_STEP) + 1
+    points = np.empty((columns * rows, 2), np.float32)
+    confidence = np.empty(columns * rows, np.float32)
+    out = WarpC(capacity=columns * rows, points=points.ctypes.data_as(F), confidence=confidence.ctypes.data_as(F))
+    report = np.zeros(4, np.float32)
+    ref = np.ascontiguousarray(reference.data, np.float32)
+    tgt = np.ascontiguousarray(target.data, np.float32)
+    base_c = warp_c(base)
+    st = lib().oracle_refine_resolution_warp(ref.ctypes.data_as(F), reference.width, reference.height,
+                                             tgt.ctypes.data_as(F), target.width, target.height, C.byref(base_c),
+                                             width, height, C.byref(out), report.ctypes.data_as(F))
+    assert st == 0, st
+    return ResolutionWarp(Warp(WARP_STEP, columns, rows, points, confidence),
+                          ResolutionAlignmentReport(*[float(v) for v in report]))
