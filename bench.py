@@ -290,6 +290,7 @@ def run_ours(args, rank, world, local):
 
     finest = finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap)
     resolution = resolution_warp(args, scene, ctx)
+    alignment = global_alignment(args, scene, ctx)
     quantised = quantised_sgm(args, scene, work, ctx, torch, device, stream, flush)
     batched = batched_sgm(args, ctx, torch, device, stream, flush)
     band = None
@@ -323,6 +324,7 @@ def run_ours(args, rank, world, local):
                      "peak_source": peaks["source"], "algorithmic_bytes": work["sgm_bytes"]},
         "finest_coarse_grid": finest,
         "resolution_warp": resolution,
+        "global_alignment": alignment,
         "quantised_sgm": dict(quantised, roofline=dict(
             quantised["roofline"], peak=peaks["hbm_gbs"],
             frac=round(quantised["roofline"]["achieved"] / peaks["hbm_gbs"], 4))),
@@ -359,6 +361,22 @@ def run_ours(args, rank, world, local):
         cpu_ms = (time.perf_counter() - t0) * 1e3 / max(1, len(scene.cameras) - 1)
         line["resolution_warp"]["cpu_oracle_ms_per_target"] = round(cpu_ms, 1)
         line["resolution_warp"]["cpu_oracle_threads"] = 1
+        # align_module of one target through the oracle (one host thread, as the reference runs a module)
+        from chiaro_b200.abi import AlignmentReportC, WarpC
+        from chiaro_b200.align import AlignOptions, align_input_c
+        inputs = scene.inputs()
+        target = next(t for t in range(len(scene.cameras)) if t != scene.reference_index)
+        ref_c, keep_r = align_input_c(inputs[scene.reference_index])
+        tgt_c, keep_t = align_input_c(inputs[target])
+        columns, rows = -(-scene.width // 32) + 1, -(-scene.height // 32) + 1
+        points = np.empty(2 * columns * rows, np.float32)
+        out = WarpC(capacity=columns * rows, points=points.ctypes.data_as(C.POINTER(C.c_float)))
+        gain, report, opt = C.c_float(), AlignmentReportC(), AlignOptions().to_c()
+        t0 = time.perf_counter()
+        oracle_module.lib().oracle_align_module(C.byref(ref_c), C.byref(tgt_c), 0, C.byref(opt), None, C.byref(out),
+                                                C.byref(gain), C.byref(report), None)
+        line["global_alignment"]["cpu_oracle_ms_per_target"] = round((time.perf_counter() - t0) * 1e3, 1)
+        line["global_alignment"]["cpu_oracle_threads"] = 1
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -389,6 +407,30 @@ def resolution_warp(args, scene, ctx):
             "plane": [ref.width, ref.height], "control_grid": [result.warp.columns, result.warp.rows],
             "ms_per_target": round(ms, 3), "targets": len(targets),
             "last_report": {k: round(v, 4) for k, v in vars(result.report).items()}}
+
+
+def global_alignment(args, scene, ctx):
+    """align_module of every target of the workload to the reference module
+    (chiaro_align_module: host planes in, host warp out, calibrated initialisation),
+    wall-clock per call after warm-up, with the last call's report."""
+    from chiaro_b200.align import AlignOptions, align_module
+    inputs = scene.inputs()
+    targets = [t for t in range(len(scene.cameras)) if t != scene.reference_index]
+    result = None
+    for _ in range(max(args.warmup, 2)):
+        for t in targets:
+            result = align_module(inputs[scene.reference_index], inputs[t], AlignOptions(), context=ctx)
+    steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for t in targets:
+            result = align_module(inputs[scene.reference_index], inputs[t], AlignOptions(), context=ctx)
+    ms = (time.perf_counter() - t0) * 1e3 / (steps * len(targets))
+    r = result.report
+    return {"api": "chiaro_b200.align.align_module (host planes, calibrated initialisation)",
+            "ms_per_target": round(ms, 3), "targets": len(targets), "status": r.status,
+            "levels": [[lv.scale, lv.patches, lv.inliers, round(lv.median_residual_px, 3)] for lv in r.levels],
+            "inlier_ratio": round(r.inlier_ratio, 4), "gain": round(result.gain, 4)}
 
 
 def finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap):

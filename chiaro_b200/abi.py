@@ -108,6 +108,67 @@ class VignettingC(C.Structure):
     ]
 
 
+class AlignInputC(C.Structure):
+    """AlignInput (align.rs:246-257)."""
+
+    _fields_ = [
+        ("luminance", C.POINTER(C.c_float)),
+        ("luma_width", C.c_uint64),
+        ("luma_height", C.c_uint64),
+        ("width", C.c_uint64),
+        ("height", C.c_uint64),
+        ("has_camera", C.c_int32),
+        ("camera", CameraC),
+        ("nominal_focal_px", C.c_double),
+    ]
+
+
+class AlignOptionsC(C.Structure):
+    """AlignOptions (align.rs:205-243) without the depth options."""
+
+    _fields_ = [
+        ("grid_step", C.c_uint64),
+        ("patch", C.c_uint64),
+        ("coarse_radius", C.c_uint64),
+        ("min_score", C.c_float),
+        ("inlier_px", C.c_float),
+        ("min_inlier_ratio", C.c_float),
+        ("refine", C.c_int32),
+    ]
+
+
+ALIGN_MAX_LEVELS = 24
+
+
+class AlignLevelC(C.Structure):
+    _fields_ = [("scale", C.c_uint64), ("patches", C.c_uint64), ("inliers", C.c_uint64),
+                ("median_residual_px", C.c_float)]
+
+
+class AlignmentReportC(C.Structure):
+    """The alignment fields of AlignmentReport (align.rs:160-200)."""
+
+    _fields_ = [
+        ("initialised_from", C.c_int32),
+        ("status", C.c_int32),
+        ("accepted", C.c_int32),
+        ("coverage", C.c_float),
+        ("correction_median_px", C.c_float * 2),
+        ("inliers", C.c_uint64),
+        ("patches", C.c_uint64),
+        ("residual_median_px", C.c_float),
+        ("residual_p90_px", C.c_float),
+        ("inlier_ratio", C.c_float),
+        ("n_levels", C.c_uint64),
+        ("levels", AlignLevelC * ALIGN_MAX_LEVELS),
+    ]
+
+
+INITIALISED_FROM = ["reference", None, "calibration", "nominal focal group"]  # 1: the seed's name
+ALIGN_STATUS = ["reference", "rejected", "factory model only", "refined", "weak refinement",
+                "no correlation support; factory model kept"]
+
+
 class ResolutionReportC(C.Structure):
     """ResolutionAlignmentReport (resolution.rs:88-100)."""
 

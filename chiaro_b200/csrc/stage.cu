@@ -30,6 +30,7 @@
 #include "sgm_band.cuh"
 #include "bandnet.cuh"
 #include "resolution.cuh"
+#include "align.cuh"
 
 using namespace chiaro;
 
@@ -779,6 +780,9 @@ int run_resolution(chiaro_depth_ctx *ctx, const float *d_reference, int referenc
     report.mean_confidence = confidence_sum / (float)std::max<size_t>(verified, 1);
     return CHIARO_OK;
 }
+
+// ---- align_module (align.cuh, align_run.cuh; align.rs:281-830) -----------------------
+#include "align_run.cuh"
 
 // ---- learned band network (bandnet.cuh) ----------------------------------------------
 struct NetState {
@@ -2088,6 +2092,34 @@ int chiaro_luminance_half(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64
         return fail(ctx, e);
     }
     return CHIARO_OK;
+}
+
+void chiaro_align_options_default(chiaro_align_options *options) {
+    if (!options) return;
+    *options = chiaro_align_options{32, 32, 12, 0.5f, 3.0f, 0.45f, 1};  // AlignOptions::default (align.rs:229-243)
+}
+
+int chiaro_align_module(chiaro_depth_ctx *ctx, const chiaro_align_input *reference, const chiaro_align_input *target,
+                        int32_t target_is_reference, const chiaro_align_options *options, const chiaro_warp *seed,
+                        chiaro_warp *out_warp, float *gain, chiaro_alignment_report *report) {
+    if (!ctx || !reference || !target || !options || !out_warp || !out_warp->points || !gain || !report)
+        return CHIARO_ERR_ARGUMENT;
+    if (!reference->luminance || !target->luminance || options->grid_step == 0 || options->patch == 0 ||
+        reference->width > INT32_MAX / 2 || reference->height > INT32_MAX / 2 || reference->luma_width > INT32_MAX ||
+        reference->luma_height > INT32_MAX || target->luma_width > INT32_MAX || target->luma_height > INT32_MAX ||
+        options->patch > 4096 || options->coarse_radius > 4096 || options->grid_step > INT32_MAX ||
+        (seed && (!seed->points || seed->step == 0 || seed->columns == 0 || seed->rows == 0)))
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        return run_align(ctx, *reference, *target, target_is_reference != 0, *options, seed, *out_warp, *gain,
+                         *report);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    } catch (const align_host::Failure &e) {
+        ctx->error = e.message;
+        return CHIARO_INVALID;
+    }
 }
 
 int chiaro_refine_resolution_warp(chiaro_depth_ctx *ctx, const float *reference, uint64_t reference_width,

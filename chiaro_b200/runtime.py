@@ -47,6 +47,10 @@ SIGNATURES = {
                                                     C.c_int]),
     "chiaro_sgm_batch_report": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int)]),
     "chiaro_sgm_banded_report": (C.c_int, [C.c_void_p, P(C.c_int)]),
+    "chiaro_align_options_default": (None, [P(abi.AlignOptionsC)]),
+    "chiaro_align_module": (C.c_int, [C.c_void_p, P(abi.AlignInputC), P(abi.AlignInputC), C.c_int32,
+                                      P(abi.AlignOptionsC), P(abi.WarpC), P(abi.WarpC), P(C.c_float),
+                                      P(abi.AlignmentReportC)]),
     "chiaro_refine_resolution_warp": (C.c_int, [C.c_void_p, P(C.c_float), C.c_uint64, C.c_uint64, P(C.c_float),
                                                 C.c_uint64, C.c_uint64, P(abi.WarpC), C.c_uint64, C.c_uint64,
                                                 P(abi.WarpC), P(abi.ResolutionReportC)]),

@@ -460,6 +460,92 @@ int chiaro_luminance_half_device(chiaro_depth_ctx *ctx, const uint16_t *samples,
                                  uint64_t height, float black_q6, float white_q6,
                                  const chiaro_vignetting *mesh, float *out);
 
+/* ---- global alignment ------------------------------------------------------------- */
+
+/* AlignInput (crates/chiaro-fusion/src/align.rs:246-257). */
+typedef struct chiaro_align_input {
+    const float *luminance;   /* half-resolution log luminance, luma_width * luma_height */
+    uint64_t luma_width;
+    uint64_t luma_height;
+    uint64_t width;           /* raster */
+    uint64_t height;
+    int32_t has_camera;       /* camera.is_some() */
+    chiaro_camera camera;
+    double nominal_focal_px;  /* used without cameras */
+} chiaro_align_input;
+
+/* AlignOptions (align.rs:205-243) without the depth options. */
+typedef struct chiaro_align_options {
+    uint64_t grid_step;      /* 32 */
+    uint64_t patch;          /* 32 */
+    uint64_t coarse_radius;  /* 12 */
+    float min_score;         /* 0.5 */
+    float inlier_px;         /* 3.0 */
+    float min_inlier_ratio;  /* 0.45 */
+    int32_t refine;          /* 1 */
+} chiaro_align_options;
+
+/* AlignmentReport.initialised_from and .status (align.rs:290-300, 463-477). */
+enum chiaro_align_initialisation {
+    CHIARO_INIT_REFERENCE = 0,
+    CHIARO_INIT_SEED = 1,
+    CHIARO_INIT_CALIBRATION = 2,
+    CHIARO_INIT_NOMINAL_FOCAL_GROUP = 3
+};
+enum chiaro_align_status {
+    CHIARO_ALIGN_REFERENCE = 0,
+    CHIARO_ALIGN_REJECTED = 1,      /* "rejected: NN% correspondence consensus" (inlier_ratio) */
+    CHIARO_ALIGN_FACTORY_MODEL = 2,
+    CHIARO_ALIGN_REFINED = 3,
+    CHIARO_ALIGN_WEAK_REFINEMENT = 4,
+    CHIARO_ALIGN_NO_SUPPORT = 5     /* "no correlation support; factory model kept" */
+};
+
+#define CHIARO_ALIGN_MAX_LEVELS 24
+
+/* LevelReport (align.rs:202-207). */
+typedef struct chiaro_align_level {
+    uint64_t scale;
+    uint64_t patches;
+    uint64_t inliers;
+    float median_residual_px;  /* NaN when the level had no fit */
+} chiaro_align_level;
+
+/* The alignment fields of AlignmentReport (align.rs:160-200); the camera name,
+ * focus fields and the depth report belong to other stages. */
+typedef struct chiaro_alignment_report {
+    int32_t initialised_from;  /* enum chiaro_align_initialisation */
+    int32_t status;            /* enum chiaro_align_status */
+    int32_t accepted;
+    float coverage;
+    float correction_median_px[2];
+    uint64_t inliers;
+    uint64_t patches;
+    float residual_median_px;
+    float residual_p90_px;
+    float inlier_ratio;
+    uint64_t n_levels;         /* coarsest first, as the reference pushes them */
+    chiaro_align_level levels[CHIARO_ALIGN_MAX_LEVELS];
+} chiaro_alignment_report;
+
+void chiaro_align_options_default(chiaro_align_options *options);
+
+/* Replaces align_module / align_module_seeded (align.rs:281-519), called per module
+ * by the pipeline before the depth stage. target_is_reference stands for the
+ * reference's name comparison (the reference aligns to itself with an identity
+ * warp); seed (NULL for none) is the externally predicted warp. The target plane
+ * is matched against the reference over both luminance pyramids: the rendering
+ * through the current homography, the patch searches and the RANSAC inlier counts
+ * run on the GPU, the homography fits and the report on the host. out_warp (host
+ * memory, step options->grid_step, capacity >= columns * rows; step, columns and
+ * rows are set on return) receives the warp, gain the photometric gain. Returns
+ * CHIARO_INVALID where the reference returns Err (no correlation in the
+ * no-calibration search), with its message in chiaro_depth_last_error. */
+int chiaro_align_module(chiaro_depth_ctx *ctx, const chiaro_align_input *reference,
+                        const chiaro_align_input *target, int32_t target_is_reference,
+                        const chiaro_align_options *options, const chiaro_warp *seed,
+                        chiaro_warp *out_warp, float *gain, chiaro_alignment_report *report);
+
 /* ---- resolution-domain local warp refinement ------------------------------------ */
 
 /* ResolutionAlignmentReport (crates/chiaro-fusion/src/resolution.rs:88-100). */

@@ -32,9 +32,11 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <functional>
 #include <optional>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -2665,4 +2667,500 @@ extern "C" int oracle_refine_resolution_warp(const float *reference_data, size_t
     report[2] = verified ? corrections[verified / 2] : 0.0f;
     report[3] = confidence_sum / (float)std::max<size_t>(verified, 1);
     return CHIARO_OK;
+}
+
+// ---- align.rs: align_module_seeded (281-519) and its helpers (521-830) -------------------
+
+namespace {
+
+struct PlaneBuf {  // an owned Plane
+    size_t width = 0, height = 0;
+    std::vector<float> data;
+    Plane view() const {
+        Plane p;
+        p.width = width;
+        p.height = height;
+        p.data = data.data();
+        return p;
+    }
+    float at(size_t x, size_t y) const { return data[y * width + x]; }
+};
+
+PlaneBuf plane_copy(const float *data, size_t width, size_t height) {
+    PlaneBuf p;
+    p.width = width;
+    p.height = height;
+    p.data.assign(data, data + width * height);
+    return p;
+}
+
+// Plane::downsample (image.rs:469-483)
+PlaneBuf downsample_o(const PlaneBuf &in) {
+    PlaneBuf out;
+    out.width = std::max<size_t>(in.width / 2, 1);
+    out.height = std::max<size_t>(in.height / 2, 1);
+    out.data.resize(out.width * out.height);
+    for (size_t j = 0; j < out.height; ++j)
+        for (size_t i = 0; i < out.width; ++i) {
+            const size_t x = 2 * i, y = 2 * j, x1 = std::min(x + 1, in.width - 1), y1 = std::min(y + 1, in.height - 1);
+            out.data[j * out.width + i] = 0.25f * (in.at(x, y) + in.at(x1, y) + in.at(x, y1) + in.at(x1, y1));
+        }
+    return out;
+}
+
+// Plane::pyramid (image.rs:487-497)
+std::vector<PlaneBuf> pyramid_o(const PlaneBuf &base, size_t min_size) {
+    std::vector<PlaneBuf> levels{base};
+    while (std::min(levels.back().width, levels.back().height) / 2 >= std::max<size_t>(min_size, 8))
+        levels.push_back(downsample_o(levels.back()));
+    return levels;
+}
+
+struct OwnedWarp {  // Warp with owned arrays
+    size_t step = 0, columns = 0, rows = 0;
+    std::vector<float> points, confidence;
+    Warp view() const {
+        Warp w;
+        w.step = step;
+        w.columns = columns;
+        w.rows = rows;
+        w.points = points.data();
+        return w;
+    }
+};
+
+// Warp::from_fn (align.rs:50-80)
+template <class F>
+OwnedWarp from_fn_o(size_t width, size_t height, size_t step, F map) {
+    OwnedWarp w;
+    w.step = step;
+    w.columns = div_ceil(width, step) + 1;
+    w.rows = div_ceil(height, step) + 1;
+    for (size_t row = 0; row < w.rows; ++row)
+        for (size_t column = 0; column < w.columns; ++column) {
+            const Vec2 p = {(double)(column * step), (double)(row * step)};
+            const std::optional<Vec2> q = map(p);
+            if (q) {
+                w.points.push_back((float)(*q)[0]);
+                w.points.push_back((float)(*q)[1]);
+                w.confidence.push_back(1.0f);
+            } else {
+                w.points.push_back(std::numeric_limits<float>::quiet_NaN());
+                w.points.push_back(std::numeric_limits<float>::quiet_NaN());
+                w.confidence.push_back(0.0f);
+            }
+        }
+    return w;
+}
+
+Mat3 mat_mul_o(const Mat3 &a, const Mat3 &b) {  // math.rs:48-56
+    Mat3 out{};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[i][j] = a[i][0] * b[0][j] + a[i][1] * b[1][j] + a[i][2] * b[2][j];
+    return out;
+}
+
+std::optional<Vec2> apply_homography_o(const Mat3 &h, const Vec2 &p) {  // math.rs:131-138
+    const Vec3 v = mul_vec(h, {p[0], p[1], 1.0});
+    if (std::fabs(v[2]) < 1e-12) return std::nullopt;
+    return Vec2{v[0] / v[2], v[1] / v[2]};
+}
+
+// solve_linear (align.rs:765-793)
+std::optional<std::array<double, 8>> solve_linear_o(std::array<std::array<double, 8>, 8> a, std::array<double, 8> b) {
+    for (size_t column = 0; column < 8; ++column) {
+        size_t pivot = column;  // max_by(total_cmp) over |a[i][column]|: the last maximum
+        for (size_t i = column + 1; i < 8; ++i)
+            if (!(total_key_f64(std::fabs(a[i][column])) < total_key_f64(std::fabs(a[pivot][column])))) pivot = i;
+        if (std::fabs(a[pivot][column]) < 1e-12) return std::nullopt;
+        std::swap(a[column], a[pivot]);
+        std::swap(b[column], b[pivot]);
+        const std::array<double, 8> pivot_row = a[column];
+        for (size_t row = column + 1; row < 8; ++row) {
+            const double factor = a[row][column] / pivot_row[column];
+            for (size_t k = column; k < 8; ++k) a[row][k] -= factor * pivot_row[k];
+            b[row] -= factor * b[column];
+        }
+    }
+    std::array<double, 8> x{};
+    for (int row = 7; row >= 0; --row) {
+        double sum = b[row];
+        for (size_t k = row + 1; k < 8; ++k) sum -= a[row][k] * x[k];
+        x[row] = sum / a[row][row];
+    }
+    return x;
+}
+
+struct PairO {
+    Vec2 a, b;
+    float score;
+};
+
+// fit_homography_least_squares (align.rs:702-760)
+std::optional<Mat3> fit_least_squares_o(const std::vector<PairO> &pairs) {
+    if (pairs.size() < 4) return std::nullopt;
+    const double n = (double)pairs.size();
+    auto mean = [&](auto f) {
+        double s = -0.0;  // f64 Sum
+        for (const PairO &p : pairs) s += f(p);
+        return s / n;
+    };
+    const double ax = mean([](const PairO &p) { return p.a[0]; }), ay = mean([](const PairO &p) { return p.a[1]; });
+    const double bx = mean([](const PairO &p) { return p.b[0]; }), by = mean([](const PairO &p) { return p.b[1]; });
+    const double sa = dmax_r(mean([&](const PairO &p) {
+        return std::sqrt((p.a[0] - ax) * (p.a[0] - ax) + (p.a[1] - ay) * (p.a[1] - ay));
+    }), 1e-9);
+    const double sb = dmax_r(mean([&](const PairO &p) {
+        return std::sqrt((p.b[0] - bx) * (p.b[0] - bx) + (p.b[1] - by) * (p.b[1] - by));
+    }), 1e-9);
+    std::array<std::array<double, 8>, 8> ata{};
+    std::array<double, 8> atb{};
+    for (const PairO &p : pairs) {
+        const double w = dmax_r((double)p.score, 0.05);
+        const double x = (p.a[0] - ax) / sa, y = (p.a[1] - ay) / sa;
+        const double u = (p.b[0] - bx) / sb, v = (p.b[1] - by) / sb;
+        const double rows[2][8] = {{x, y, 1.0, 0.0, 0.0, 0.0, -u * x, -u * y}, {0.0, 0.0, 0.0, x, y, 1.0, -v * x, -v * y}};
+        const double rhs[2] = {u, v};
+        for (int r = 0; r < 2; ++r)
+            for (int i = 0; i < 8; ++i) {
+                atb[i] += w * rows[r][i] * rhs[r];
+                for (int j = 0; j < 8; ++j) ata[i][j] += w * rows[r][i] * rows[r][j];
+            }
+    }
+    const auto s = solve_linear_o(ata, atb);
+    if (!s) return std::nullopt;
+    const Mat3 normalized = {{{(*s)[0], (*s)[1], (*s)[2]}, {(*s)[3], (*s)[4], (*s)[5]}, {(*s)[6], (*s)[7], 1.0}}};
+    const Mat3 t_a = {{{1.0 / sa, 0.0, -ax / sa}, {0.0, 1.0 / sa, -ay / sa}, {0.0, 0.0, 1.0}}};
+    const Mat3 t_b_inv = {{{sb, 0.0, bx}, {0.0, sb, by}, {0.0, 0.0, 1.0}}};
+    Mat3 h = mat_mul_o(mat_mul_o(t_b_inv, normalized), t_a);
+    const double scale = h[2][2];
+    if (std::fabs(scale) < 1e-12 || !std::isfinite(scale)) return std::nullopt;
+    for (auto &row : h)
+        for (double &v : row) v = v / scale;
+    return h;
+}
+
+struct FitO {
+    Mat3 h;
+    size_t inliers;
+    std::vector<float> residuals;
+};
+
+// fit_homography_ransac (align.rs:631-700)
+std::optional<FitO> fit_ransac_o(const std::vector<PairO> &pairs, float threshold) {
+    if (pairs.size() < 6) return std::nullopt;
+    std::vector<size_t> best_inliers;
+    uint64_t state = 0x9E3779B97F4A7C15ull ^ (uint64_t)pairs.size();
+    auto next = [&](size_t n) {
+        state = state * 6364136223846793005ull + 1442695040888963407ull;
+        return (size_t)(state >> 33) % n;
+    };
+    for (int iteration = 0; iteration < 300; ++iteration) {
+        size_t sample[4] = {0, 0, 0, 0};
+        for (int slot = 0; slot < 4; ++slot)
+            for (;;) {
+                const size_t candidate = next(pairs.size());
+                bool taken = false;
+                for (int k = 0; k < slot; ++k) taken = taken || sample[k] == candidate;
+                if (!taken) {
+                    sample[slot] = candidate;
+                    break;
+                }
+            }
+        std::vector<PairO> subset;
+        for (size_t i : sample) subset.push_back(pairs[i]);
+        const auto h = fit_least_squares_o(subset);
+        if (!h) continue;
+        std::vector<size_t> inliers;
+        for (size_t i = 0; i < pairs.size(); ++i) {
+            const auto p = apply_homography_o(*h, pairs[i].a);
+            if (p && std::sqrt(((*p)[0] - pairs[i].b[0]) * ((*p)[0] - pairs[i].b[0]) +
+                               ((*p)[1] - pairs[i].b[1]) * ((*p)[1] - pairs[i].b[1])) <= (double)threshold)
+                inliers.push_back(i);
+        }
+        if (inliers.size() > best_inliers.size()) best_inliers = inliers;
+    }
+    if (best_inliers.size() < 6) return std::nullopt;
+    std::vector<PairO> inlier_pairs;
+    for (size_t i : best_inliers) inlier_pairs.push_back(pairs[i]);
+    const auto h = fit_least_squares_o(inlier_pairs);
+    if (!h) return std::nullopt;
+    FitO fit{*h, 0, {}};
+    for (const PairO &pair : pairs)
+        if (auto p = apply_homography_o(*h, pair.a)) {
+            const float r = (float)std::sqrt(((*p)[0] - pair.b[0]) * ((*p)[0] - pair.b[0]) +
+                                             ((*p)[1] - pair.b[1]) * ((*p)[1] - pair.b[1]));
+            if (r <= threshold) {
+                ++fit.inliers;
+                fit.residuals.push_back(r);
+            }
+        }
+    if (fit.inliers < 6) return std::nullopt;
+    std::stable_sort(fit.residuals.begin(), fit.residuals.end(), total_less_o);
+    return fit;
+}
+
+// photometric_gain (align.rs:795-826)
+std::optional<float> photometric_gain_o(const Plane &reference, const Plane &target, const Warp &warp) {
+    std::vector<float> ratios;
+    const size_t step = 16;
+    for (size_t y = step; y + step < reference.height; y += step)
+        for (size_t x = step; x + step < reference.width; x += step) {
+            const float rx = (float)x * 2.0f + 0.5f, ry = (float)y * 2.0f + 0.5f;
+            const auto q = warp.map(rx, ry);
+            if (!q) continue;
+            const auto t = target.sample(((*q)[0] - 0.5f) / 2.0f, ((*q)[1] - 0.5f) / 2.0f);
+            if (!t) continue;
+            const float r = reference.at(x, y);
+            const float lr = (std::exp(r) - 1.0f) / 1000.0f, lt = (std::exp(*t) - 1.0f) / 1000.0f;
+            if (lr > 0.01f && lt > 0.01f && lr < 0.95f && lt < 0.95f) ratios.push_back(lr / lt);
+        }
+    if (ratios.size() < 16) return std::nullopt;
+    std::stable_sort(ratios.begin(), ratios.end(), total_less_o);
+    return clamp_rust_o(ratios[ratios.size() / 2], 0.25f, 4.0f);
+}
+
+// coarse_global_shift (align.rs:561-628); nullopt with a message for Err
+std::optional<Vec2> coarse_global_shift_o(const PlaneBuf &reference_luma, const PlaneBuf &target_luma, double scale,
+                                          float min_score, std::string &error) {
+    const auto reference_pyramid = pyramid_o(reference_luma, 32);
+    const PlaneBuf &reference_plane = reference_pyramid.back();
+    const double reference_scale = (double)((size_t)1 << (reference_pyramid.size() - 1));
+    const auto target_pyramid = pyramid_o(target_luma, 16);
+    const double wanted = reference_scale * scale;
+    const size_t target_level =
+        std::min(sat_usize(dmax_r(std::round(std::log2(wanted)), 0.0)), target_pyramid.size() - 1);
+    const PlaneBuf &target_plane = target_pyramid[target_level];
+    const double target_scale = (double)((size_t)1 << target_level);
+    const float ratio = (float)(target_scale / wanted);
+    const size_t rw = sat_usize(fmax_r(std::floor((float)target_plane.width * ratio), 4.0f));
+    const size_t rh = sat_usize(fmax_r(std::floor((float)target_plane.height * ratio), 4.0f));
+    PlaneBuf resampled;
+    resampled.width = rw;
+    resampled.height = rh;
+    resampled.data.resize(rw * rh);
+    const Plane tp = target_plane.view();
+    for (size_t y = 0; y < rh; ++y)
+        for (size_t x = 0; x < rw; ++x) resampled.data[y * rw + x] = tp.sample((float)x / ratio, (float)y / ratio).value_or(0.0f);
+    if (rw + 2 > reference_plane.width || rh + 2 > reference_plane.height) return Vec2{0.0, 0.0};
+    const size_t patch = std::min({rw, rh, reference_plane.width / 2, reference_plane.height / 2});
+    const size_t radius = std::max<size_t>((std::min(reference_plane.width, reference_plane.height) - patch) / 2, 1);
+    const size_t rx = (reference_plane.width - patch) / 2, ry = (reference_plane.height - patch) / 2;
+    const size_t tx = (rw - patch) / 2, ty = (rh - patch) / 2;
+    PlaneBuf embedded;
+    embedded.width = reference_plane.width;
+    embedded.height = reference_plane.height;
+    embedded.data.assign(embedded.width * embedded.height, std::numeric_limits<float>::quiet_NaN());
+    for (size_t y = 0; y < patch; ++y)
+        for (size_t x = 0; x < patch; ++x) embedded.data[(ry + y) * embedded.width + rx + x] = resampled.at(tx + x, ty + y);
+    const auto found =
+        match_patch_o(reference_plane.view(), embedded.view(), rx, ry, patch, std::min({radius, rx, ry}));
+    if (!found) {
+        error = "no correlation between the module and the reference";
+        return std::nullopt;
+    }
+    if (found->score < min_score * 0.6f) {
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "module does not correlate with the reference (%.2f)", found->score);
+        error = buf;
+        return std::nullopt;
+    }
+    return Vec2{-(double)found->shift[0] * reference_scale * 2.0 * scale,
+                -(double)found->shift[1] * reference_scale * 2.0 * scale};
+}
+
+}  // namespace
+
+// fit_homography_ransac (align.rs:631-700) over (ax, ay, bx, by) pairs with f32 scores.
+// Returns 0 for None; h is row-major.
+extern "C" int oracle_fit_homography_ransac(const double *points, const float *scores, size_t n, float threshold,
+                                            double *h, size_t *inliers, float *residuals) {
+    std::vector<PairO> pairs(n);
+    for (size_t i = 0; i < n; ++i)
+        pairs[i] = PairO{{points[4 * i], points[4 * i + 1]}, {points[4 * i + 2], points[4 * i + 3]}, scores[i]};
+    const auto fit = fit_ransac_o(pairs, threshold);
+    if (!fit) return 0;
+    for (int i = 0; i < 9; ++i) h[i] = fit->h[i / 3][i % 3];
+    *inliers = fit->inliers;
+    if (residuals) std::copy(fit->residuals.begin(), fit->residuals.end(), residuals);
+    return 1;
+}
+
+// align_module_seeded (align.rs:281-519). error (optional, 128 bytes) receives the Err message.
+extern "C" int oracle_align_module(const chiaro_align_input *reference, const chiaro_align_input *target,
+                                   int target_is_reference, const chiaro_align_options *options,
+                                   const chiaro_warp *seed, chiaro_warp *out_warp, float *gain,
+                                   chiaro_alignment_report *report, char *error) {
+    constexpr double FAR_DEPTH = 1.0e8;
+    const size_t width = (size_t)reference->width, height = (size_t)reference->height;
+    std::memset(report, 0, sizeof(*report));
+    auto emit = [&](const OwnedWarp &w) {
+        out_warp->step = w.step;
+        out_warp->columns = w.columns;
+        out_warp->rows = w.rows;
+        if (out_warp->capacity < w.columns * w.rows) return (int)CHIARO_ERR_CAPACITY;
+        std::copy(w.points.begin(), w.points.end(), out_warp->points);
+        if (out_warp->confidence) std::copy(w.confidence.begin(), w.confidence.end(), out_warp->confidence);
+        return (int)CHIARO_OK;
+    };
+    if (target_is_reference) {
+        const OwnedWarp w = from_fn_o(width, height, options->grid_step, [](const Vec2 &p) { return std::optional<Vec2>(p); });
+        report->initialised_from = CHIARO_INIT_REFERENCE;
+        report->coverage = 1.0f;
+        report->inlier_ratio = 1.0f;
+        report->accepted = 1;
+        report->status = CHIARO_ALIGN_REFERENCE;
+        *gain = 1.0f;
+        return emit(w);
+    }
+    const PlaneBuf reference_luma = plane_copy(reference->luminance, reference->luma_width, reference->luma_height);
+    const PlaneBuf target_luma = plane_copy(target->luminance, target->luma_width, target->luma_height);
+    // Step 1 (align.rs:311-345)
+    OwnedWarp initial_grid;
+    if (seed) {
+        report->initialised_from = CHIARO_INIT_SEED;
+        initial_grid.step = seed->step;
+        initial_grid.columns = seed->columns;
+        initial_grid.rows = seed->rows;
+        initial_grid.points.assign(seed->points, seed->points + 2 * seed->columns * seed->rows);
+        initial_grid.confidence.assign(seed->columns * seed->rows, 1.0f);
+        if (seed->confidence) initial_grid.confidence.assign(seed->confidence, seed->confidence + seed->columns * seed->rows);
+    } else if (reference->has_camera && target->has_camera) {
+        report->initialised_from = CHIARO_INIT_CALIBRATION;
+        const Camera reference_camera(reference->camera), target_camera(target->camera);
+        initial_grid = from_fn_o(width, height, 8, [&](const Vec2 &p) -> std::optional<Vec2> {
+            auto q = target_camera.map_from(reference_camera, p, FAR_DEPTH);
+            if (q && std::isfinite((*q)[0]) && std::isfinite((*q)[1])) return q;
+            return std::nullopt;
+        });
+    } else {
+        report->initialised_from = CHIARO_INIT_NOMINAL_FOCAL_GROUP;
+        const double scale = target->nominal_focal_px / reference->nominal_focal_px;
+        const double cx = ((double)width - 1.0) / 2.0, cy = ((double)height - 1.0) / 2.0;
+        const double tx = ((double)target->width - 1.0) / 2.0, ty = ((double)target->height - 1.0) / 2.0;
+        std::string message;
+        const auto shift = coarse_global_shift_o(reference_luma, target_luma, scale, options->min_score, message);
+        if (!shift) {
+            if (error) std::snprintf(error, 128, "%s", message.c_str());
+            return CHIARO_INVALID;
+        }
+        initial_grid = from_fn_o(width, height, 8, [&](const Vec2 &p) -> std::optional<Vec2> {
+            return Vec2{(p[0] - cx) * scale + tx + (*shift)[0], (p[1] - cy) * scale + ty + (*shift)[1]};
+        });
+    }
+    const Warp initial_view = initial_grid.view();
+    auto initial = [&](const Vec2 &p) -> std::optional<Vec2> {
+        auto q = initial_view.map((float)p[0], (float)p[1]);
+        if (!q) return std::nullopt;
+        return Vec2{(double)(*q)[0], (double)(*q)[1]};
+    };
+    // Step 2 (align.rs:347-455)
+    Mat3 correction = {{{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}}};
+    std::vector<float> finest_residuals;
+    if (options->refine) {
+        const auto reference_pyramid = pyramid_o(reference_luma, 96);
+        const auto target_pyramid = pyramid_o(target_luma, 48);
+        double magnification;
+        {
+            const Vec2 c = {(double)width / 2.0, (double)height / 2.0};
+            const double h = 64.0;
+            const auto a = initial(c), b = initial({c[0] + h, c[1]}), d = initial({c[0], c[1] + h});
+            if (a && b && d) {
+                const double dx = std::sqrt(((*b)[0] - (*a)[0]) * ((*b)[0] - (*a)[0]) + ((*b)[1] - (*a)[1]) * ((*b)[1] - (*a)[1])) / h;
+                const double dy = std::sqrt(((*d)[0] - (*a)[0]) * ((*d)[0] - (*a)[0]) + ((*d)[1] - (*a)[1]) * ((*d)[1] - (*a)[1])) / h;
+                magnification = std::sqrt(dx * dy);
+            } else {
+                magnification = target->nominal_focal_px / reference->nominal_focal_px;
+            }
+        }
+        for (size_t level = reference_pyramid.size(); level-- > 0;) {
+            const size_t scale = (size_t)1 << level;
+            const Plane reference_plane = reference_pyramid[level].view();
+            const size_t target_level = std::min(
+                sat_usize(dmax_r(std::round(std::log2((double)scale * magnification)), 0.0)), target_pyramid.size() - 1);
+            const Plane target_plane = target_pyramid[target_level].view();
+            const double target_scale = (double)((size_t)1 << target_level);
+            // render_through (align.rs:523-549)
+            PlaneBuf rendered;
+            rendered.width = reference_plane.width;
+            rendered.height = reference_plane.height;
+            rendered.data.resize(rendered.width * rendered.height);
+            for (size_t y = 0; y < rendered.height; ++y)
+                for (size_t x = 0; x < rendered.width; ++x) {
+                    auto to_raster = [&](float v) { return ((double)v * (double)scale * 2.0) + (double)scale - 0.5; };
+                    auto from_raster = [&](double v) { return (float)((v + 0.5) / (2.0 * target_scale) - 0.5); };
+                    float value = std::numeric_limits<float>::quiet_NaN();
+                    if (auto c = apply_homography_o(correction, {to_raster((float)x), to_raster((float)y)}))
+                        if (auto q = initial(*c))
+                            if (auto s = target_plane.sample(from_raster((*q)[0]), from_raster((*q)[1]))) value = *s;
+                    rendered.data[y * rendered.width + x] = value;
+                }
+            const Plane rendered_view = rendered.view();
+            const size_t radius = level + 1 == reference_pyramid.size() ? (size_t)options->coarse_radius : 3;
+            const size_t patch = std::max<size_t>(std::min<size_t>(options->patch, reference_plane.width / 4), 8);
+            std::vector<PairO> pairs;
+            const size_t stride = patch / 2;
+            for (size_t y = radius; y + patch + radius <= reference_plane.height; y += stride)
+                for (size_t x = radius; x + patch + radius <= reference_plane.width; x += stride) {
+                    bool covered = true;  // rendered_covered (align.rs:551-559)
+                    for (size_t row = y; row < y + patch && covered; ++row)
+                        for (size_t col = x; col < x + patch && covered; ++col)
+                            covered = !std::isnan(rendered_view.at(col, row));
+                    if (!covered) continue;
+                    const auto found = match_patch_o(reference_plane, rendered_view, x, y, patch, radius);
+                    if (!found || !(found->score >= options->min_score)) continue;
+                    auto convert = [&](float v) { return (double)v * (double)scale * 2.0 + (double)scale - 0.5; };
+                    const float half = (float)patch / 2.0f;
+                    const Vec2 centre = {convert((float)x + half), convert((float)y + half)};
+                    const Vec2 shifted = {convert((float)x + half + found->shift[0]), convert((float)y + half + found->shift[1])};
+                    pairs.push_back(PairO{centre, shifted, found->score});
+                }
+            const float threshold = fmax_r(options->inlier_px * (float)scale * 2.0f, options->inlier_px);
+            chiaro_align_level &lr = report->levels[report->n_levels < CHIARO_ALIGN_MAX_LEVELS ? report->n_levels : CHIARO_ALIGN_MAX_LEVELS - 1];
+            if (auto fit = fit_ransac_o(pairs, threshold)) {
+                correction = mat_mul_o(correction, fit->h);
+                lr = chiaro_align_level{scale * 2, pairs.size(), fit->inliers, fit->residuals[fit->residuals.size() / 2]};
+                if (level == 0) {
+                    finest_residuals = fit->residuals;
+                    report->patches = pairs.size();
+                    report->inliers = fit->inliers;
+                }
+            } else {
+                lr = chiaro_align_level{scale * 2, pairs.size(), 0, std::numeric_limits<float>::quiet_NaN()};
+            }
+            if (report->n_levels < CHIARO_ALIGN_MAX_LEVELS) ++report->n_levels;
+        }
+    }
+    // Final warp and report (align.rs:457-519)
+    const OwnedWarp warp = from_fn_o(width, height, options->grid_step, [&](const Vec2 &p) -> std::optional<Vec2> {
+        auto corrected = apply_homography_o(correction, p);
+        if (!corrected) return std::nullopt;
+        return initial(*corrected);
+    });
+    size_t covered = 0;
+    for (size_t i = 0; i < warp.columns * warp.rows; ++i) {
+        const float qx = warp.points[2 * i], qy = warp.points[2 * i + 1];
+        covered += std::isfinite(qx) && qx >= 0.0f && qy >= 0.0f && qx <= (float)(target->width - 1) &&
+                   qy <= (float)(target->height - 1);
+    }
+    report->coverage = (float)covered / (float)(warp.columns * warp.rows);
+    if (!finest_residuals.empty()) {
+        report->residual_median_px = finest_residuals[finest_residuals.size() / 2];
+        report->residual_p90_px = finest_residuals[std::min(finest_residuals.size() * 9 / 10, finest_residuals.size() - 1)];
+    }
+    {
+        const Vec2 centre = {(double)(width / 2), (double)(height / 2)};
+        const Vec2 moved = apply_homography_o(correction, centre).value_or(centre);
+        report->correction_median_px[0] = (float)(moved[0] - centre[0]);
+        report->correction_median_px[1] = (float)(moved[1] - centre[1]);
+    }
+    report->inlier_ratio = report->patches == 0 ? 0.0f : (float)report->inliers / (float)report->patches;
+    report->accepted = !options->refine || report->inlier_ratio >= options->min_inlier_ratio;
+    report->status = !report->accepted ? CHIARO_ALIGN_REJECTED
+                     : !options->refine ? CHIARO_ALIGN_FACTORY_MODEL
+                     : report->inliers >= 12 && report->residual_median_px < options->inlier_px ? CHIARO_ALIGN_REFINED
+                     : report->inliers > 0 ? CHIARO_ALIGN_WEAK_REFINEMENT
+                                           : CHIARO_ALIGN_NO_SUPPORT;
+    *gain = photometric_gain_o(reference_luma.view(), target_luma.view(), warp.view()).value_or(1.0f);
+    return emit(warp);
 }

@@ -80,6 +80,11 @@ def lib():
             "oracle_map_from": (C.c_int, [P(CameraC), P(CameraC), P(C.c_double), C.c_double, P(C.c_double)]),
             "oracle_warp_map": (C.c_int, [P(WarpC), C.c_float, C.c_float, P(C.c_float)]),
             "oracle_warp_magnification": (C.c_int, [P(WarpC), C.c_float, C.c_float, P(C.c_float)]),
+            "oracle_fit_homography_ransac": (C.c_int, [P(C.c_double), P(C.c_float), C.c_size_t, C.c_float,
+                                                       P(C.c_double), P(C.c_size_t), P(C.c_float)]),
+            "oracle_align_module": (C.c_int, [P(abi.AlignInputC), P(abi.AlignInputC), C.c_int,
+                                              P(abi.AlignOptionsC), P(WarpC), P(WarpC), P(C.c_float),
+                                              P(abi.AlignmentReportC), C.c_char_p]),
             "oracle_match_patch": (C.c_int, [P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_float), C.c_size_t,
                                              C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
                                              P(C.c_float), P(C.c_float)]),
