@@ -31,6 +31,7 @@
 #include "bandnet.cuh"
 #include "resolution.cuh"
 #include "align.cuh"
+#include "consumers.cuh"
 
 using namespace chiaro;
 
@@ -2087,6 +2088,52 @@ int chiaro_luminance_half(chiaro_depth_ctx *ctx, const uint16_t *samples, uint64
         }
         launch_luminance(ctx, ds, width, height, black_q6, white_q6, m, dout);
         download(ctx, out, dout, n_out);
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_warp_sample_device(chiaro_depth_ctx *ctx, const chiaro_warp *warp, const float *xy, uint64_t n,
+                              float *mapped, float *confidence) {
+    if (!ctx || !warp || !warp->points || !mapped || (n && !xy)) return CHIARO_ERR_ARGUMENT;
+    if (warp->step == 0 || warp->columns == 0 || warp->rows == 0 || warp->columns > INT32_MAX ||
+        warp->rows > INT32_MAX || warp->step > INT32_MAX)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        if (n == 0) return CHIARO_OK;
+        const WarpRef w{reinterpret_cast<const float2 *>(warp->points), (int)warp->step, (int)warp->columns,
+                        (int)warp->rows};
+        warp_sample_kernel<<<(unsigned)std::min<uint64_t>(div_ceil((size_t)n, 256), (uint64_t)ctx->sm_count * 16), 256,
+                             0, ctx->stream>>>(w, warp->confidence, reinterpret_cast<const float2 *>(xy), (long)n,
+                                               reinterpret_cast<float2 *>(mapped), confidence);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->stream));
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_depth_sample_nearest_device(chiaro_depth_ctx *ctx, const chiaro_depth_map *map, const float *xy,
+                                       uint64_t n, double *depth, float *confidence, uint8_t *provenance,
+                                       int64_t *node) {
+    if (!ctx || !map || (n && !xy)) return CHIARO_ERR_ARGUMENT;
+    if ((depth && !map->depth) || (confidence && !map->confidence) || (provenance && !map->provenance) ||
+        map->columns > INT32_MAX || map->rows > INT32_MAX || map->step > INT32_MAX)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        if (n == 0) return CHIARO_OK;
+        depth_sample_nearest_kernel<<<(unsigned)std::min<uint64_t>(div_ceil((size_t)n, 256), (uint64_t)ctx->sm_count * 16),
+                                      256, 0, ctx->stream>>>(map->depth, map->confidence, map->provenance,
+                                                             (int)map->columns, (int)map->rows, (int)map->step,
+                                                             reinterpret_cast<const float2 *>(xy), (long)n, depth,
+                                                             confidence, provenance,
+                                                             reinterpret_cast<long long *>(node));
+        CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->stream));
     } catch (const CudaError &e) {
         return fail(ctx, e);

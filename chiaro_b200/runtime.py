@@ -47,6 +47,10 @@ SIGNATURES = {
                                                     C.c_int]),
     "chiaro_sgm_batch_report": (C.c_int, [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int)]),
     "chiaro_sgm_banded_report": (C.c_int, [C.c_void_p, P(C.c_int)]),
+    "chiaro_warp_sample_device": (C.c_int, [C.c_void_p, P(abi.WarpC), C.c_void_p, C.c_uint64, C.c_void_p,
+                                            C.c_void_p]),
+    "chiaro_depth_sample_nearest_device": (C.c_int, [C.c_void_p, P(abi.DepthMapC), C.c_void_p, C.c_uint64,
+                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "chiaro_align_options_default": (None, [P(abi.AlignOptionsC)]),
     "chiaro_align_module": (C.c_int, [C.c_void_p, P(abi.AlignInputC), P(abi.AlignInputC), C.c_int32,
                                       P(abi.AlignOptionsC), P(abi.WarpC), P(abi.WarpC), P(C.c_float),

@@ -460,6 +460,26 @@ int chiaro_luminance_half_device(chiaro_depth_ctx *ctx, const uint16_t *samples,
                                  uint64_t height, float black_q6, float white_q6,
                                  const chiaro_vignetting *mesh, float *out);
 
+/* ---- consumers of the stage's outputs ------------------------------------------- */
+
+/* Warp::map and Warp::confidence (crates/chiaro-fusion/src/align.rs:84-131), the
+ * per-pixel warp lookups of synthesize (synth.rs:591-700), at n reference-raster
+ * points xy (2n floats, (x, y) interleaved). Every array is device memory of the
+ * context's device, warp->points and warp->confidence included (confidence may be
+ * NULL: every confidence is then 0, as for the reference's length mismatch).
+ * mapped (2n) receives the target point, NaN for None; confidence (n, may be NULL)
+ * the bilinear confidence. Bit-identical to the reference. */
+int chiaro_warp_sample_device(chiaro_depth_ctx *ctx, const chiaro_warp *warp, const float *xy, uint64_t n,
+                              float *mapped, float *confidence);
+
+/* DenseDepthMap::sample_nearest (depth.rs:152-159) at n reference-raster points xy
+ * (device memory, as are map's arrays and the outputs): node (may be NULL) receives
+ * the nearest node's index or -1 for None; depth / confidence / provenance (each may
+ * be NULL) the node's fields (NaN / 0 / 0 for None). */
+int chiaro_depth_sample_nearest_device(chiaro_depth_ctx *ctx, const chiaro_depth_map *map, const float *xy,
+                                       uint64_t n, double *depth, float *confidence, uint8_t *provenance,
+                                       int64_t *node);
+
 /* ---- global alignment ------------------------------------------------------------- */
 
 /* AlignInput (crates/chiaro-fusion/src/align.rs:246-257). */

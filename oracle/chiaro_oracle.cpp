@@ -3164,3 +3164,15 @@ extern "C" int oracle_align_module(const chiaro_align_input *reference, const ch
     *gain = photometric_gain_o(reference_luma.view(), target_luma.view(), warp.view()).value_or(1.0f);
     return emit(warp);
 }
+
+// Warp::confidence (align.rs:113-131) at one point.
+extern "C" float oracle_warp_confidence(const chiaro_warp *w, float x, float y) { return warp_confidence_o(*w, x, y); }
+
+// DenseDepthMap::sample_nearest (depth.rs:152-159): the node index, or -1 for None.
+extern "C" long oracle_sample_nearest(const chiaro_depth_map *map, float x, float y) {
+    if (x < 0.0f || y < 0.0f || map->step == 0) return -1;
+    const size_t column = sat_usize(std::round(x / (float)map->step));
+    const size_t row = sat_usize(std::round(y / (float)map->step));
+    if (!(column < map->columns && row < map->rows)) return -1;
+    return (long)(row * map->columns + column);
+}

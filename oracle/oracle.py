@@ -85,6 +85,8 @@ def lib():
             "oracle_align_module": (C.c_int, [P(abi.AlignInputC), P(abi.AlignInputC), C.c_int,
                                               P(abi.AlignOptionsC), P(WarpC), P(WarpC), P(C.c_float),
                                               P(abi.AlignmentReportC), C.c_char_p]),
+            "oracle_warp_confidence": (C.c_float, [P(WarpC), C.c_float, C.c_float]),
+            "oracle_sample_nearest": (C.c_long, [P(DepthMapC), C.c_float, C.c_float]),
             "oracle_match_patch": (C.c_int, [P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_float), C.c_size_t,
                                              C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
                                              P(C.c_float), P(C.c_float)]),
