@@ -229,3 +229,31 @@ def refine_resolution_warp(reference, target, base, width: int, height: int):
     assert st == 0, st
     return ResolutionWarp(Warp(WARP_STEP, columns, rows, points, confidence),
                           ResolutionAlignmentReport(*[float(v) for v in report]))
+
+
+def align_module(reference, target, options=None, seed=None):
+    """oracle_align_module (align.rs:281-519) on chiaro_b200's AlignInput types:
+    (warp points [n, 2], confidence [n], gain, chiaro_alignment_report)."""
+    from chiaro_b200.align import AlignOptions, align_input_c
+    F = C.POINTER(C.c_float)
+    options = options or AlignOptions()
+    ref_c, keep_r = align_input_c(reference)
+    tgt_c, keep_t = align_input_c(target)
+    step = options.grid_step
+    columns, rows = -(-reference.width // step) + 1, -(-reference.height // step) + 1
+    points = np.empty((columns * rows, 2), np.float32)
+    confidence = np.empty(columns * rows, np.float32)
+    out = WarpC(capacity=columns * rows, points=points.ctypes.data_as(F), confidence=confidence.ctypes.data_as(F))
+    seed_c, keep_s = None, None
+    if seed is not None:
+        keep_s = (np.ascontiguousarray(seed.points, np.float32), np.ascontiguousarray(seed.confidence, np.float32))
+        seed_c = WarpC(step=seed.step, columns=seed.columns, rows=seed.rows, points=keep_s[0].ctypes.data_as(F),
+                       confidence=keep_s[1].ctypes.data_as(F), capacity=seed.columns * seed.rows)
+    gain = C.c_float()
+    report = abi.AlignmentReportC()
+    opt = options.to_c()
+    st = lib().oracle_align_module(C.byref(ref_c), C.byref(tgt_c), int(reference.name == target.name), C.byref(opt),
+                                   C.byref(seed_c) if seed_c is not None else None, C.byref(out), C.byref(gain),
+                                   C.byref(report), None)
+    assert st == 0, st
+    return points, confidence, gain.value, report
