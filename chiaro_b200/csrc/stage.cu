@@ -2155,7 +2155,8 @@ int chiaro_align_module(chiaro_depth_ctx *ctx, const chiaro_align_input *referen
         reference->width > INT32_MAX / 2 || reference->height > INT32_MAX / 2 || reference->luma_width > INT32_MAX ||
         reference->luma_height > INT32_MAX || target->luma_width > INT32_MAX || target->luma_height > INT32_MAX ||
         options->patch > 4096 || options->coarse_radius > 4096 || options->grid_step > INT32_MAX ||
-        (seed && (!seed->points || seed->step == 0 || seed->columns == 0 || seed->rows == 0)))
+        (seed && (!seed->points || seed->step == 0 || seed->columns == 0 || seed->rows == 0 ||
+                  seed->step > INT32_MAX || seed->columns > INT32_MAX || seed->rows > INT32_MAX)))
         return CHIARO_ERR_ARGUMENT;
     try {
         CK(cudaSetDevice(ctx->device));
@@ -2175,7 +2176,8 @@ int chiaro_refine_resolution_warp(chiaro_depth_ctx *ctx, const float *reference,
                                   chiaro_warp *out, chiaro_resolution_report *report) {
     if (!ctx || !reference || !target || !base || !base->points || !out || !out->points || !report)
         return CHIARO_ERR_ARGUMENT;
-    if (base->step == 0 || base->columns == 0 || base->rows == 0 || reference_width > INT32_MAX ||
+    if (base->step == 0 || base->columns == 0 || base->rows == 0 || base->step > INT32_MAX ||
+        base->columns > INT32_MAX || base->rows > INT32_MAX || reference_width > INT32_MAX ||
         reference_height > INT32_MAX || target_width > INT32_MAX || target_height > INT32_MAX ||
         width > INT32_MAX / 2 || height > INT32_MAX / 2)
         return CHIARO_ERR_ARGUMENT;
