@@ -560,7 +560,11 @@ void chiaro_align_options_default(chiaro_align_options *options);
  * memory, step options->grid_step, capacity >= columns * rows; step, columns and
  * rows are set on return) receives the warp, gain the photometric gain. Returns
  * CHIARO_INVALID where the reference returns Err (no correlation in the
- * no-calibration search), with its message in chiaro_depth_last_error. */
+ * no-calibration search), with its message in chiaro_depth_last_error. A level's
+ * patch search keeps the window and its scores in shared memory: (patch^2 +
+ * (2 radius + 1)^2) * 4 bytes must fit 48 KiB (a patch up to 110 at the fine
+ * levels' radius 3; the default 32 with radius 12 takes 6.5 KiB), else
+ * CHIARO_ERR_ARGUMENT. */
 int chiaro_align_module(chiaro_depth_ctx *ctx, const chiaro_align_input *reference,
                         const chiaro_align_input *target, int32_t target_is_reference,
                         const chiaro_align_options *options, const chiaro_warp *seed,

@@ -113,3 +113,56 @@ def test_python_api_and_short_output(gpu_ctx):
     st = gpu_ctx.lib.chiaro_align_module(gpu_ctx.handle, C.byref(ref), C.byref(tgt), 0, C.byref(options), None,
                                          C.byref(out), C.byref(gain), C.byref(report))
     assert st == abi.ERR_CAPACITY and (out.step, out.columns, out.rows) == (32, 34, 26)
+
+
+def test_uncorrelated_module_is_the_references_error(gpu_ctx, oracle_lib):
+    """Without cameras a featureless tele target (twice the reference's focal length, so
+    the search slides it over the reference) gives the no-calibration search nothing to
+    correlate: align_module's Err (align.rs:610-617), as CHIARO_INVALID with the message."""
+    from chiaro_b200.align import AlignmentError
+    from chiaro_b200.image import Plane
+    sc = scenes.workload("small", seed=2)
+    ref, keep_r = align_input(sc, 0)
+    flat = np.full((sc.luminance[1].height, sc.luminance[1].width), 3.0, np.float32)
+    tgt, _ = align_input(sc, 1)
+    tgt.luminance = flat.ctypes.data_as(F)
+    ref.has_camera = tgt.has_camera = 0
+    tgt.nominal_focal_px = 2.0 * ref.nominal_focal_px
+    options = default_options()
+    columns, rows = -(-sc.width // 32) + 1, -(-sc.height // 32) + 1
+    points = np.empty(2 * columns * rows, np.float32)
+    out = abi.WarpC(capacity=columns * rows, points=points.ctypes.data_as(F))
+    gain, report = C.c_float(), abi.AlignmentReportC()
+    st = gpu_ctx.lib.chiaro_align_module(gpu_ctx.handle, C.byref(ref), C.byref(tgt), 0, C.byref(options), None,
+                                         C.byref(out), C.byref(gain), C.byref(report))
+    message = gpu_ctx.lib.chiaro_depth_last_error(gpu_ctx.handle).decode()
+    err = C.create_string_buffer(128)
+    st_o = oracle_lib.oracle_align_module(C.byref(ref), C.byref(tgt), 0, C.byref(options), None, C.byref(out),
+                                          C.byref(gain), C.byref(report), err)
+    assert st == st_o == abi.INVALID and message == err.value.decode() and "correlat" in message
+    inputs = sc.inputs()
+    inputs[0].camera = inputs[1].camera = None
+    inputs[0].nominal_focal_px, inputs[1].nominal_focal_px = ref.nominal_focal_px, 2.0 * ref.nominal_focal_px
+    inputs[1].luminance = Plane(inputs[1].luminance.width, inputs[1].luminance.height, flat)
+    with pytest.raises(AlignmentError):
+        align_module(inputs[0], inputs[1], context=gpu_ctx)
+
+
+def test_invalid_arguments_are_refused(gpu_ctx):
+    sc = scenes.workload("band", seed=3)
+    ref, keep_r = align_input(sc, 0)
+    tgt, keep_t = align_input(sc, 1)
+    points = np.empty(2 * 34 * 26, np.float32)
+    out = abi.WarpC(capacity=34 * 26, points=points.ctypes.data_as(F))
+    gain, report = C.c_float(), abi.AlignmentReportC()
+    big = default_options()
+    big.patch = 130  # at the finest level (520 px wide) a 130 x 130 window does not fit a CTA's shared memory
+    lib, h = gpu_ctx.lib, gpu_ctx.handle
+    assert lib.chiaro_align_module(h, C.byref(ref), C.byref(tgt), 0, C.byref(big), None, C.byref(out),
+                                   C.byref(gain), C.byref(report)) == abi.ERR_ARGUMENT
+    assert lib.chiaro_align_module(h, None, C.byref(tgt), 0, C.byref(big), None, C.byref(out), C.byref(gain),
+                                   C.byref(report)) == abi.ERR_ARGUMENT
+    zero = default_options()
+    zero.grid_step = 0
+    assert lib.chiaro_align_module(h, C.byref(ref), C.byref(tgt), 0, C.byref(zero), None, C.byref(out),
+                                   C.byref(gain), C.byref(report)) == abi.ERR_ARGUMENT
