@@ -378,6 +378,7 @@ int run_align(chiaro_depth_ctx *ctx, const chiaro_align_input &reference, const 
     using namespace align_host;
     constexpr double FAR_DEPTH = 1.0e8;
     cudaStream_t s = ctx->stream;
+    set_smem_limits();  // align_match_kernel's windows may exceed 48 KiB per CTA
     const int width = (int)reference.width, height = (int)reference.height;
     std::memset(&report, 0, sizeof(report));
     const int step = (int)o.grid_step;
@@ -533,8 +534,8 @@ int run_align(chiaro_depth_ctx *ctx, const chiaro_align_input &reference, const 
             if (nx > 0 && ny > 0) {
                 const int span = 2 * radius + 1;
                 const size_t per_warp = ((size_t)patch * patch + (size_t)span * span) * sizeof(float);
-                if (per_warp > 48 * 1024) return CHIARO_ERR_ARGUMENT;
-                const int warps = (int)std::min<size_t>(8, 48 * 1024 / per_warp);
+                if (per_warp > 200 * 1024) return CHIARO_ERR_ARGUMENT;  // the kernel's opted-in maximum
+                const int warps = (int)std::min<size_t>(8, 200 * 1024 / per_warp);
                 const size_t jobs = (size_t)nx * ny;
                 AlignMatch *d_matches = dbuf<AlignMatch>(ctx, "al.matches", jobs);
                 align_match_kernel<<<(unsigned)div_ceil(jobs, (size_t)warps), 32 * warps, warps * per_warp, s>>>(

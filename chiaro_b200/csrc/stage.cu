@@ -169,14 +169,21 @@ void download(chiaro_depth_ctx *ctx, T *dst, const T *src, size_t count) {
     CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
 }
 
+// Opt the kernels that need more than 48 KiB of dynamic shared memory in, once per
+// device (the attribute belongs to the current device's context).
 void set_smem_limits() {
-    static bool done = false;
-    if (done) return;
+    static std::mutex lock;
+    static std::vector<int> done_devices;
+    int device = 0;
+    CK(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> guard(lock);
+    if (std::find(done_devices.begin(), done_devices.end(), device) != done_devices.end()) return;
     CK(cudaFuncSetAttribute(cost_volume_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(direct_depth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(direct_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(target_decision_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    done = true;
+    CK(cudaFuncSetAttribute(align_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    done_devices.push_back(device);
 }
 
 // Per (node, target) geometry records of a step-spaced grid.

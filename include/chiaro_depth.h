@@ -562,7 +562,7 @@ void chiaro_align_options_default(chiaro_align_options *options);
  * CHIARO_INVALID where the reference returns Err (no correlation in the
  * no-calibration search), with its message in chiaro_depth_last_error. A level's
  * patch search keeps the window and its scores in shared memory: (patch^2 +
- * (2 radius + 1)^2) * 4 bytes must fit 48 KiB (a patch up to 110 at the fine
+ * (2 radius + 1)^2) * 4 bytes must fit 200 KiB (a patch up to 226 at the fine
  * levels' radius 3; the default 32 with radius 12 takes 6.5 KiB), else
  * CHIARO_ERR_ARGUMENT. */
 int chiaro_align_module(chiaro_depth_ctx *ctx, const chiaro_align_input *reference,

@@ -148,15 +148,29 @@ def test_uncorrelated_module_is_the_references_error(gpu_ctx, oracle_lib):
         align_module(inputs[0], inputs[1], context=gpu_ctx)
 
 
-def test_invalid_arguments_are_refused(gpu_ctx):
+def test_wide_windows_and_invalid_arguments(gpu_ctx, oracle_lib):
     sc = scenes.workload("band", seed=3)
     ref, keep_r = align_input(sc, 0)
     tgt, keep_t = align_input(sc, 1)
     points = np.empty(2 * 34 * 26, np.float32)
     out = abi.WarpC(capacity=34 * 26, points=points.ctypes.data_as(F))
     gain, report = C.c_float(), abi.AlignmentReportC()
+    wide = default_options()
+    wide.patch = 130  # 130 x 130 windows at the finest level (520 px wide): 67 KiB per warp, allowed
+    assert gpu_ctx.lib.chiaro_align_module(gpu_ctx.handle, C.byref(ref), C.byref(tgt), 0, C.byref(wide), None,
+                                           C.byref(out), C.byref(gain), C.byref(report)) == abi.OK
+    wide_points = points.copy()
+    st, po, co, go, ro, _ = oracle_align(oracle_lib, sc, 1, wide)
+    assert st == 0 and np.array_equal(wide_points.view(np.uint32), po.view(np.uint32))
+    # 240 x 240 windows (225 KiB per warp) exceed what a CTA may hold: they need a level at
+    # least 960 px wide (a patch is at most a quarter of its level), so 1000 x 1000 planes
+    rng = np.random.default_rng(0)
+    large = [rng.uniform(0, 7, (1000, 1000)).astype(np.float32) for _ in range(2)]
+    for inp, plane in zip((ref, tgt), large):
+        inp.luminance = plane.ctypes.data_as(F)
+        inp.luma_width = inp.luma_height = 1000
     big = default_options()
-    big.patch = 130  # at the finest level (520 px wide) a 130 x 130 window does not fit a CTA's shared memory
+    big.patch = 240
     lib, h = gpu_ctx.lib, gpu_ctx.handle
     assert lib.chiaro_align_module(h, C.byref(ref), C.byref(tgt), 0, C.byref(big), None, C.byref(out),
                                    C.byref(gain), C.byref(report)) == abi.ERR_ARGUMENT
