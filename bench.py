@@ -403,7 +403,20 @@ def resolution_warp(args, scene, ctx):
             result = refine_resolution_warp(ref, scene.luminance[t], scene.warps[t], scene.width, scene.height,
                                             context=ctx)
     ms = (time.perf_counter() - t0) * 1e3 / (steps * len(targets))
+    import torch
+    planes = [torch.from_numpy(p.data).cuda() for p in scene.luminance]
+    for t in targets:  # warm-up of the device-plane form
+        refine_resolution_warp(planes[scene.reference_index], planes[t], scene.warps[t], scene.width, scene.height,
+                               context=ctx)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for t in targets:
+            refine_resolution_warp(planes[scene.reference_index], planes[t], scene.warps[t], scene.width,
+                                   scene.height, context=ctx)
+    device_ms = (time.perf_counter() - t0) * 1e3 / (steps * len(targets))
+    del planes
     return {"api": "chiaro_b200.resolution.refine_resolution_warp (host planes and warps)",
+            "ms_per_target_device_planes": round(device_ms, 3),
             "plane": [ref.width, ref.height], "control_grid": [result.warp.columns, result.warp.rows],
             "ms_per_target": round(ms, 3), "targets": len(targets),
             "last_report": {k: round(v, 4) for k, v in vars(result.report).items()}}

@@ -641,6 +641,26 @@ struct Correction {
     float x, y;
 };
 
+// Up to nine values of a 3 x 3 neighbourhood, sorted in total order by insertion
+// (equal keys are equal bit patterns, so the order among them does not matter).
+struct Neighbours {
+    float v[9];
+    int n = 0;
+    void push(float x) { v[n++] = x; }
+    void sort() {
+        for (int i = 1; i < n; ++i) {
+            const float x = v[i];
+            int j = i - 1;
+            while (j >= 0 && total_less(x, v[j])) {
+                v[j + 1] = v[j];
+                --j;
+            }
+            v[j + 1] = x;
+        }
+    }
+    float median() const { return v[n / 2]; }
+};
+
 }  // namespace resolution_host
 
 // The device half (render, patch searches) and the host half (the control grid's
@@ -698,20 +718,20 @@ int run_resolution(chiaro_depth_ctx *ctx, const float *d_reference, int referenc
             bool refined = false;
             float qx = 0.0f, qy = 0.0f, local = 0.0f, median_x = 0.0f, median_y = 0.0f;
             if (measured[index].measured) {
-                std::vector<float> xs, ys;
+                Neighbours xs, ys;
                 for (int nr = std::max(row - 1, 0); nr <= std::min(row + 1, rows - 1); ++nr)
                     for (int nc = std::max(column - 1, 0); nc <= std::min(column + 1, columns - 1); ++nc) {
                         const ResolutionNode &m = measured[(size_t)nr * columns + nc];
                         if (m.measured) {
-                            xs.push_back(m.shift_x);
-                            ys.push_back(m.shift_y);
+                            xs.push(m.shift_x);
+                            ys.push(m.shift_y);
                         }
                     }
-                if (xs.size() >= 3) {
-                    std::sort(xs.begin(), xs.end(), total_less);
-                    std::sort(ys.begin(), ys.end(), total_less);
-                    median_x = xs[xs.size() / 2];
-                    median_y = ys[ys.size() / 2];
+                if (xs.n >= 3) {
+                    xs.sort();
+                    ys.sort();
+                    median_x = xs.median();
+                    median_y = ys.median();
                     const ResolutionNode &c = measured[index];
                     if (!(std::hypot(c.shift_x - median_x, c.shift_y - median_y) > 1.5f) &&
                         warp_map(hbase, rx + median_x, ry + median_y, qx, qy)) {
@@ -745,33 +765,32 @@ int run_resolution(chiaro_depth_ctx *ctx, const float *d_reference, int referenc
             for (int column = 0; column < columns; ++column) {
                 const size_t index = (size_t)row * columns + column;
                 if (grid_snapshot[index].some) continue;
-                std::vector<float> xs, ys;
+                Neighbours sx, sy;
                 float neighbour_confidence = 0.0f;
                 for (int nr = std::max(row - 1, 0); nr <= std::min(row + 1, rows - 1); ++nr)
                     for (int nc = std::max(column - 1, 0); nc <= std::min(column + 1, columns - 1); ++nc) {
                         const size_t neighbour = (size_t)nr * columns + nc;
                         if (grid_snapshot[neighbour].some) {
-                            xs.push_back(grid_snapshot[neighbour].x);
-                            ys.push_back(grid_snapshot[neighbour].y);
+                            sx.push(grid_snapshot[neighbour].x);
+                            sy.push(grid_snapshot[neighbour].y);
                             neighbour_confidence += confidence_snapshot[neighbour];
                         }
                     }
-                if (xs.size() < 3) continue;
-                std::vector<float> sx = xs, sy = ys;
-                std::sort(sx.begin(), sx.end(), total_less);
-                std::sort(sy.begin(), sy.end(), total_less);
-                const float cx = sx[sx.size() / 2], cy = sy[sy.size() / 2];
+                if (sx.n < 3) continue;
+                sx.sort();
+                sy.sort();
+                const float cx = sx.median(), cy = sy.median();
                 // coherence over the sorted lists, pairing the k-th sorted x with the k-th sorted y
                 bool coherent = true;
-                for (size_t k = 0; k < sx.size() && coherent; ++k)
-                    coherent = std::hypot(sx[k] - cx, sy[k] - cy) <= 1.5f;
+                for (int k = 0; k < sx.n && coherent; ++k)
+                    coherent = std::hypot(sx.v[k] - cx, sy.v[k] - cy) <= 1.5f;
                 if (!coherent) continue;
                 const float rx = (float)(column * RES_WARP_STEP), ry = (float)(row * RES_WARP_STEP);
                 float qx, qy;
                 if (warp_map(hbase, rx + cx, ry + cy, qx, qy)) {
                     points[2 * index] = qx;
                     points[2 * index + 1] = qy;
-                    confidence[index] = 0.45f * neighbour_confidence / (float)xs.size();
+                    confidence[index] = 0.45f * neighbour_confidence / (float)sx.n;
                     grid[index] = Correction{true, cx, cy};
                 }
             }
@@ -2146,6 +2165,26 @@ int chiaro_depth_sample_nearest_device(chiaro_depth_ctx *ctx, const chiaro_depth
         return fail(ctx, e);
     }
     return CHIARO_OK;
+}
+
+int chiaro_refine_resolution_warp_device(chiaro_depth_ctx *ctx, const float *reference, uint64_t reference_width,
+                                         uint64_t reference_height, const float *target, uint64_t target_width,
+                                         uint64_t target_height, const chiaro_warp *base, uint64_t width,
+                                         uint64_t height, chiaro_warp *out, chiaro_resolution_report *report) {
+    if (!ctx || !reference || !target || !base || !base->points || !out || !out->points || !report)
+        return CHIARO_ERR_ARGUMENT;
+    if (base->step == 0 || base->columns == 0 || base->rows == 0 || base->step > INT32_MAX ||
+        base->columns > INT32_MAX || base->rows > INT32_MAX || reference_width > INT32_MAX ||
+        reference_height > INT32_MAX || target_width > INT32_MAX || target_height > INT32_MAX ||
+        width > INT32_MAX / 2 || height > INT32_MAX / 2)
+        return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        return run_resolution(ctx, reference, (int)reference_width, (int)reference_height, target, (int)target_width,
+                              (int)target_height, *base, (int)width, (int)height, *out, *report);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
 }
 
 void chiaro_align_options_default(chiaro_align_options *options) {

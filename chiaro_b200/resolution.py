@@ -48,9 +48,13 @@ def warp_c(warp: Warp) -> abi.WarpC:
 def refine_resolution_warp(reference: Plane, target: Plane, base: Warp, width: int, height: int,
                            context=None) -> ResolutionWarp:
     """The reference's refine_resolution_warp: ``reference`` and ``target`` are half-resolution
-    luminance planes, ``base`` the target's warp from the ``width`` x ``height`` reference raster."""
+    luminance planes, ``base`` the target's warp from the ``width`` x ``height`` reference raster.
+    A plane may also be given as a CUDA tensor (row-major f32 on the context's device); then
+    both must be, and they are read in place."""
     from .runtime import default_context
     ctx = context or default_context()
+    if not isinstance(reference, Plane):
+        return _refine_device(reference, target, base, width, height, ctx)
     columns, rows = -(-width // WARP_STEP) + 1, -(-height // WARP_STEP) + 1
     points = np.empty((columns * rows, 2), np.float32)
     confidence = np.empty(columns * rows, np.float32)
@@ -68,3 +72,21 @@ def refine_resolution_warp(reference: Plane, target: Plane, base: Warp, width: i
                           ResolutionAlignmentReport(report.verified_fraction, report.supported_fraction,
                                                     report.median_correction_px, report.mean_confidence))
 
+
+
+def _refine_device(reference, target, base: Warp, width: int, height: int, ctx) -> ResolutionWarp:
+    """chiaro_refine_resolution_warp_device on two CUDA tensors of shape (height, width)."""
+    columns, rows = -(-width // WARP_STEP) + 1, -(-height // WARP_STEP) + 1
+    points = np.empty((columns * rows, 2), np.float32)
+    confidence = np.empty(columns * rows, np.float32)
+    out = abi.WarpC(capacity=columns * rows, points=points.ctypes.data_as(C.POINTER(C.c_float)),
+                    confidence=confidence.ctypes.data_as(C.POINTER(C.c_float)))
+    report = abi.ResolutionReportC()
+    ref, tgt = reference.contiguous(), target.contiguous()
+    base_c = warp_c(base)
+    ctx.check(ctx.lib.chiaro_refine_resolution_warp_device(
+        ctx.handle, ref.data_ptr(), ref.shape[1], ref.shape[0], tgt.data_ptr(), tgt.shape[1], tgt.shape[0],
+        C.byref(base_c), width, height, C.byref(out), C.byref(report)))
+    return ResolutionWarp(Warp(WARP_STEP, columns, rows, points, confidence),
+                          ResolutionAlignmentReport(report.verified_fraction, report.supported_fraction,
+                                                    report.median_correction_px, report.mean_confidence))

@@ -55,6 +55,9 @@ SIGNATURES = {
     "chiaro_align_module": (C.c_int, [C.c_void_p, P(abi.AlignInputC), P(abi.AlignInputC), C.c_int32,
                                       P(abi.AlignOptionsC), P(abi.WarpC), P(abi.WarpC), P(C.c_float),
                                       P(abi.AlignmentReportC)]),
+    "chiaro_refine_resolution_warp_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p,
+                                                       C.c_uint64, C.c_uint64, P(abi.WarpC), C.c_uint64,
+                                                       C.c_uint64, P(abi.WarpC), P(abi.ResolutionReportC)]),
     "chiaro_refine_resolution_warp": (C.c_int, [C.c_void_p, P(C.c_float), C.c_uint64, C.c_uint64, P(C.c_float),
                                                 C.c_uint64, C.c_uint64, P(abi.WarpC), C.c_uint64, C.c_uint64,
                                                 P(abi.WarpC), P(abi.ResolutionReportC)]),

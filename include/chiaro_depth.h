@@ -597,6 +597,14 @@ int chiaro_refine_resolution_warp(chiaro_depth_ctx *ctx, const float *reference,
                                   uint64_t reference_height, const float *target, uint64_t target_width,
                                   uint64_t target_height, const chiaro_warp *base, uint64_t width,
                                   uint64_t height, chiaro_warp *out, chiaro_resolution_report *report);
+/* The same with reference and target in device memory of the context's device (the
+ * warps and the report stay host memory): a pipeline that keeps the modules' planes
+ * in HBM refines every target without uploading them. */
+int chiaro_refine_resolution_warp_device(chiaro_depth_ctx *ctx, const float *reference,
+                                         uint64_t reference_width, uint64_t reference_height,
+                                         const float *target, uint64_t target_width,
+                                         uint64_t target_height, const chiaro_warp *base, uint64_t width,
+                                         uint64_t height, chiaro_warp *out, chiaro_resolution_report *report);
 
 /* ---- allocation-free operator --------------------------------------------- */
 

@@ -86,3 +86,13 @@ def test_short_output_is_refused_with_the_grid_shape(gpu_ctx):
         gpu_ctx.handle, ref.ctypes.data_as(C.POINTER(C.c_float)), 256, 192, tgt.ctypes.data_as(C.POINTER(C.c_float)),
         256, 192, C.byref(base_c), 512, 384, C.byref(out), C.byref(report))
     assert st == abi.ERR_CAPACITY and (out.step, out.columns, out.rows) == (32, 17, 13)
+
+
+def test_device_planes_give_the_same_result(gpu_ctx):
+    import torch
+    sc = scenes.workload("small", seed=1)
+    ref, tgt = sc.luminance[sc.reference_index], sc.luminance[1]
+    host = refine_resolution_warp(ref, tgt, sc.warps[1], sc.width, sc.height, context=gpu_ctx)
+    device = refine_resolution_warp(torch.from_numpy(ref.data).cuda(), torch.from_numpy(tgt.data).cuda(),
+                                    sc.warps[1], sc.width, sc.height, context=gpu_ctx)
+    _same(device, host)
