@@ -1,7 +1,7 @@
 // align.cuh — align_module_seeded (crates/chiaro-fusion/src/align.rs:281-519): the device
-// half of the global alignment. The host (stage.cu) builds the pyramids' shapes, the
-// RANSAC samples and fits, the final warp and the report; these kernels carry the
-// per-pixel and per-patch work.
+// half of the global alignment. The host (align_run.cuh) builds the pyramids' shapes,
+// the RANSAC samples, the refit, the final warp and the report; these kernels carry the
+// per-pixel, per-patch and per-candidate work.
 //
 // * align_downsample_kernel: Plane::downsample (image.rs:469-483), a thread per pixel.
 // * align_initial_grid_kernel: Warp::from_fn on the 8 px grid of the calibrated mapping
@@ -12,6 +12,9 @@
 //   rendered_covered (align.rs:551-559) and match_patch (image.rs:531-640) with the
 //   window's statistics in the reference's order by lane 0 and one search shift per
 //   lane, the last maximum in total order and the parabolic refinement.
+// * align_fit_kernel: the 300 RANSAC candidates (align.rs:640-659), a thread per
+//   candidate: fit_homography_least_squares (align.rs:702-760) and solve_linear
+//   (align.rs:765-793) on its four pairs, in f64 code shared with the host's refit.
 // * align_inlier_kernel: the RANSAC inlier counts (align.rs:660-671) of every
 //   candidate homography at once, a thread per (candidate, pair).
 #pragma once
@@ -33,6 +36,118 @@ CH_HD bool apply_homography(const Hom &h, double px, double py, double &qx, doub
     qx = v0 / v2;
     qy = v1 / v2;
     return true;
+}
+
+CH_HD Hom hom_identity() { return Hom{{1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0}}; }
+
+CH_HD Hom hom_mul(const Hom &a, const Hom &b) {  // math.rs:48-56
+    Hom out;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            out.m[3 * i + j] = a.m[3 * i] * b.m[j] + a.m[3 * i + 1] * b.m[3 + j] + a.m[3 * i + 2] * b.m[6 + j];
+    return out;
+}
+
+CH_HD int64_t total_key_f64(double v) {  // order of f64::total_cmp
+    int64_t bits;
+    memcpy(&bits, &v, sizeof bits);
+    return bits ^ (int64_t)((uint64_t)(bits >> 63) >> 1);
+}
+
+// solve_linear (align.rs:765-793)
+CH_HD bool solve_linear8(double a[8][8], double b[8], double x[8]) {
+    for (int column = 0; column < 8; ++column) {
+        int pivot = column;  // the last maximum of |a[i][column]| in total order
+        for (int i = column + 1; i < 8; ++i)
+            if (!(total_key_f64(fabs(a[i][column])) < total_key_f64(fabs(a[pivot][column])))) pivot = i;
+        if (fabs(a[pivot][column]) < 1e-12) return false;
+        for (int k = 0; k < 8; ++k) {
+            const double tmp = a[column][k];
+            a[column][k] = a[pivot][k];
+            a[pivot][k] = tmp;
+        }
+        const double tb = b[column];
+        b[column] = b[pivot];
+        b[pivot] = tb;
+        double pivot_row[8];
+        for (int k = 0; k < 8; ++k) pivot_row[k] = a[column][k];
+        for (int row = column + 1; row < 8; ++row) {
+            const double factor = a[row][column] / pivot_row[column];
+            for (int k = column; k < 8; ++k) a[row][k] -= factor * pivot_row[k];
+            b[row] -= factor * b[column];
+        }
+    }
+    for (int row = 7; row >= 0; --row) {
+        double sum = b[row];
+        for (int k = row + 1; k < 8; ++k) sum -= a[row][k] * x[k];
+        x[row] = sum / a[row][row];
+    }
+    return true;
+}
+
+// fit_homography_least_squares (align.rs:702-760) over pairs[idx[0..n)] (idx NULL: 0..n),
+// pairs as (ax, ay, bx, by) with their scores; false for None.
+CH_HD bool fit_homography(const double4 *pairs, const float *scores, const int *idx, int n, Hom &h) {
+    if (n < 4) return false;
+    const double count = (double)n;
+    double sx = -0.0, sy = -0.0, tx = -0.0, ty = -0.0;  // f64 Sum
+    for (int k = 0; k < n; ++k) sx += pairs[idx ? idx[k] : k].x;
+    for (int k = 0; k < n; ++k) sy += pairs[idx ? idx[k] : k].y;
+    for (int k = 0; k < n; ++k) tx += pairs[idx ? idx[k] : k].z;
+    for (int k = 0; k < n; ++k) ty += pairs[idx ? idx[k] : k].w;
+    const double ax = sx / count, ay = sy / count, bx = tx / count, by = ty / count;
+    double da = -0.0, db = -0.0;
+    for (int k = 0; k < n; ++k) {
+        const double4 p = pairs[idx ? idx[k] : k];
+        da += sqrt((p.x - ax) * (p.x - ax) + (p.y - ay) * (p.y - ay));
+    }
+    for (int k = 0; k < n; ++k) {
+        const double4 p = pairs[idx ? idx[k] : k];
+        db += sqrt((p.z - bx) * (p.z - bx) + (p.w - by) * (p.w - by));
+    }
+    const double sa = fmax(da / count, 1e-9), sb = fmax(db / count, 1e-9);
+    double ata[8][8], atb[8];
+    for (int i = 0; i < 8; ++i) {
+        atb[i] = 0.0;
+        for (int j = 0; j < 8; ++j) ata[i][j] = 0.0;
+    }
+    for (int k = 0; k < n; ++k) {
+        const int i_ = idx ? idx[k] : k;
+        const double4 p = pairs[i_];
+        const double w = fmax((double)scores[i_], 0.05);
+        const double x = (p.x - ax) / sa, y = (p.y - ay) / sa, u = (p.z - bx) / sb, v = (p.w - by) / sb;
+        const double rows[2][8] = {{x, y, 1.0, 0.0, 0.0, 0.0, -u * x, -u * y},
+                                   {0.0, 0.0, 0.0, x, y, 1.0, -v * x, -v * y}};
+        const double rhs[2] = {u, v};
+        for (int r = 0; r < 2; ++r)
+            for (int i = 0; i < 8; ++i) {
+                atb[i] += w * rows[r][i] * rhs[r];
+                for (int j = 0; j < 8; ++j) ata[i][j] += w * rows[r][i] * rows[r][j];
+            }
+    }
+    double s[8];
+    if (!solve_linear8(ata, atb, s)) return false;
+    const Hom normalized{{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], 1.0}};
+    const Hom t_a{{1.0 / sa, 0.0, -ax / sa, 0.0, 1.0 / sa, -ay / sa, 0.0, 0.0, 1.0}};
+    const Hom t_b_inv{{sb, 0.0, bx, 0.0, sb, by, 0.0, 0.0, 1.0}};
+    h = hom_mul(hom_mul(t_b_inv, normalized), t_a);
+    const double scale = h.m[8];
+    if (fabs(scale) < 1e-12 || !isfinite(scale)) return false;
+    for (int k = 0; k < 9; ++k) h.m[k] = h.m[k] / scale;
+    return true;
+}
+
+// The RANSAC candidates (align.rs:640-659): candidate k fits samples[k]'s four pairs.
+__global__ void align_fit_kernel(const double4 *__restrict__ pairs, const float *__restrict__ scores,
+                                 const int4 *__restrict__ samples, int count, Hom *__restrict__ candidates,
+                                 int *__restrict__ valid) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int4 s = samples[k];
+    const int idx[4] = {s.x, s.y, s.z, s.w};
+    Hom h = hom_identity();
+    valid[k] = fit_homography(pairs, scores, idx, 4, h) ? 1 : 0;
+    candidates[k] = h;
 }
 
 __global__ void align_downsample_kernel(const float *__restrict__ in, int width, int height, float *__restrict__ out,

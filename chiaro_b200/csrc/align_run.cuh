@@ -110,97 +110,11 @@ bool match_patch(const HostPlane &reference, const HostPlane &target, int rx, in
     return true;
 }
 
-Hom identity() { return Hom{{1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0}}; }
-
-Hom mat_mul(const Hom &a, const Hom &b) {  // math.rs:48-56
-    Hom out;
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-            out.m[3 * i + j] = a.m[3 * i] * b.m[j] + a.m[3 * i + 1] * b.m[3 + j] + a.m[3 * i + 2] * b.m[6 + j];
-    return out;
-}
-
-int64_t total_key_d(double v) {  // order of f64::total_cmp
-    int64_t bits;
-    std::memcpy(&bits, &v, sizeof bits);
-    return bits ^ (int64_t)((uint64_t)(bits >> 63) >> 1);
-}
-
-// solve_linear (align.rs:765-793)
-bool solve_linear(double a[8][8], double b[8], double x[8]) {
-    for (int column = 0; column < 8; ++column) {
-        int pivot = column;  // the last maximum of |a[i][column]| in total order
-        for (int i = column + 1; i < 8; ++i)
-            if (!(total_key_d(std::fabs(a[i][column])) < total_key_d(std::fabs(a[pivot][column])))) pivot = i;
-        if (std::fabs(a[pivot][column]) < 1e-12) return false;
-        for (int k = 0; k < 8; ++k) std::swap(a[column][k], a[pivot][k]);
-        std::swap(b[column], b[pivot]);
-        double pivot_row[8];
-        std::copy(a[column], a[column] + 8, pivot_row);
-        for (int row = column + 1; row < 8; ++row) {
-            const double factor = a[row][column] / pivot_row[column];
-            for (int k = column; k < 8; ++k) a[row][k] -= factor * pivot_row[k];
-            b[row] -= factor * b[column];
-        }
-    }
-    for (int row = 7; row >= 0; --row) {
-        double sum = b[row];
-        for (int k = row + 1; k < 8; ++k) sum -= a[row][k] * x[k];
-        x[row] = sum / a[row][row];
-    }
-    return true;
-}
-
-struct Pair {
-    double ax, ay, bx, by;
-    float score;
-};
-
-// fit_homography_least_squares (align.rs:702-760)
-bool fit_least_squares(const std::vector<Pair> &pairs, Hom &h) {
-    if (pairs.size() < 4) return false;
-    const double n = (double)pairs.size();
-    auto mean = [&](auto f) {
-        double s = -0.0;  // f64 Sum
-        for (const Pair &p : pairs) s += f(p);
-        return s / n;
-    };
-    const double ax = mean([](const Pair &p) { return p.ax; }), ay = mean([](const Pair &p) { return p.ay; });
-    const double bx = mean([](const Pair &p) { return p.bx; }), by = mean([](const Pair &p) { return p.by; });
-    const double sa = std::fmax(
-        mean([&](const Pair &p) { return std::sqrt((p.ax - ax) * (p.ax - ax) + (p.ay - ay) * (p.ay - ay)); }), 1e-9);
-    const double sb = std::fmax(
-        mean([&](const Pair &p) { return std::sqrt((p.bx - bx) * (p.bx - bx) + (p.by - by) * (p.by - by)); }), 1e-9);
-    double ata[8][8] = {}, atb[8] = {};
-    for (const Pair &p : pairs) {
-        const double w = std::fmax((double)p.score, 0.05);
-        const double x = (p.ax - ax) / sa, y = (p.ay - ay) / sa, u = (p.bx - bx) / sb, v = (p.by - by) / sb;
-        const double rows[2][8] = {{x, y, 1.0, 0.0, 0.0, 0.0, -u * x, -u * y},
-                                   {0.0, 0.0, 0.0, x, y, 1.0, -v * x, -v * y}};
-        const double rhs[2] = {u, v};
-        for (int r = 0; r < 2; ++r)
-            for (int i = 0; i < 8; ++i) {
-                atb[i] += w * rows[r][i] * rhs[r];
-                for (int j = 0; j < 8; ++j) ata[i][j] += w * rows[r][i] * rows[r][j];
-            }
-    }
-    double s[8];
-    if (!solve_linear(ata, atb, s)) return false;
-    const Hom normalized{{s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], 1.0}};
-    const Hom t_a{{1.0 / sa, 0.0, -ax / sa, 0.0, 1.0 / sa, -ay / sa, 0.0, 0.0, 1.0}};
-    const Hom t_b_inv{{sb, 0.0, bx, 0.0, sb, by, 0.0, 0.0, 1.0}};
-    h = mat_mul(mat_mul(t_b_inv, normalized), t_a);
-    const double scale = h.m[8];
-    if (std::fabs(scale) < 1e-12 || !std::isfinite(scale)) return false;
-    for (double &v : h.m) v = v / scale;
-    return true;
-}
-
-double residual(const Hom &h, const Pair &p, bool &some) {
+double residual(const Hom &h, const double4 &p, bool &some) {
     double qx = 0.0, qy = 0.0;
-    some = apply_homography(h, p.ax, p.ay, qx, qy);
+    some = apply_homography(h, p.x, p.y, qx, qy);
     if (!some) return 0.0;
-    return std::sqrt((qx - p.bx) * (qx - p.bx) + (qy - p.by) * (qy - p.by));
+    return std::sqrt((qx - p.z) * (qx - p.z) + (qy - p.w) * (qy - p.w));
 }
 
 struct Fit {
@@ -209,10 +123,11 @@ struct Fit {
     std::vector<float> residuals;
 };
 
-// fit_homography_ransac (align.rs:631-700): the 300 samples and fits on the host (the
-// sample sequence does not depend on the counts), their inlier counts on the device,
-// the refit and residuals on the host.
-bool fit_ransac(chiaro_depth_ctx *ctx, const std::vector<Pair> &pairs, float threshold, Fit &fit) {
+// fit_homography_ransac (align.rs:631-700): the 300 four-pair samples from the LCG on the
+// host (the sequence does not depend on the fits), their fits and inlier counts on the
+// device, the refit on the best candidate's inliers and the residuals on the host.
+bool fit_ransac(chiaro_depth_ctx *ctx, const std::vector<double4> &pairs, const std::vector<float> &scores,
+                float threshold, Fit &fit) {
     if (pairs.size() < 6) return false;
     constexpr int ITERATIONS = 300;
     uint64_t state = 0x9E3779B97F4A7C15ull ^ (uint64_t)pairs.size();
@@ -220,13 +135,12 @@ bool fit_ransac(chiaro_depth_ctx *ctx, const std::vector<Pair> &pairs, float thr
         state = state * 6364136223846793005ull + 1442695040888963407ull;
         return (size_t)(state >> 33) % n;
     };
-    std::vector<Hom> candidates(ITERATIONS, identity());
-    std::vector<uint8_t> valid(ITERATIONS, 0);
+    std::vector<int4> samples(ITERATIONS);
     for (int it = 0; it < ITERATIONS; ++it) {
-        size_t sample[4] = {0, 0, 0, 0};
+        int sample[4] = {0, 0, 0, 0};
         for (int slot = 0; slot < 4; ++slot)
             for (;;) {
-                const size_t candidate = next(pairs.size());
+                const int candidate = (int)next(pairs.size());
                 bool taken = false;
                 for (int k = 0; k < slot; ++k) taken = taken || sample[k] == candidate;
                 if (!taken) {
@@ -234,26 +148,32 @@ bool fit_ransac(chiaro_depth_ctx *ctx, const std::vector<Pair> &pairs, float thr
                     break;
                 }
             }
-        std::vector<Pair> subset;
-        for (size_t i : sample) subset.push_back(pairs[i]);
-        valid[it] = fit_least_squares(subset, candidates[it]);
+        samples[it] = make_int4(sample[0], sample[1], sample[2], sample[3]);
     }
     cudaStream_t s = ctx->stream;
-    std::vector<double4> packed(pairs.size());
-    for (size_t i = 0; i < pairs.size(); ++i)
-        packed[i] = make_double4(pairs[i].ax, pairs[i].ay, pairs[i].bx, pairs[i].by);
     double4 *d_pairs = dbuf<double4>(ctx, "al.pairs", pairs.size());
+    float *d_scores = dbuf<float>(ctx, "al.scores", pairs.size());
+    int4 *d_samples = dbuf<int4>(ctx, "al.samples", ITERATIONS);
     Hom *d_candidates = dbuf<Hom>(ctx, "al.candidates", ITERATIONS);
+    int *d_valid = dbuf<int>(ctx, "al.valid", ITERATIONS);
     unsigned *d_counts = dbuf<unsigned>(ctx, "al.counts", ITERATIONS);
-    upload(ctx, d_pairs, packed.data(), pairs.size());
-    upload(ctx, d_candidates, candidates.data(), ITERATIONS);
+    upload(ctx, d_pairs, pairs.data(), pairs.size());
+    upload(ctx, d_scores, scores.data(), scores.size());
+    upload(ctx, d_samples, samples.data(), ITERATIONS);
+    align_fit_kernel<<<(ITERATIONS + 63) / 64, 64, 0, s>>>(d_pairs, d_scores, d_samples, ITERATIONS, d_candidates,
+                                                           d_valid);
+    CK(cudaGetLastError());
     CK(cudaMemsetAsync(d_counts, 0, ITERATIONS * sizeof(unsigned), s));
     const unsigned blocks = (unsigned)std::min<size_t>(div_ceil(pairs.size(), 256), 64);
     align_inlier_kernel<<<dim3(blocks, ITERATIONS), 256, 0, s>>>(d_pairs, (int)pairs.size(), d_candidates,
                                                                   (double)threshold, d_counts);
     CK(cudaGetLastError());
     std::vector<unsigned> counts(ITERATIONS);
+    std::vector<int> valid(ITERATIONS);
+    std::vector<Hom> candidates(ITERATIONS);
     CK(cudaMemcpyAsync(counts.data(), d_counts, ITERATIONS * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(valid.data(), d_valid, ITERATIONS * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(candidates.data(), d_candidates, ITERATIONS * sizeof(Hom), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     int best = -1;
     unsigned best_count = 0;  // the first candidate with the most inliers
@@ -263,16 +183,16 @@ bool fit_ransac(chiaro_depth_ctx *ctx, const std::vector<Pair> &pairs, float thr
             best_count = counts[it];
         }
     if (best < 0 || best_count < 6) return false;
-    std::vector<Pair> inlier_pairs;
-    for (const Pair &p : pairs) {
+    std::vector<int> inliers;
+    for (size_t i = 0; i < pairs.size(); ++i) {
         bool some;
-        const double r = residual(candidates[best], p, some);
-        if (some && r <= (double)threshold) inlier_pairs.push_back(p);
+        const double r = residual(candidates[best], pairs[i], some);
+        if (some && r <= (double)threshold) inliers.push_back((int)i);
     }
-    if (!fit_least_squares(inlier_pairs, fit.h)) return false;
+    if (!fit_homography(pairs.data(), scores.data(), inliers.data(), (int)inliers.size(), fit.h)) return false;
     fit.inliers = 0;
     fit.residuals.clear();
-    for (const Pair &p : pairs) {
+    for (const double4 &p : pairs) {
         bool some;
         const float r = (float)residual(fit.h, p, some);
         if (some && r <= threshold) {
@@ -469,7 +389,7 @@ int run_align(chiaro_depth_ctx *ctx, const chiaro_align_input &reference, const 
         return true;
     };
     // Step 2: coarse-to-fine refinement of the reference-space homography (align.rs:347-455)
-    Hom correction = identity();
+    Hom correction = hom_identity();
     std::vector<float> finest_residuals;
     if (o.refine) {
         const auto reference_shapes = pyramid_shapes(reference_plane.width, reference_plane.height, 96);
@@ -530,7 +450,8 @@ int run_align(chiaro_depth_ctx *ctx, const chiaro_align_input &reference, const 
             const int stride = patch / 2;
             const int nx = rs.width >= patch + 2 * radius ? (rs.width - patch - 2 * radius) / stride + 1 : 0;
             const int ny = rs.height >= patch + 2 * radius ? (rs.height - patch - 2 * radius) / stride + 1 : 0;
-            std::vector<Pair> pairs;
+            std::vector<double4> pairs;
+            std::vector<float> pair_scores;
             if (nx > 0 && ny > 0) {
                 const int span = 2 * radius + 1;
                 const size_t per_warp = ((size_t)patch * patch + (size_t)span * span) * sizeof(float);
@@ -550,16 +471,17 @@ int run_align(chiaro_depth_ctx *ctx, const chiaro_align_input &reference, const 
                 for (size_t j = 0; j < jobs; ++j) {  // the reference's scan order: rows, then columns
                     if (!matches[j].found) continue;
                     const int x = radius + (int)(j % nx) * stride, y = radius + (int)(j / nx) * stride;
-                    pairs.push_back(Pair{convert((float)x + half), convert((float)y + half),
-                                         convert((float)x + half + matches[j].shift_x),
-                                         convert((float)y + half + matches[j].shift_y), matches[j].score});
+                    pairs.push_back(make_double4(convert((float)x + half), convert((float)y + half),
+                                                 convert((float)x + half + matches[j].shift_x),
+                                                 convert((float)y + half + matches[j].shift_y)));
+                    pair_scores.push_back(matches[j].score);
                 }
             }
             const float threshold = std::fmax(o.inlier_px * (float)scale * 2.0f, o.inlier_px);
             chiaro_align_level &lr = report.levels[report.n_levels++];
             Fit fit;
-            if (fit_ransac(ctx, pairs, threshold, fit)) {
-                correction = mat_mul(correction, fit.h);
+            if (fit_ransac(ctx, pairs, pair_scores, threshold, fit)) {
+                correction = hom_mul(correction, fit.h);
                 lr = chiaro_align_level{(uint64_t)scale * 2, pairs.size(), fit.inliers,
                                         fit.residuals[fit.residuals.size() / 2]};
                 if (level == 0) {
