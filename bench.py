@@ -288,6 +288,7 @@ def run_ours(args, rank, world, local):
     d2h = M * (8 + 4 + 1) + targets * M * (8 + 4)
     e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
 
+    graph = stage_graph(args, ctx, torch, stream, flush, step, [out_depth, out_conf, out_prov] + out_warps)
     finest = finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap)
     resolution = resolution_warp(args, scene, ctx)
     alignment = global_alignment(args, scene, ctx)
@@ -322,6 +323,7 @@ def run_ours(args, rank, world, local):
                      "traffic": sgm_traffic() if args.workload == "five_view" else None,
                      "traffic_source": "profiles/sgm_five_view_dram.md (ncu dram__bytes_read + write, one call)",
                      "peak_source": peaks["source"], "algorithmic_bytes": work["sgm_bytes"]},
+        "stage_graph": graph,
         "finest_coarse_grid": finest,
         "resolution_warp": resolution,
         "global_alignment": alignment,
@@ -481,6 +483,50 @@ def finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined
             "sgm_cells_per_step": work["cells"], "ms_per_step": round(ms, 3),
             "gcells_s": round(work["cells"] / (ms / 1e3) / 1e9, 3),
             "stage_ms": {k: round(statistics.median(s[k] for s in stages), 4) for k in stages[0]}}
+
+
+def stage_graph(args, ctx, torch, stream, flush, step, outputs):
+    """The whole stage replayed from its CUDA graph (chiaro_depth_set_stage_graph): the first
+    call launches, the second captures, the rest replay. The replay's outputs must equal the
+    launched stage's bit for bit before it is timed, with the same flush and events as the
+    main leg."""
+    lib = ctx.lib
+
+    def snapshot():
+        return [t.clone() for t in outputs]
+
+    step()
+    plain = snapshot()
+    ctx.check(lib.chiaro_depth_set_stage_graph(ctx.handle, 1))
+    try:
+        states = []
+        for _ in range(3):
+            for t in outputs:
+                t.zero_()
+            step()
+            states.append(lib.chiaro_depth_stage_graph_state(ctx.handle))
+        torch.cuda.synchronize()
+        identical = all(torch.equal(a.view(torch.uint8), b.view(torch.uint8)) for a, b in zip(plain, snapshot()))
+        if not identical or states != [0, 1, 2]:
+            return {"error": f"replay differs from the launched stage (states {states})"}
+        total = 0.0
+        steps = max(1, args.steps)
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            step()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        replayed = lib.chiaro_depth_stage_graph_state(ctx.handle) == 2
+    finally:
+        ctx.check(lib.chiaro_depth_set_stage_graph(ctx.handle, 0))
+    return {"ms_per_step": round(total / steps, 3), "launches_per_step": ctx.launches(),
+            "bit_identical_to_launched": True, "replayed": replayed,
+            "note": "one cudaGraphLaunch per call on unchanged views, options and buffers"}
 
 
 def quantised_sgm(args, scene, work, ctx, torch, device, stream, flush):

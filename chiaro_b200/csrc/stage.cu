@@ -54,6 +54,14 @@ struct chiaro_depth_ctx {
     std::map<uint64_t, int> batch_tuning;
     int batch_warps = 0, batch_waves = 0, batch_replayed = 0;
     int band_windows = 0;  // fallback windows of the last banded SGM
+    // whole-stage graph of the device-buffer entry point (opt-in): the key of the last
+    // call, the buffer-allocation epoch its pointers belong to, and the captured graph
+    uint64_t alloc_epoch = 0;  // bumped by every (re)allocation of a cached buffer
+    int stage_graph = 0;       // enabled by chiaro_depth_set_stage_graph
+    std::string stage_key;     // key of the last device-buffer call
+    uint64_t stage_key_epoch = 0;
+    cudaGraphExec_t stage_exec = nullptr;
+    int stage_graph_state = 0;  // last call: 0 launched, 1 captured, 2 replayed
     float timings[7] = {};
     int launches = 0;  // this library's kernel launches in the last stage call
 };
@@ -81,6 +89,7 @@ T *dbuf(chiaro_depth_ctx *ctx, const std::string &name, size_t count) {
         b.ptr = nullptr;
         CK(cudaMalloc(&b.ptr, bytes));
         b.bytes = bytes;
+        ++ctx->alloc_epoch;  // a captured stage graph holding the old pointer is void
     }
     return static_cast<T *>(b.ptr);
 }
@@ -1024,6 +1033,88 @@ void download_field(chiaro_depth_ctx *ctx, const Field &f, size_t n, uint8_t *ha
     download(ctx, regularized, f.regularized, n);
 }
 
+// The whole-stage graph of the device-buffer entry point. A call's key holds what the
+// captured launches depend on: every view's pointers, sizes, flags and camera, the
+// reference, the options, the grids and the output pointers (the data behind the
+// pointers may change: a replay reads it afresh). The first call with a key runs the
+// stage (and allocates its buffers), the second captures it, later ones replay it;
+// any (re)allocation of a cached buffer voids the graph.
+template <class T>
+void key_put(std::string &key, const T &v) {
+    key.append(reinterpret_cast<const char *>(&v), sizeof(T));
+}
+
+std::string stage_key(const std::vector<DevView> &views, int reference, const chiaro_depth_options &o, const Grids &g,
+                      const StageOutputs &out, const DevView *d_views, const Results *d_results) {
+    std::string key;
+    for (const DevView &v : views) {
+        key_put(key, v.luma.data);
+        key_put(key, v.luma.width);
+        key_put(key, v.luma.height);
+        key_put(key, v.warp.points);
+        key_put(key, v.warp.step);
+        key_put(key, v.warp.columns);
+        key_put(key, v.warp.rows);
+        key_put(key, v.width);
+        key_put(key, v.height);
+        key_put(key, v.has_camera);
+        key_put(key, v.accepted);
+        key_put(key, v.cam);  // doubles then four ints: no padding
+    }
+    key_put(key, reference);
+    key_put(key, o.enabled);
+    key_put(key, o.grid_step);
+    key_put(key, o.near_depth);
+    key_put(key, o.far_depth);
+    key_put(key, o.planes);
+    key_put(key, o.patch_radius);
+    key_put(key, o.minimum_support);
+    key_put(key, o.best_view_count);
+    key_put(key, o.minimum_score);
+    key_put(key, o.minimum_margin);
+    key_put(key, o.minimum_improvement);
+    key_put(key, o.minimum_neighbour_support);
+    key_put(key, o.completion_iterations);
+    key_put(key, g.coarse_step);
+    key_put(key, g.coarse_columns);
+    key_put(key, g.coarse_rows);
+    key_put(key, g.step);
+    key_put(key, g.columns);
+    key_put(key, g.rows);
+    key_put(key, out.depth);
+    key_put(key, out.confidence);
+    key_put(key, out.provenance);
+    for (int t = 0; t < MAX_VIEWS; ++t) {
+        key_put(key, out.points[t]);
+        key_put(key, out.warp_confidence[t]);
+    }
+    key_put(key, d_views);
+    key_put(key, d_results);
+    return key;
+}
+
+// Ends a stream capture that an exception interrupted.
+struct CaptureGuard {
+    cudaStream_t stream = nullptr;
+    bool active = false;
+    ~CaptureGuard() {
+        if (!active) return;
+        cudaGraph_t graph = nullptr;
+        cudaStreamEndCapture(stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+    }
+};
+
+// An event of the stage's timing; inside a capture an external record node, so that a
+// replay records it too.
+void record_event(cudaEvent_t event, cudaStream_t s, bool capturing) {
+    if (capturing)
+        CK(cudaEventRecordWithFlags(event, s, cudaEventRecordExternal));
+    else
+        CK(cudaEventRecord(event, s));
+}
+
 // Run the whole stage on device-resident views. h_views: the DevView array
 // (device pointers inside), d_views: its device copy.
 void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_views, int reference,
@@ -1067,15 +1158,54 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     upload(ctx, d_sp_direct, sp_direct.data(), sp_direct.size());
     upload(ctx, d_sp_wide, sp_wide.data(), sp_wide.size());
     upload(ctx, d_sp25, spatial25.data(), 25);
+    // the quad planes' buffers and the views that point at them, before any launch
+    for (int t : targets) {
+        const PlaneRef &lp = h_views[t].luma;
+        h_views[t].quads = dbuf<float4>(ctx, "quads" + std::to_string(t), (size_t)lp.width * lp.height);
+    }
+    upload(ctx, d_views, h_views.data(), h_views.size());
+    GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
+    GeomRec *fine_geometry = dbuf<GeomRec>(ctx, "fine_geometry", M * std::max(V, 1));
+    // quad planes 1 per target, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
+    // decisions 1 + 3 per target, map 1
+    ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
+    // the whole-stage graph (device-buffer calls only)
+    ctx->stage_graph_state = 0;
+    bool capturing = false;
+    CaptureGuard guard;
+    if (ctx->stage_graph && !host && !debug) {
+        const std::string key = stage_key(h_views, reference, o, g, out, d_views, d_results);
+        const bool same = key == ctx->stage_key && ctx->alloc_epoch == ctx->stage_key_epoch;
+        if (same && ctx->stage_exec) {
+            CK(cudaGraphLaunch(ctx->stage_exec, s));
+            ctx->stage_graph_state = 2;
+            rewritten = targets;
+            if (V == 0) rewritten.clear();
+            CK(cudaMemcpyAsync(&h_results, d_results, sizeof(Results), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ctx->timings[i], ctx->events[i], ctx->events[i + 1]));
+            CK(cudaEventElapsedTime(&ctx->timings[6], ctx->events[0], ctx->events[6]));
+            return;
+        }
+        if (ctx->stage_exec) {
+            CK(cudaGraphExecDestroy(ctx->stage_exec));
+            ctx->stage_exec = nullptr;
+        }
+        capturing = same;  // the second call with this key: capture it
+        ctx->stage_key = key;
+    }
+    if (capturing) {
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        guard.stream = s;
+        guard.active = true;
+    }
     CK(cudaMemsetAsync(d_results, 0, sizeof(Results), s));
 
-    CK(cudaEventRecord(ctx->events[0], s));
+    record_event(ctx->events[0], s, capturing);
     // per (node, target) geometry of both grids: cameras and warps only, so it runs
     // while the luminance planes are still arriving
-    GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
     launch_geometry(ctx, d_views, reference, targets, g.coarse_columns, g.coarse_rows, g.coarse_step,
                     coarse_geometry);
-    GeomRec *fine_geometry = dbuf<GeomRec>(ctx, "fine_geometry", M * std::max(V, 1));
     launch_geometry(ctx, d_views, reference, targets, g.columns, g.rows, g.step, fine_geometry);
     if (host && !host->planes.empty()) {
         for (const auto &u : host->planes)
@@ -1087,12 +1217,10 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     for (int t : targets) {
         const PlaneRef &lp = h_views[t].luma;
         size_t n = (size_t)lp.width * lp.height;
-        float4 *quads = dbuf<float4>(ctx, "quads" + std::to_string(t), n);
-        quad_plane_kernel<<<blocks_for(n, 256), 256, 0, s>>>(lp.data, lp.width, lp.height, quads);
+        quad_plane_kernel<<<blocks_for(n, 256), 256, 0, s>>>(lp.data, lp.width, lp.height,
+                                                             const_cast<float4 *>(h_views[t].quads));
         CK(cudaGetLastError());
-        h_views[t].quads = quads;
     }
-    upload(ctx, d_views, h_views.data(), h_views.size());
     // ---- cost volume
     float *scores = dbuf<float>(ctx, "scores", N * D);
     float *costs = dbuf<float>(ctx, "costs", N * D);
@@ -1126,11 +1254,11 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         cost_volume_kernel<<<(unsigned)N, COST_THREADS, smem, s>>>(p);
         CK(cudaGetLastError());
     }
-    CK(cudaEventRecord(ctx->events[1], s));
+    record_event(ctx->events[1], s, capturing);
     // ---- SGM
     float *regularised = dbuf<float>(ctx, "regularised", N * D);
     launch_sgm(ctx, costs, guidance, regularised, (int)g.coarse_columns, (int)g.coarse_rows, D);
-    CK(cudaEventRecord(ctx->events[2], s));
+    record_event(ctx->events[2], s, capturing);
     // ---- select (+ completion)
     Field coarse = field_bufs(ctx, "coarse", N);
     uint8_t *fillable = dbuf<uint8_t>(ctx, "fillable", N);
@@ -1173,7 +1301,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
                        debug->coarse_improvement, debug->coarse_regularized);
         download(ctx, debug->coarse_fillable, fillable, N);
     }
-    CK(cudaEventRecord(ctx->events[3], s));
+    record_event(ctx->events[3], s, capturing);
     // ---- direct measurement
     Field direct = field_bufs(ctx, "direct", M);
     float *fguidance = dbuf<float>(ctx, "fine_guidance", M);
@@ -1233,7 +1361,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         download(ctx, debug->direct_guidance, fguidance, M);
         download(ctx, debug->direct_tested, ftested, M);
     }
-    CK(cudaEventRecord(ctx->events[4], s));
+    record_event(ctx->events[4], s, capturing);
     // ---- consistency filters (depth.rs:383-392)
     uint8_t *has_a = dbuf<uint8_t>(ctx, "has_isolated", M);
     reject_isolated_kernel<<<blocks_for(M, 256), 256, 0, s>>>(direct.has, direct.depth, direct.confidence, fguidance,
@@ -1288,8 +1416,8 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     // the depth map needs only the final field, so it is ready before the decisions
     depth_map_kernel<<<blocks_for(M, 256), 256, 0, s>>>(fin, ftested, out.depth, out.confidence, out.provenance, (int)M);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(ctx->map_ready, s));
-    CK(cudaEventRecord(ctx->events[5], s));
+    if (host) CK(cudaEventRecord(ctx->map_ready, s));
+    record_event(ctx->events[5], s, capturing);
     // ---- per-target decisions (depth.rs:420-547): all targets in one launch
     rewritten.clear();
     if (V > 0) {
@@ -1334,10 +1462,21 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
             rewritten.push_back(t);
         }
     }
-    CK(cudaEventRecord(ctx->events[6], s));
-    // quad planes 1 per target, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
-    // decisions 1 + 3 per target, map 1
-    ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
+    record_event(ctx->events[6], s, capturing);
+    if (capturing) {
+        cudaGraph_t graph = nullptr;
+        guard.active = false;
+        CK(cudaStreamEndCapture(s, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&ctx->stage_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            ctx->stage_exec = nullptr;
+            throw CudaError{e, "cudaGraphInstantiate(stage)"};
+        }
+        CK(cudaGraphLaunch(ctx->stage_exec, s));
+        ctx->stage_graph_state = 1;
+    }
+    if (ctx->stage_graph && !host && !debug) ctx->stage_key_epoch = ctx->alloc_epoch;
     if (host) {
         // every kernel is queued: the depth map leaves on the copy stream while the
         // decisions run (a pageable destination blocks this thread, not the GPU)
@@ -1564,6 +1703,7 @@ void chiaro_depth_ctx_destroy(chiaro_depth_ctx *ctx) {
     for (auto &e : ctx->events)
         if (e) cudaEventDestroy(e);
     if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+    if (ctx->stage_exec) cudaGraphExecDestroy(ctx->stage_exec);
     if (ctx->planes_ready) cudaEventDestroy(ctx->planes_ready);
     if (ctx->map_ready) cudaEventDestroy(ctx->map_ready);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
@@ -1620,6 +1760,25 @@ int chiaro_refine_multiview_depth_device(chiaro_depth_ctx *ctx, const chiaro_vie
                                          chiaro_depth_map *out_map) {
     return refine(ctx, views, n_views, reference_index, options, refined, reports, out_map, nullptr, true);
 }
+
+int chiaro_depth_set_stage_graph(chiaro_depth_ctx *ctx, int32_t enabled) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        ctx->stage_graph = enabled != 0;
+        if (!ctx->stage_graph && ctx->stage_exec) {
+            CK(cudaStreamSynchronize(ctx->stream));
+            CK(cudaGraphExecDestroy(ctx->stage_exec));
+            ctx->stage_exec = nullptr;
+        }
+        ctx->stage_key.clear();
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+    return CHIARO_OK;
+}
+
+int chiaro_depth_stage_graph_state(const chiaro_depth_ctx *ctx) { return ctx ? ctx->stage_graph_state : -1; }
 
 int chiaro_depth_last_timings(const chiaro_depth_ctx *ctx, float *ms, int capacity) {
     if (!ctx || !ms) return 0;

@@ -51,6 +51,8 @@ SIGNATURES = {
                                             C.c_void_p]),
     "chiaro_depth_sample_nearest_device": (C.c_int, [C.c_void_p, P(abi.DepthMapC), C.c_void_p, C.c_uint64,
                                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "chiaro_depth_set_stage_graph": (C.c_int, [C.c_void_p, C.c_int32]),
+    "chiaro_depth_stage_graph_state": (C.c_int, [C.c_void_p]),
     "chiaro_align_options_default": (None, [P(abi.AlignOptionsC)]),
     "chiaro_align_module": (C.c_int, [C.c_void_p, P(abi.AlignInputC), P(abi.AlignInputC), C.c_int32,
                                       P(abi.AlignOptionsC), P(abi.WarpC), P(abi.WarpC), P(C.c_float),

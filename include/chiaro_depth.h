@@ -254,6 +254,20 @@ int chiaro_refine_multiview_depth_device(chiaro_depth_ctx *ctx,
                                          chiaro_depth_report *reports,
                                          chiaro_depth_map *out_map);
 
+/* Whole-stage CUDA graph of chiaro_refine_multiview_depth_device (no counterpart in
+ * the reference; off by default). When enabled, a device-buffer call whose views
+ * (pointers, sizes, flags, cameras), reference, options and output pointers equal the
+ * previous call's is captured into a graph on its second occurrence and replayed from
+ * the third on: the stage's ~50 launches become one, and a replay reads the current
+ * contents of the same buffers. Any other call, or any buffer the context reallocates
+ * (another entry point on a larger size, for instance), voids the graph and the next
+ * calls run, capture and replay afresh. Calls with debug arrays or host buffers never
+ * use it. The first call of a key should not come during another stream capture. */
+int chiaro_depth_set_stage_graph(chiaro_depth_ctx *ctx, int32_t enabled);
+/* What the last device-buffer stage call did: 0 launched its kernels, 1 captured and
+ * launched the graph, 2 replayed it. */
+int chiaro_depth_stage_graph_state(const chiaro_depth_ctx *ctx);
+
 /* Device time in milliseconds of each stage of the last call on this context:
  * [0] cost volume, [1] SGM, [2] select, [3] direct pass, [4] filters,
  * [5] per-target decisions, [6] whole stage. Returns the count written. */
