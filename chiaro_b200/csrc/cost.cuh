@@ -27,6 +27,7 @@ struct CostParams {
     const float *spatial;       // [(2r+1)^2] spatial weights
     const GeomRec *geometry;    // [node][target]
     int radius;
+    TapLattice lattice;         // of this grid, or planes == nullptr
     int minimum_support, best_view_count;
     float *scores, *costs, *guidance;
     uint8_t *tested;
@@ -97,17 +98,33 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
     const DevView &rv = p.views[p.reference];
     const D3 origin = camera_origin(rv.cam);
 
-    // ---- staging: geometry, reference patch, tap positions
+    // ---- staging: geometry, reference patch, tap positions (from the tap lattice when
+    // the grid has one)
     if (tid < V) geom_from_rec(p.geometry[(size_t)node * V + tid], origin, s.geom[tid]);
+    const TapLattice &lat = p.lattice;
+    const size_t at0 = lat.planes ? lat.index(cx, cy) : 0;
     float centre = 0.0f;
-    const bool centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+    bool centre_ok;
+    if (lat.planes) {
+        const float2 c = __ldg(lat.planes + at0);
+        centre = c.x;
+        centre_ok = c.y != 0.0f;
+    } else {
+        centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+    }
     bool sampled = true;
     for (int t = tid; t < taps; t += COST_THREADS) {
         int dx, dy;
         tap_offset(t, p.radius, dx, dy);
-        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
         float value = 0.0f;
-        sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+        if (lat.planes) {
+            const float2 r = __ldg(lat.planes + at0 + (ptrdiff_t)dy * lat.columns + dx);
+            value = r.x;
+            sampled &= r.y != 0.0f;
+        } else {
+            double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+            sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+        }
         float weight = p.spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
         float weighted = weight * value;
         s.wt[t] = make_float2(weight, weighted);
@@ -118,9 +135,17 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         const int v = i / taps, t = i - v * taps;
         int dx, dy;
         tap_offset(t, p.radius, dx, dy);
-        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
         float qx = 0.0f, qy = 0.0f;
-        if (!warp_map(p.views[p.targets[v]].warp, (float)px, (float)py, qx, qy)) undefined |= 1u << v;
+        if (lat.planes) {
+            const float2 q = __ldg(lat.planes + (size_t)(v + 1) * lat.plane_size() + at0 +
+                                   (ptrdiff_t)dy * lat.columns + dx);
+            qx = q.x;
+            qy = q.y;
+            if (qx != qx) undefined |= 1u << v;
+        } else {
+            double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+            if (!warp_map(p.views[p.targets[v]].warp, (float)px, (float)py, qx, qy)) undefined |= 1u << v;
+        }
         s.gh[i] = make_double2((double)qx * 0.5, (double)qy * 0.5);
     }
     // displacement of every (target, label) item, view-major: item = v * D + label

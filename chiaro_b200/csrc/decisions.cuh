@@ -29,6 +29,7 @@ struct DecisionParams {
     int columns, rows, step;
     Field field;
     const GeomRec *geometry;  // [node][target] of the fine grid
+    TapLattice lattice;       // of the fine grid, or planes == nullptr
     double inverse_step, near_depth, far_depth;
     int radius;
     const float *spatial;
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
     defined = __reduce_or_sync(full, defined);
     if (!has || !defined) return;  // whole warp
     const unsigned undefined_taps = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, p.radius,
-                                                     p.spatial, d.rr, d.wt, d.gh, d.box, patch);
+                                                     p.spatial, d.rr, d.wt, d.gh, d.box, patch, p.lattice);
     const bool patch_ok = patch.ok;
     const D3 origin = camera_origin(rv.cam);
     const double shared_inverse = 1.0 / p.field.depth[node];

@@ -90,6 +90,7 @@ struct DirectParams {
     double inverse_step, near_depth, far_depth;
     const double *unseeded;                            // 32 candidates, far to near
     const GeomRec *geometry;                           // [node][target] of the fine grid
+    TapLattice lattice;                                // of the fine grid, or planes == nullptr
     int radius, wide_radius;
     const float *spatial, *spatial_wide;
     float minimum_score, minimum_margin, minimum_improvement;
@@ -200,7 +201,7 @@ __device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot<T
     const int lane = threadIdx.x & 31;
     const int V = p.n_targets;
     const unsigned undefined = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, radius, spatial, d.rr,
-                                                d.wt, d.gh, d.box, patch);
+                                                d.wt, d.gh, d.box, patch, p.lattice);
     if (lane < V) {
         geom_from_rec(recs[lane], camera_origin(p.views[p.reference].cam), d.geom[lane]);
         d.geom[lane].taps_ok = ((undefined >> lane) & 1u) ? 0 : 1;

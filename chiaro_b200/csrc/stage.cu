@@ -1166,9 +1166,28 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     upload(ctx, d_views, h_views.data(), h_views.size());
     GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
     GeomRec *fine_geometry = dbuf<GeomRec>(ctx, "fine_geometry", M * std::max(V, 1));
+    // the tap lattice of the grids with an even step (every tap of theirs is a lattice point)
+    const bool coarse_lattice = V > 0 && g.coarse_step % 2 == 0, fine_lattice = V > 0 && g.step % 2 == 0;
+    TapLattice lattice{};
+    if (coarse_lattice || fine_lattice) {
+        size_t extent_x = 0, extent_y = 0;
+        if (coarse_lattice) {
+            extent_x = (g.coarse_columns - 1) * g.coarse_step;
+            extent_y = (g.coarse_rows - 1) * g.coarse_step;
+        }
+        if (fine_lattice) {
+            extent_x = std::max(extent_x, (g.columns - 1) * g.step);
+            extent_y = std::max(extent_y, (g.rows - 1) * g.step);
+        }
+        lattice.margin = std::max({radius, direct_radius, wide_radius});
+        lattice.columns = (int)(extent_x / 2 + 2 * (size_t)lattice.margin + 1);
+        lattice.rows = (int)(extent_y / 2 + 2 * (size_t)lattice.margin + 1);
+        lattice.planes = dbuf<float2>(ctx, "tap_lattice", (size_t)(V + 1) * lattice.columns * lattice.rows);
+    }
     // quad planes 1 per target, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
     // decisions 1 + 3 per target, map 1
-    ctx->launches = V + (V > 0 ? 2 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 + 2 + (V > 0 ? 1 + 3 * V : 0) + 1;
+    ctx->launches = V + (V > 0 ? 2 : 0) + (lattice.planes ? 1 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 +
+                    2 + (V > 0 ? 1 + 3 * V : 0) + 1;
     // the whole-stage graph (device-buffer calls only)
     ctx->stage_graph_state = 0;
     bool capturing = false;
@@ -1213,6 +1232,19 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         CK(cudaEventRecord(ctx->planes_ready, ctx->copy_stream));
         CK(cudaStreamWaitEvent(s, ctx->planes_ready, 0));
     }
+    if (lattice.planes) {
+        LatticeParams p{};
+        p.views = d_views;
+        p.reference = reference;
+        p.n_targets = V;
+        for (int v = 0; v < V; ++v) p.targets[v] = targets[v];
+        p.columns = lattice.columns;
+        p.rows = lattice.rows;
+        p.margin = lattice.margin;
+        p.out = const_cast<float2 *>(lattice.planes);
+        tap_lattice_kernel<<<blocks_for((size_t)lattice.columns * lattice.rows, 256), 256, 0, s>>>(p);
+        CK(cudaGetLastError());
+    }
     // quad planes of the target luminance for the fast ZNCC path
     for (int t : targets) {
         const PlaneRef &lp = h_views[t].luma;
@@ -1241,6 +1273,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         p.label_depth = d_labels;
         p.spatial = d_sp;
         p.radius = radius;
+        if (coarse_lattice) p.lattice = lattice;
         p.minimum_support = (int)o.minimum_support;
         p.best_view_count = (int)std::min<uint64_t>(o.best_view_count, MAX_VIEWS);
         p.scores = scores;
@@ -1309,6 +1342,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     {
         DirectParams p{};
         p.geometry = fine_geometry;
+        if (fine_lattice) p.lattice = lattice;
         p.views = d_views;
         p.reference = reference;
         p.n_targets = V;
@@ -1434,6 +1468,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         p.step = (int)g.step;
         p.field = fin;
         p.geometry = fine_geometry;
+        if (fine_lattice) p.lattice = lattice;
         p.inverse_step = inverse_step;
         p.near_depth = o.near_depth;
         p.far_depth = o.far_depth;

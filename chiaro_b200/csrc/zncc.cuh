@@ -101,6 +101,51 @@ __device__ inline void store_reference_sum(RefPatch &patch, int which, float sum
         patch.sum_rr = sum;
 }
 
+// Tap lattice. A node of a grid with an even step sits at even pixel coordinates and its
+// taps lie 2 px apart, so every tap of every node is a point (px, py) of the even lattice.
+// The reference sample and each target's global warp at a tap depend on (px, py) alone,
+// so they are evaluated once per lattice point and call (tap_lattice_kernel) instead of
+// once per node and tap; a node reads them back with plain loads. Plane 0 holds the
+// reference sample (plane_sample's value, 1 if it is Some else 0; the value is 0 when
+// None, as the staging's initial value), plane 1 + v target v's Warp::map (NaN for None).
+// Point (i, j) is the pixel (2 (i - margin), 2 (j - margin)). planes == nullptr: none.
+struct TapLattice {
+    const float2 *planes;  // [(V + 1)][rows][columns]
+    int columns, rows, margin;
+    __device__ __forceinline__ size_t plane_size() const { return (size_t)columns * rows; }
+    // the lattice point of the even pixel (cx, cy)
+    __device__ __forceinline__ size_t index(double cx, double cy) const {
+        return (size_t)((int)(cy * 0.5) + margin) * columns + ((int)(cx * 0.5) + margin);
+    }
+};
+
+struct LatticeParams {
+    const DevView *views;
+    int reference, n_targets;
+    int targets[MAX_VIEWS];
+    int columns, rows, margin;
+    float2 *out;
+};
+
+// A thread per lattice point: the reference sample and every target's global warp there,
+// with the staging's own expressions (warp_stage_patch).
+__global__ void __launch_bounds__(256) tap_lattice_kernel(LatticeParams p) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long size = (long)p.columns * p.rows;
+    if (i >= size) return;
+    const double px = (double)(2 * ((int)(i % p.columns) - p.margin));
+    const double py = (double)(2 * ((int)(i / p.columns) - p.margin));
+    float value = 0.0f;
+    const bool ok =
+        plane_sample(p.views[p.reference].luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+    p.out[i] = make_float2(value, ok ? 1.0f : 0.0f);
+    for (int v = 0; v < p.n_targets; ++v) {
+        float qx = 0.0f, qy = 0.0f;
+        const bool defined = warp_map(p.views[p.targets[v]].warp, (float)px, (float)py, qx, qy);
+        p.out[(size_t)(v + 1) * size + i] = defined ? make_float2(qx, qy) : make_float2(NAN, NAN);
+    }
+}
+
 // Warp-cooperative staging of one node at (cx, cy) and `radius`: the
 // reference patch ((w, w r) and (w r) r per tap, the three sums, the energy and the
 // centre sample) and, for each target, g/2 of every tap and their box. Returns
@@ -110,30 +155,51 @@ __device__ inline void store_reference_sum(RefPatch &patch, int which, float sum
 template <typename TapT>
 __device__ inline unsigned warp_stage_patch(const DevView *views, int reference, const int *targets, int V,
                                             double cx, double cy, int radius, const float *spatial, float *rr,
-                                            float2 *wt, TapT *gh, TapBox *box, RefPatch &patch) {
+                                            float2 *wt, TapT *gh, TapBox *box, RefPatch &patch,
+                                            const TapLattice &lattice) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int taps = (2 * radius + 1) * (2 * radius + 1);
     const DevView &rv = views[reference];
     float centre = 0.0f;
-    const bool centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+    bool centre_ok;
+    const size_t at0 = lattice.planes ? lattice.index(cx, cy) : 0;
+    if (lattice.planes) {
+        const float2 c = __ldg(lattice.planes + at0);
+        centre = c.x;
+        centre_ok = c.y != 0.0f;
+    } else {
+        centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+    }
     bool sampled = true;
     unsigned undefined = 0u;
     for (int t = lane; t < taps; t += 32) {
         int dx, dy;
         tap_offset(t, radius, dx, dy);
-        double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
         float value = 0.0f;
-        sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+        if (lattice.planes) {
+            const size_t at = at0 + (ptrdiff_t)dy * lattice.columns + dx;
+            const float2 r = __ldg(lattice.planes + at);
+            value = r.x;
+            sampled &= r.y != 0.0f;
+            for (int v = 0; v < V; ++v) {
+                const float2 q = __ldg(lattice.planes + (size_t)(v + 1) * lattice.plane_size() + at);
+                if (q.x != q.x) undefined |= 1u << v;
+                store_tap(gh[v * taps + t], q.x, q.y);
+            }
+        } else {
+            double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+            sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+            for (int v = 0; v < V; ++v) {
+                float qx = 0.0f, qy = 0.0f;
+                if (!warp_map(views[targets[v]].warp, (float)px, (float)py, qx, qy)) undefined |= 1u << v;
+                store_tap(gh[v * taps + t], qx, qy);
+            }
+        }
         float weight = spatial[t] * exp_f32(-1.2f * fabsf(value - centre));
         float weighted = weight * value;
         wt[t] = make_float2(weight, weighted);
         rr[t] = weighted * value;
-        for (int v = 0; v < V; ++v) {
-            float qx = 0.0f, qy = 0.0f;
-            if (!warp_map(views[targets[v]].warp, (float)px, (float)py, qx, qy)) undefined |= 1u << v;
-            store_tap(gh[v * taps + t], qx, qy);
-        }
     }
     undefined = __reduce_or_sync(full, undefined);
     sampled = __all_sync(full, sampled);

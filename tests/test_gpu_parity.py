@@ -204,6 +204,17 @@ def test_stage_with_completion_and_grid_step_bit_exact():
     _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
 
 
+@pytest.mark.parametrize("grid_step", [5, 10])
+def test_stage_with_an_odd_grid_step_bit_exact(grid_step):
+    """An odd step puts taps off the even tap lattice: grid_step 5 gives an odd coarse step
+    (the cost volume samples the planes per tap) and an even fine step (the direct pass and
+    the decisions read the lattice); grid_step 10 the other way round."""
+    sc = scenes.workload("tiny", seed=7)
+    opt = DepthOptions(**{**sc.options.__dict__, "grid_step": grid_step})
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc, options=opt)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+
+
 def test_stage_at_the_finest_coarse_grid_bit_exact():
     """grid_step 4: the coarse grid at the direct grid's step (the finest the reference
     reaches, depth.rs:326-328), as in the five-view workload's step-4 configuration."""
