@@ -209,23 +209,23 @@ __device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot<T
     __syncwarp();
 }
 
-// Warp-cooperative scores of the baseline and candidates cand[0..n) over all
-// targets, aggregated into d.agg[0..n]. NaN = None. Item i is (candidate
-// i / V - 1, target i % V), candidate -1 being the baseline. A first sweep
-// settles which items reach the correlation and whether their taps are all
-// inside (the fast path), and lists them fast-first; the correlations then run
-// over that list, so lanes idle only in the last round.
+// Warp-cooperative listing of the baseline and candidates cand[0..n) over all
+// targets. Item i is (candidate i / V - 1, target i % V), candidate -1 being the
+// baseline. It settles which items reach the correlation and whether their taps
+// are all inside (the fast path), sets the others' scores to None and lists the
+// scored ones: fast from the front of d.list, exact from the back of its
+// (n + 1) V entries. Every lane returns the two counts.
 template <typename TapT>
-__device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlot<TapT> &d, const RefPatch &patch,
-                                          const double *cand, int n, int radius) {
+__device__ inline void warp_direct_list(const DirectParams &p, const DirectSlot<TapT> &d, const RefPatch &patch,
+                                        const double *cand, int n, int &n_fast, int &n_exact) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const int V = p.n_targets;
-    const int taps = (2 * radius + 1) * (2 * radius + 1);
     const int total = (n + 1) * V;
     const ViewGeom *geom = d.geom;
-    int n_fast = 0, n_exact = 0;
+    n_fast = 0;
+    n_exact = 0;
     for (int base = 0; base < total; base += 32) {
         const int item = base + lane;
         bool scored = false, fast = false;
@@ -250,21 +250,29 @@ __device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlo
         n_fast += __popc(fast_mask);
         n_exact += __popc(exact_mask);
     }
-    __syncwarp();
-    const int listed = n_fast + n_exact;
-    for (int j = lane; j < listed; j += 32) {
-        const int item = j < n_fast ? d.list[j] : d.list[total - 1 - (j - n_fast)];
-        const int c = item / V - 1, v = item - (item / V) * V;
-        const DevView &tv = p.views[p.targets[v]];
-        double ddx = 0.0, ddy = 0.0;
-        if (c >= 0) depth_delta(tv.cam, geom[v], cand[c], ddx, ddy);
-        float score = NAN, sc;
-        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, ddx, ddy, sc))
-            score = sc;
-        d.items[item] = score;
-    }
-    __syncwarp();
-    for (int c = lane; c <= n; c += 32) {
+}
+
+// The correlation of one listed item (warp_direct_list) into d.items; one thread.
+template <typename TapT>
+__device__ __forceinline__ void direct_item_score(const DirectParams &p, const DirectSlot<TapT> &d,
+                                                  const RefPatch &patch, const double *cand, int item, int taps) {
+    const int V = p.n_targets;
+    const int c = item / V - 1, v = item - (item / V) * V;
+    const DevView &tv = p.views[p.targets[v]];
+    double ddx = 0.0, ddy = 0.0;
+    if (c >= 0) depth_delta(tv.cam, d.geom[v], cand[c], ddx, ddy);
+    float score = NAN, sc;
+    if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, ddx, ddy, sc))
+        score = sc;
+    d.items[item] = score;
+}
+
+// aggregate (depth.rs:1761-1770) of the baseline and candidates over the targets into
+// d.agg[0..n]; the warp of the node.
+template <typename TapT>
+__device__ inline void warp_direct_aggregate(const DirectParams &p, const DirectSlot<TapT> &d, int n) {
+    const int V = p.n_targets;
+    for (int c = threadIdx.x & 31; c <= n; c += 32) {
         float sc[MAX_VIEWS];
         for (int v = 0; v < V; ++v) sc[v] = d.items[c * V + v];
         float a;
@@ -273,23 +281,76 @@ __device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlo
     __syncwarp();
 }
 
-// A warp per fine node; the CTA holds nodes_per_cta nodes.
+// Warp-cooperative scores of the baseline and candidates cand[0..n) over all
+// targets, aggregated into d.agg[0..n] (NaN = None): the node's list, scored by
+// its own warp.
+template <typename TapT>
+__device__ inline void warp_direct_scores(const DirectParams &p, const DirectSlot<TapT> &d, const RefPatch &patch,
+                                          const double *cand, int n, int radius) {
+    const int lane = threadIdx.x & 31;
+    const int taps = (2 * radius + 1) * (2 * radius + 1);
+    const int total = (n + 1) * p.n_targets;
+    int n_fast, n_exact;
+    warp_direct_list(p, d, patch, cand, n, n_fast, n_exact);
+    __syncwarp();
+    const int listed = n_fast + n_exact;
+    for (int j = lane; j < listed; j += 32)
+        direct_item_score(p, d, patch, cand, j < n_fast ? d.list[j] : d.list[total - 1 - (j - n_fast)], taps);
+    __syncwarp();
+    warp_direct_aggregate(p, d, n);
+}
+
+// A warp per fine node; the CTA holds nodes_per_cta nodes. Each warp lists its
+// node's items; the CTA then scores the pooled lists (every node's fast items,
+// then every node's exact items), so the lanes of all warps stay busy up to the
+// pool's last round instead of each node's; each warp then selects its node.
 __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patches[8];
+    __shared__ int pool[8][3];  // per node: fast count, exact count, list length
     const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nodes = blockDim.x >> 5;  // == p.nodes_per_cta
     const int node = blockIdx.x * p.nodes_per_cta + slot;
-    if (slot >= p.nodes_per_cta || node >= p.columns * p.rows) return;  // whole warps
+    const bool active = node < p.columns * p.rows;  // whole warps
     const int V = p.n_targets;
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
-    DirectSlot<float2> d =
-        carve_direct_slot<float2>(smem_raw + (size_t)slot * direct_slot_bytes<float2>(V, taps), V, taps);
+    const size_t slot_bytes = direct_slot_bytes<float2>(V, taps);
+    DirectSlot<float2> d = carve_direct_slot<float2>(smem_raw + (size_t)slot * slot_bytes, V, taps);
     RefPatch &patch = patches[slot];
     const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
-    int seeded;
-    const int n = warp_direct_candidates(p, cx, cy, d.cand, seeded);
-    warp_stage_node(p, d, patch, cx, cy, p.radius, p.spatial, p.geometry + (size_t)node * V);
-    warp_direct_scores(p, d, patch, d.cand, n, p.radius);
+    int seeded = 0, n = 0, n_fast = 0, n_exact = 0;
+    if (active) {
+        n = warp_direct_candidates(p, cx, cy, d.cand, seeded);
+        warp_stage_node(p, d, patch, cx, cy, p.radius, p.spatial, p.geometry + (size_t)node * V);
+        warp_direct_list(p, d, patch, d.cand, n, n_fast, n_exact);
+    }
+    if (lane == 0) {
+        pool[slot][0] = n_fast;
+        pool[slot][1] = n_exact;
+        pool[slot][2] = (n + 1) * V;
+    }
+    __syncthreads();
+    int fast_total = 0, pooled = 0;
+    for (int k = 0; k < nodes; ++k) {
+        fast_total += pool[k][0];
+        pooled += pool[k][0] + pool[k][1];
+    }
+    for (int j = threadIdx.x; j < pooled; j += blockDim.x) {
+        // node k and the position of pooled entry j in its list
+        int k = 0, at = j;
+        if (j < fast_total) {
+            while (at >= pool[k][0]) at -= pool[k++][0];
+        } else {
+            at -= fast_total;
+            while (at >= pool[k][1]) at -= pool[k++][1];
+            at = pool[k][2] - 1 - at;
+        }
+        const DirectSlot<float2> dk = carve_direct_slot<float2>(smem_raw + (size_t)k * slot_bytes, V, taps);
+        direct_item_score(p, dk, patches[k], dk.cand, dk.list[at], taps);
+    }
+    __syncthreads();
+    if (!active) return;
+    warp_direct_aggregate(p, d, n);
     bool seen = false;
     for (int c = lane; c <= n; c += 32) seen |= d.agg[c] == d.agg[c];
     const bool tested = __any_sync(0xffffffffu, seen);
