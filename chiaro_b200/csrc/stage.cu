@@ -1161,7 +1161,8 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     // the quad planes' buffers and the views that point at them, before any launch
     for (int t : targets) {
         const PlaneRef &lp = h_views[t].luma;
-        h_views[t].quads = dbuf<float4>(ctx, "quads" + std::to_string(t), (size_t)lp.width * lp.height);
+        h_views[t].quads = dbuf<float4>(ctx, "quads" + std::to_string(t),
+                                        (size_t)quad_pair_stride(lp.width) * ((lp.height + 1) / 2));
     }
     upload(ctx, d_views, h_views.data(), h_views.size());
     GeomRec *coarse_geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(V, 1));
@@ -1184,7 +1185,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         lattice.rows = (int)(extent_y / 2 + 2 * (size_t)lattice.margin + 1);
         lattice.planes = dbuf<float2>(ctx, "tap_lattice", (size_t)(V + 1) * lattice.columns * lattice.rows);
     }
-    // quad planes 1 per target, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
+    // quad planes 1 per target, tap lattice 1, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
     // decisions 1 + 3 per target, map 1
     ctx->launches = V + (V > 0 ? 2 : 0) + (lattice.planes ? 1 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 +
                     2 + (V > 0 ? 1 + 3 * V : 0) + 1;
@@ -1249,7 +1250,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     for (int t : targets) {
         const PlaneRef &lp = h_views[t].luma;
         size_t n = (size_t)lp.width * lp.height;
-        quad_plane_kernel<<<blocks_for(n, 256), 256, 0, s>>>(lp.data, lp.width, lp.height,
+        quad_plane_kernel<<<blocks_for(n, 256), 256, 0, s>>>(lp.data, lp.width, lp.height, quad_pair_stride(lp.width),
                                                              const_cast<float4 *>(h_views[t].quads));
         CK(cudaGetLastError());
     }

@@ -357,19 +357,31 @@ __device__ __forceinline__ bool zncc_score(const PlaneRef &target, const TapT *g
 // bilinear fetch reads the four neighbours from a quad plane with one 16-byte
 // load.
 
-// Quad plane: quads[y * w + x] = (L[y][x], L[y][x1], L[y1][x], L[y1][x1]) with
-// x1 = min(x + 1, w - 1) and y1 = min(y + 1, h - 1).
-__global__ void quad_plane_kernel(const float *__restrict__ plane, int width, int height, float4 *quads) {
+// Quad plane: the quad of (x, y) is (L[y][x], L[y][x1], L[y1][x], L[y1][x1]) with
+// x1 = min(x + 1, w - 1) and y1 = min(y + 1, h - 1), pair-interleaved: the quads of rows
+// 2k and 2k + 1 alternate, so (x, y) sits at (y >> 1) * stride + 2 x + (y & 1) with
+// stride = 2 * roundup(w, 4), and each 128-byte line holds a 4 x 2 block of quads. The
+// taps of neighbouring labels spread along the epipolar line in any direction; against
+// row-major quads (8 x 1 per line) a 4 x 2 block keeps more of a quarter-warp's gathers
+// in one line.
+__host__ __device__ inline int quad_pair_stride(int width) { return 2 * ((width + 3) / 4 * 4); }
+
+__device__ __forceinline__ size_t quad_index(int x, int y, int stride) {
+    return (size_t)(y >> 1) * stride + 2 * x + (y & 1);
+}
+
+__global__ void quad_plane_kernel(const float *__restrict__ plane, int width, int height, int stride,
+                                  float4 *quads) {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long)width * height) return;
     int x = (int)(i % width), y = (int)(i / width);
     long right = x + 1 < width ? 1 : 0, down = y + 1 < height ? width : 0;
-    quads[i] = make_float4(plane[i], plane[i + right], plane[i + down], plane[i + down + right]);
+    quads[quad_index(x, y, stride)] = make_float4(plane[i], plane[i + right], plane[i + down], plane[i + down + right]);
 }
 
 struct TargetRef {
     PlaneRef plane;
-    const float4 *quads;
+    const float4 *quads;  // quad plane
 };
 
 // True when every tap at displacement (hdx, hdy) = (ddx/2, ddy/2) samples
@@ -384,7 +396,7 @@ __device__ __forceinline__ bool taps_inside(const TapBox &box, double hdx, doubl
 // warped_patch_zncc's hypothesis-dependent part for taps known to be inside
 // (see taps_inside). gh holds g/2 per tap.
 template <typename TapT>
-__device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, int width, const TapT *gh,
+__device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, int stride, const TapT *gh,
                                              const float2 *wt, const RefPatch &patch, int taps,
                                              double hdx, double hdy, bool &ok) {
     float st = 0.0f, stt = 0.0f, srt = 0.0f;
@@ -395,7 +407,7 @@ __device__ __forceinline__ float zncc_inside(const float4 *__restrict__ quads, i
         float y = (float)((g.y + hdy) - 0.25);
         int ix, iy;
         float tx = floor_frac_small(x, ix), ty = floor_frac_small(y, iy);
-        const float4 q = __ldg(quads + (size_t)iy * width + ix);
+        const float4 q = __ldg(quads + quad_index(ix, iy, stride));
         float top = q.x * (1.0f - tx) + q.y * tx;
         float bottom = q.z * (1.0f - tx) + q.w * tx;
         float tv = top * (1.0f - ty) + bottom * ty;
@@ -420,7 +432,7 @@ __device__ __forceinline__ bool zncc_any(const TargetRef &target, const TapT *gh
     double hdx = ddx * 0.5, hdy = ddy * 0.5;
     if (taps_inside(box, hdx, hdy, target.plane.width, target.plane.height)) {
         bool ok;
-        score = zncc_inside(target.quads, target.plane.width, gh, wt, patch, taps, hdx, hdy, ok);
+        score = zncc_inside(target.quads, quad_pair_stride(target.plane.width), gh, wt, patch, taps, hdx, hdy, ok);
         return ok;
     }
     return zncc_score(target.plane, gh, wt, patch, taps, ddx, ddy, score);
