@@ -215,6 +215,15 @@ def test_stage_with_an_odd_grid_step_bit_exact(grid_step):
     _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
 
 
+def test_stage_with_a_wide_patch_bit_exact():
+    """patch_radius 6: the wide retry's radius is 12 (25 x 25 taps), so border nodes read the
+    tap lattice out to its full margin."""
+    sc = scenes.workload("tiny", seed=8)
+    opt = DepthOptions(**{**sc.options.__dict__, "patch_radius": 6})
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc, options=opt)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+
+
 def test_stage_at_the_finest_coarse_grid_bit_exact():
     """grid_step 4: the coarse grid at the direct grid's step (the finest the reference
     reaches, depth.rs:326-328), as in the five-view workload's step-4 configuration."""
