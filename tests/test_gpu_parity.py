@@ -215,6 +215,14 @@ def test_stage_with_an_odd_grid_step_bit_exact(grid_step):
     _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
 
 
+def test_stage_with_seven_targets_bit_exact():
+    """Seven sources: each decision phase lists 42 and 56 items (two rounds of a warp), a
+    direct-pass node up to 98, and the tap lattice holds eight planes."""
+    sc = scenes.workload("tiny", seed=9, n_sources=7)
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+
+
 def test_stage_with_a_wide_patch_bit_exact():
     """patch_radius 6: the wide retry's radius is 12 (25 x 25 taps), so border nodes read the
     tap lattice out to its full margin."""
