@@ -215,6 +215,15 @@ def test_stage_with_an_odd_grid_step_bit_exact(grid_step):
     _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
 
 
+def test_stage_two_view_full_size_bit_exact():
+    """The two-view workload at its full size (1040x780, one source at 25 mm, 64 planes,
+    minimum_support = best_view_count = 1): the whole stage against the oracle."""
+    sc = scenes.workload("two_view", seed=0)
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+    assert (dmap.provenance == abi.MEASURED).sum() > 0.3 * dmap.provenance.size
+
+
 def test_stage_with_seven_targets_bit_exact():
     """Seven sources: each decision phase lists 42 and 56 items (two rounds of a warp), a
     direct-pass node up to 98, and the tap lattice holds eight planes."""
