@@ -562,6 +562,7 @@ typedef struct chiaro_alignment_report {
     chiaro_align_level levels[CHIARO_ALIGN_MAX_LEVELS];
 } chiaro_alignment_report;
 
+/* AlignOptions::default() (align.rs:231-244), without the depth options. */
 void chiaro_align_options_default(chiaro_align_options *options);
 
 /* Replaces align_module / align_module_seeded (align.rs:281-519), called per module
