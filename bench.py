@@ -166,31 +166,13 @@ def stage_bytes(scene):
             "cost_taps": n * d * targets * taps, "cost_flop": 16 * n * d * targets * taps}
 
 
-def device_views(scene, torch, device):
-    """Upload luminance planes and warps; return (views, keepalive)."""
-    from chiaro_b200.abi import ViewC
-    from chiaro_b200.depth import pack_views
-    views, keep = pack_views(scene.inputs(), scene.alignments())
-    tensors = []
-    for i, (lum, w) in enumerate(zip(scene.luminance, scene.warps)):
-        tl = torch.from_numpy(lum.data.reshape(-1)).to(device)
-        tp = torch.from_numpy(w.points.reshape(-1)).to(device)
-        tc = torch.from_numpy(w.confidence.reshape(-1)).to(device)
-        tensors += [tl, tp, tc]
-        views[i].luminance = C.cast(C.c_void_p(tl.data_ptr()), C.POINTER(C.c_float))
-        views[i].warp.points = C.cast(C.c_void_p(tp.data_ptr()), C.POINTER(C.c_float))
-        views[i].warp.confidence = C.cast(C.c_void_p(tc.data_ptr()), C.POINTER(C.c_float))
-    return views, keep + tensors
-
-
 def run_ours(args, rank, world, local):
     import numpy as np
     import torch
     import torch.distributed as dist
 
-    from chiaro_b200 import abi, build, scenes
-    from chiaro_b200.abi import DepthMapC, DepthReportC, WarpC
-    from chiaro_b200.depth import refine_multiview_depth
+    from chiaro_b200 import build, scenes
+    from chiaro_b200.depth import DeviceStage, refine_multiview_depth
     from chiaro_b200.runtime import DepthContext
 
     device = torch.device("cuda", local)
@@ -201,31 +183,15 @@ def run_ours(args, rank, world, local):
     scene = scenes.workload(args.workload, seed=args.seed)
     work = stage_bytes(scene)
     ctx = DepthContext(local)
-    lib = ctx.lib
-    opt = scene.options.to_c()
     n = len(scene.cameras)
     M = work["fine_nodes"]
-    views, keep = device_views(scene, torch, device)
-    out_depth = torch.empty(M, dtype=torch.float64, device=device)
-    out_conf = torch.empty(M, dtype=torch.float32, device=device)
-    out_prov = torch.empty(M, dtype=torch.uint8, device=device)
-    dmap = DepthMapC(capacity=M, depth=C.cast(C.c_void_p(out_depth.data_ptr()), C.POINTER(C.c_double)),
-                     confidence=C.cast(C.c_void_p(out_conf.data_ptr()), C.POINTER(C.c_float)),
-                     provenance=C.cast(C.c_void_p(out_prov.data_ptr()), C.POINTER(C.c_uint8)))
-    refined = (WarpC * n)()
-    out_warps = []
-    for t in range(n):
-        pts = torch.empty(2 * M, dtype=torch.float32, device=device)
-        cf = torch.empty(M, dtype=torch.float32, device=device)
-        out_warps += [pts, cf]
-        refined[t].points = C.cast(C.c_void_p(pts.data_ptr()), C.POINTER(C.c_float))
-        refined[t].confidence = C.cast(C.c_void_p(cf.data_ptr()), C.POINTER(C.c_float))
-        refined[t].capacity = M
-    reports = (DepthReportC * n)()
+    # planes, warps and outputs resident in HBM: the device-buffer entry point
+    stage = DeviceStage(scene.inputs(), scene.reference_index, scene.alignments(), scene.options, context=ctx)
+    assert stage.nodes == M
 
     def step():
-        ctx.check(lib.chiaro_refine_multiview_depth_device(ctx.handle, views, n, scene.reference_index,
-                                                           C.byref(opt), refined, reports, C.byref(dmap)))
+        if not stage():
+            raise RuntimeError("the stage returned None on the benchmark workload")
 
     stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > 126 MB L2
@@ -288,8 +254,8 @@ def run_ours(args, rank, world, local):
     d2h = M * (8 + 4 + 1) + targets * M * (8 + 4)
     e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
 
-    graph = stage_graph(args, ctx, torch, stream, flush, step, [out_depth, out_conf, out_prov] + out_warps)
-    finest = finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap)
+    graph = stage_graph(args, torch, stream, flush, stage)
+    finest = finest_coarse_grid(args, scene, stage, torch, stream, flush)
     resolution = resolution_warp(args, scene, ctx)
     alignment = global_alignment(args, scene, ctx)
     quantised = quantised_sgm(args, scene, work, ctx, torch, device, stream, flush)
@@ -448,7 +414,7 @@ def global_alignment(args, scene, ctx):
             "inlier_ratio": round(r.inlier_ratio, 4), "gain": round(result.gain, 4)}
 
 
-def finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined, reports, dmap):
+def finest_coarse_grid(args, scene, stage, torch, stream, flush):
     """The workload at grid_step 4: the coarse grid (cost volume and SGM) at the direct grid's
     step, the finest the reference reaches (1041x781 nodes for 4160x3120, four times the
     default's cells). Same inputs, device buffers and timing as the main leg."""
@@ -456,12 +422,11 @@ def finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined
 
     options = dataclasses.replace(scene.options, grid_step=4)
     work = stage_bytes(dataclasses.replace(scene, options=options))
-    opt = options.to_c()
-    lib = ctx.lib
+    ctx = stage.ctx
 
     def step():
-        ctx.check(lib.chiaro_refine_multiview_depth_device(ctx.handle, views, n, scene.reference_index,
-                                                           C.byref(opt), refined, reports, C.byref(dmap)))
+        if not stage(options):
+            raise RuntimeError("the stage returned None at grid_step 4")
 
     for _ in range(max(args.warmup, 2)):
         step()
@@ -485,26 +450,28 @@ def finest_coarse_grid(args, scene, ctx, torch, stream, flush, views, n, refined
             "stage_ms": {k: round(statistics.median(s[k] for s in stages), 4) for k in stages[0]}}
 
 
-def stage_graph(args, ctx, torch, stream, flush, step, outputs):
-    """The whole stage replayed from its CUDA graph (chiaro_depth_set_stage_graph): the first
-    call launches, the second captures, the rest replay. The replay's outputs must equal the
-    launched stage's bit for bit before it is timed, with the same flush and events as the
-    main leg."""
-    lib = ctx.lib
+def stage_graph(args, torch, stream, flush, stage):
+    """The whole stage replayed from its CUDA graph (``DeviceStage(graph=True)``): the first
+    call launches, the second captures, the rest replay. The replay's outputs must equal
+    the launched stage's bit for bit before it is timed, with the same flush and events as
+    the main leg."""
+    outputs = [stage.depth, stage.confidence, stage.provenance] + \
+        [x for t in stage.targets for x in (stage.points[t], stage.point_confidence[t])]
 
     def snapshot():
         return [t.clone() for t in outputs]
 
-    step()
+    stage.graph = False
+    stage()
     plain = snapshot()
-    ctx.check(lib.chiaro_depth_set_stage_graph(ctx.handle, 1))
+    stage.graph = True
     try:
         states = []
         for _ in range(3):
             for t in outputs:
                 t.zero_()
-            step()
-            states.append(lib.chiaro_depth_stage_graph_state(ctx.handle))
+            stage()
+            states.append(stage.graph_state)
         torch.cuda.synchronize()
         identical = all(torch.equal(a.view(torch.uint8), b.view(torch.uint8)) for a, b in zip(plain, snapshot()))
         if not identical or states != [0, 1, 2]:
@@ -516,15 +483,15 @@ def stage_graph(args, ctx, torch, stream, flush, step, outputs):
                 flush.zero_()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-            step()
+            stage()
             with torch.cuda.stream(stream):
                 e1.record(stream)
             e1.synchronize()
             total += e0.elapsed_time(e1)
-        replayed = lib.chiaro_depth_stage_graph_state(ctx.handle) == 2
+        replayed = stage.graph_state == 2
     finally:
-        ctx.check(lib.chiaro_depth_set_stage_graph(ctx.handle, 0))
-    return {"ms_per_step": round(total / steps, 3), "launches_per_step": ctx.launches(),
+        stage.graph = False
+    return {"ms_per_step": round(total / steps, 3), "launches_per_step": stage.ctx.launches(),
             "bit_identical_to_launched": True, "replayed": replayed,
             "note": "one cudaGraphLaunch per call on unchanged views, options and buffers"}
 

@@ -1801,6 +1801,7 @@ int chiaro_depth_set_stage_graph(chiaro_depth_ctx *ctx, int32_t enabled) {
     if (!ctx) return CHIARO_ERR_ARGUMENT;
     try {
         CK(cudaSetDevice(ctx->device));
+        if ((enabled != 0) == (ctx->stage_graph != 0)) return CHIARO_OK;  // unchanged: keep the graph
         ctx->stage_graph = enabled != 0;
         if (!ctx->stage_graph && ctx->stage_exec) {
             CK(cudaStreamSynchronize(ctx->stream));

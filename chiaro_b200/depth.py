@@ -335,3 +335,115 @@ def refine_multiview_depth(inputs: Sequence, reference_index: int, alignments: S
             alignments[t].report.depth = DepthAlignmentReport.from_c(reports[t])
     return DenseDepthMap(int(dmap.columns), int(dmap.rows), int(dmap.step), float(dmap.near_depth),
                          float(dmap.far_depth), depth, confidence, provenance)
+
+
+class DeviceStage:
+    """refine_multiview_depth (depth.rs:312-580) on device buffers, for callers that keep
+    frames resident in HBM (``chiaro_refine_multiview_depth_device``).
+
+    The luminance planes and warps of ``inputs`` / ``alignments`` are copied once into CUDA
+    tensors on the context's device (``planes[i]``, ``warp_points[i]``,
+    ``warp_confidence[i]``); a new frame is written into those tensors in place. Each call
+    runs the stage on what they hold and writes the outputs this object owns: ``depth``
+    (f64), ``confidence`` (f32) and ``provenance`` (u8) over the M output nodes, and for
+    each target t (accepted, calibrated, not the reference) ``points[t]`` (f32 [M, 2]) and
+    ``point_confidence[t]`` (f32 [M]); ``reports[t]`` is the stage's report of target t.
+    The call returns False where the reference returns None.
+
+    ``graph=True`` enables the whole-stage CUDA graph: with unchanged views, options and
+    buffers the first call launches the stage's kernels, the second captures them and
+    later calls replay the graph (``graph_state``: 0, 1, 2).
+
+    A call waits on the device for torch's current stream and returns when its outputs
+    are complete.
+    """
+
+    def __init__(self, inputs: Sequence, reference_index: int, alignments: Sequence, options: DepthOptions,
+                 context=None, graph: bool = False):
+        import torch
+
+        from .runtime import default_context
+
+        if len(inputs) != len(alignments):
+            raise ValueError("inputs and alignments differ in length")
+        self.ctx = context if context is not None else default_context()
+        self.reference_index = reference_index
+        self.options = options
+        device = torch.device("cuda", self.ctx.device)
+        n = len(inputs)
+        self.views, self._keep = pack_views(inputs, alignments)
+        self.planes, self.warp_points, self.warp_confidence = [], [], []
+        for i, (inp, al) in enumerate(zip(inputs, alignments)):
+            plane = torch.from_numpy(np.ascontiguousarray(inp.luminance.data, dtype=np.float32).reshape(-1))
+            points = torch.from_numpy(np.ascontiguousarray(al.warp.points, dtype=np.float32).reshape(-1))
+            conf = torch.from_numpy(np.ascontiguousarray(al.warp.confidence, dtype=np.float32).reshape(-1))
+            plane, points, conf = plane.to(device), points.to(device), conf.to(device)
+            self.planes.append(plane)
+            self.warp_points.append(points)
+            self.warp_confidence.append(conf)
+            self.views[i].luminance = C.cast(C.c_void_p(plane.data_ptr()), C.POINTER(C.c_float))
+            self.views[i].warp.points = C.cast(C.c_void_p(points.data_ptr()), C.POINTER(C.c_float))
+            self.views[i].warp.confidence = C.cast(C.c_void_p(conf.data_ptr()), C.POINTER(C.c_float))
+        self._keep = None  # the host copies are no longer referenced by the views
+        ref = inputs[reference_index]
+        (columns, rows, _), _ = output_shape(ref.width, ref.height, options)
+        self.shape = (ref.width, ref.height)
+        self.nodes = m = columns * rows
+        self.depth = torch.empty(m, dtype=torch.float64, device=device)
+        self.confidence = torch.empty(m, dtype=torch.float32, device=device)
+        self.provenance = torch.empty(m, dtype=torch.uint8, device=device)
+        self.map = DepthMapC(capacity=m, depth=C.cast(C.c_void_p(self.depth.data_ptr()), C.POINTER(C.c_double)),
+                             confidence=C.cast(C.c_void_p(self.confidence.data_ptr()), C.POINTER(C.c_float)),
+                             provenance=C.cast(C.c_void_p(self.provenance.data_ptr()), C.POINTER(C.c_uint8)))
+        self.targets = [t for t in range(n) if t != reference_index and inputs[t].camera is not None
+                        and alignments[t].report.accepted]
+        self.refined = (WarpC * n)()
+        self.points: List = [None] * n
+        self.point_confidence: List = [None] * n
+        for t in self.targets:
+            self.points[t] = torch.empty((m, 2), dtype=torch.float32, device=device)
+            self.point_confidence[t] = torch.empty(m, dtype=torch.float32, device=device)
+            self.refined[t].points = C.cast(C.c_void_p(self.points[t].data_ptr()), C.POINTER(C.c_float))
+            self.refined[t].confidence = C.cast(C.c_void_p(self.point_confidence[t].data_ptr()),
+                                                C.POINTER(C.c_float))
+            self.refined[t].capacity = m
+        self.reports = (DepthReportC * n)()
+        # the library's stream, which waits for torch's current stream before each call, so
+        # that plane writes queued there are seen
+        self.stream = torch.cuda.ExternalStream(self.ctx.stream_handle(), device=device)
+        self._device = device
+        self.graph = graph
+
+    @property
+    def graph(self) -> bool:
+        return self._graph
+
+    @graph.setter
+    def graph(self, enabled: bool):
+        self.ctx.check(self.ctx.lib.chiaro_depth_set_stage_graph(self.ctx.handle, 1 if enabled else 0))
+        self._graph = bool(enabled)
+
+    @property
+    def graph_state(self) -> int:
+        """What the last call did: 0 launched its kernels, 1 captured the graph, 2 replayed it."""
+        return int(self.ctx.lib.chiaro_depth_stage_graph_state(self.ctx.handle))
+
+    def __call__(self, options: Optional[DepthOptions] = None) -> bool:
+        """Run the stage (with ``options`` instead of the constructor's, if given; they must
+        give the same output grid)."""
+        options = self.options if options is None else options
+        (columns, rows, _), _ = output_shape(self.shape[0], self.shape[1], options)
+        if columns * rows != self.nodes:
+            raise ValueError("options change the output grid")
+        import torch
+
+        self.ctx.check(self.ctx.lib.chiaro_depth_set_stage_graph(self.ctx.handle, 1 if self._graph else 0))
+        self.stream.wait_stream(torch.cuda.current_stream(self._device))
+        opt = options.to_c()
+        status = self.ctx.lib.chiaro_refine_multiview_depth_device(
+            self.ctx.handle, self.views, len(self.planes), self.reference_index, C.byref(opt), self.refined,
+            self.reports, C.byref(self.map))
+        if status == abi.INVALID:
+            return False
+        self.ctx.check(status)
+        return True

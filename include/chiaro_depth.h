@@ -258,11 +258,13 @@ int chiaro_refine_multiview_depth_device(chiaro_depth_ctx *ctx,
  * the reference; off by default). When enabled, a device-buffer call whose views
  * (pointers, sizes, flags, cameras), reference, options and output pointers equal the
  * previous call's is captured into a graph on its second occurrence and replayed from
- * the third on: the stage's ~50 launches become one, and a replay reads the current
+ * the third on: the stage's ~35 launches become one, and a replay reads the current
  * contents of the same buffers. Any other call, or any buffer the context reallocates
  * (another entry point on a larger size, for instance), voids the graph and the next
  * calls run, capture and replay afresh. Calls with debug arrays or host buffers never
- * use it. The first call of a key should not come during another stream capture. */
+ * use it. The first call of a key should not come during another stream capture.
+ * Switching it off drops the graph and switching it on starts afresh; setting the
+ * current value again changes nothing. */
 int chiaro_depth_set_stage_graph(chiaro_depth_ctx *ctx, int32_t enabled);
 /* What the last device-buffer stage call did: 0 launched its kernels, 1 captured and
  * launched the graph, 2 replayed it. */

@@ -1,8 +1,8 @@
-"""The whole-stage CUDA graph of chiaro_refine_multiview_depth_device: launched, then
-captured, then replayed, each call bit-identical to the stage without it; a replay
-reads new data from the same buffers, and a new key or a reallocated buffer starts
-over."""
-import ctypes as C
+"""The device-buffer stage (chiaro_b200.depth.DeviceStage over
+chiaro_refine_multiview_depth_device) and its whole-stage CUDA graph: the same bits as the
+host-buffer API; launched, then captured, then replayed, each call bit-identical to the
+stage without the graph; a replay reads new planes written into the same buffers, and a
+new key or a reallocated buffer starts over."""
 import dataclasses
 
 import numpy as np
@@ -10,62 +10,27 @@ import pytest
 import torch
 
 from chiaro_b200 import scenes
-from chiaro_b200.abi import DepthMapC, DepthReportC, WarpC
-from chiaro_b200.depth import output_shape, pack_views
+from chiaro_b200.depth import DeviceStage, refine_multiview_depth
 
 pytestmark = pytest.mark.gpu
 
 
-class DeviceStage:
-    """A scene's inputs and the stage's outputs in device memory, called through the ABI."""
+def _stage(ctx, name, seed):
+    sc = scenes.workload(name, seed=seed)
+    return DeviceStage(sc.inputs(), sc.reference_index, sc.alignments(), sc.options, context=ctx)
 
-    def __init__(self, ctx, scene, options=None):
-        self.ctx, self.scene = ctx, scene
-        self.options = options or scene.options
-        self.views, keep = pack_views(scene.inputs(), scene.alignments())
-        self.keep = keep
-        self.planes = []
-        for i, (lum, w) in enumerate(zip(scene.luminance, scene.warps)):
-            tl = torch.from_numpy(lum.data.reshape(-1).copy()).cuda()
-            tp = torch.from_numpy(w.points.reshape(-1).copy()).cuda()
-            tc = torch.from_numpy(w.confidence.reshape(-1).copy()).cuda()
-            self.planes.append(tl)
-            self.keep += [tp, tc]
-            self.views[i].luminance = C.cast(C.c_void_p(tl.data_ptr()), C.POINTER(C.c_float))
-            self.views[i].warp.points = C.cast(C.c_void_p(tp.data_ptr()), C.POINTER(C.c_float))
-            self.views[i].warp.confidence = C.cast(C.c_void_p(tc.data_ptr()), C.POINTER(C.c_float))
-        (cols, rows, _), _ = output_shape(scene.width, scene.height, self.options)
-        self.M = M = cols * rows
-        self.n = n = len(scene.cameras)
-        self.depth = torch.empty(M, dtype=torch.float64, device="cuda")
-        self.conf = torch.empty(M, dtype=torch.float32, device="cuda")
-        self.prov = torch.empty(M, dtype=torch.uint8, device="cuda")
-        self.dmap = DepthMapC(capacity=M, depth=C.cast(C.c_void_p(self.depth.data_ptr()), C.POINTER(C.c_double)),
-                              confidence=C.cast(C.c_void_p(self.conf.data_ptr()), C.POINTER(C.c_float)),
-                              provenance=C.cast(C.c_void_p(self.prov.data_ptr()), C.POINTER(C.c_uint8)))
-        self.refined = (WarpC * n)()
-        self.warps = []
-        for t in range(n):
-            pts = torch.empty(2 * M, dtype=torch.float32, device="cuda")
-            cf = torch.empty(M, dtype=torch.float32, device="cuda")
-            self.warps += [pts, cf]
-            self.refined[t].points = C.cast(C.c_void_p(pts.data_ptr()), C.POINTER(C.c_float))
-            self.refined[t].confidence = C.cast(C.c_void_p(cf.data_ptr()), C.POINTER(C.c_float))
-            self.refined[t].capacity = M
-        self.reports = (DepthReportC * n)()
 
-    def run(self):
-        opt = self.options.to_c()
-        for w in self.warps:
-            w.fill_(float("nan"))
-        self.depth.fill_(-1.0)
-        self.ctx.check(self.ctx.lib.chiaro_refine_multiview_depth_device(
-            self.ctx.handle, self.views, self.n, self.scene.reference_index, C.byref(opt), self.refined,
-            self.reports, C.byref(self.dmap)))
-        outputs = [self.depth.cpu().numpy().view(np.uint64), self.conf.cpu().numpy().view(np.uint32),
-                   self.prov.cpu().numpy()] + [w.cpu().numpy().view(np.uint32) for w in self.warps]
-        reports = [bytes(r) for r in self.reports]
-        return outputs, reports, self.ctx.lib.chiaro_depth_stage_graph_state(self.ctx.handle)
+def _run(stage, options=None):
+    for t in stage.targets:
+        stage.points[t].fill_(float("nan"))
+    stage.depth.fill_(-1.0)
+    assert stage(options)
+    outputs = [stage.depth.cpu().numpy().view(np.uint64), stage.confidence.cpu().numpy().view(np.uint32),
+               stage.provenance.cpu().numpy()]
+    for t in stage.targets:
+        outputs += [stage.points[t].cpu().numpy().reshape(-1).view(np.uint32),
+                    stage.point_confidence[t].cpu().numpy().view(np.uint32)]
+    return outputs, [bytes(r) for r in stage.reports], stage.graph_state
 
 
 def _same(a, b):
@@ -73,43 +38,69 @@ def _same(a, b):
     assert a[1] == b[1]
 
 
+def test_device_stage_matches_the_host_api(gpu_ctx):
+    sc = scenes.workload("small", seed=2)
+    stage = DeviceStage(sc.inputs(), sc.reference_index, sc.alignments(), sc.options, context=gpu_ctx)
+    outputs, _, _ = _run(stage)
+    alignments = sc.alignments()
+    dmap = refine_multiview_depth(sc.inputs(), sc.reference_index, alignments, sc.options, context=gpu_ctx)
+    assert np.array_equal(outputs[0], dmap.depth.view(np.uint64))
+    assert np.array_equal(outputs[1], dmap.confidence.view(np.uint32))
+    assert np.array_equal(outputs[2], dmap.provenance)
+    for k, t in enumerate(stage.targets):
+        assert np.array_equal(outputs[3 + 2 * k], alignments[t].warp.points.reshape(-1).view(np.uint32))
+        assert np.array_equal(outputs[4 + 2 * k], alignments[t].warp.confidence.view(np.uint32))
+
+
+def test_setting_the_same_graph_state_keeps_the_graph(gpu_ctx):
+    stage = _stage(gpu_ctx, "tiny", 1)
+    stage.graph = True
+    try:
+        states = []
+        for _ in range(3):
+            stage.graph = True  # every call sets it again
+            states.append(_run(stage)[2])
+        assert states == [0, 1, 2]
+    finally:
+        stage.graph = False
+
+
 def test_stage_graph_captures_replays_and_starts_over(gpu_ctx):
     lib, h = gpu_ctx.lib, gpu_ctx.handle
-    stage = DeviceStage(gpu_ctx, scenes.workload("small", seed=3))
-    gpu_ctx.check(lib.chiaro_depth_set_stage_graph(h, 0))
-    plain = stage.run()
+    stage = _stage(gpu_ctx, "small", 3)
+    plain = _run(stage)
     assert plain[2] == 0
-    gpu_ctx.check(lib.chiaro_depth_set_stage_graph(h, 1))
+    stage.graph = True
     try:
         states = []
         for _ in range(4):
-            r = stage.run()
+            r = _run(stage)
             _same(r, plain)
             states.append(r[2])
         assert states == [0, 1, 2, 2]
         # new data in the same buffers: a replay reads it
         other = scenes.workload("small", seed=4)
-        for tl, lum in zip(stage.planes, other.luminance):
-            tl.copy_(torch.from_numpy(lum.data.reshape(-1).copy()))
-        replayed = stage.run()
+        for plane, lum in zip(stage.planes, other.luminance):
+            plane.copy_(torch.from_numpy(lum.data.reshape(-1).copy()))
+        replayed = _run(stage)
         assert replayed[2] == 2
-        gpu_ctx.check(lib.chiaro_depth_set_stage_graph(h, 0))
-        fresh = stage.run()
+        stage.graph = False
+        fresh = _run(stage)
         _same(replayed, fresh)
         assert not all(np.array_equal(x, y) for x, y in zip(replayed[0], plain[0]))
-        gpu_ctx.check(lib.chiaro_depth_set_stage_graph(h, 1))
+        stage.graph = True
         # other options: a new key
         stage.options = dataclasses.replace(stage.options, minimum_score=stage.options.minimum_score + 0.05)
-        assert [stage.run()[2] for _ in range(3)] == [0, 1, 2]
+        assert [_run(stage)[2] for _ in range(3)] == [0, 1, 2]
         # a buffer the graph uses reallocated by another entry point voids it
         big = torch.rand(600 * 500 * 129, device="cuda")
         guide = torch.rand(600 * 500, device="cuda")
         out = torch.empty_like(big)
         gpu_ctx.check(lib.chiaro_sgm_aggregate_device(h, big.data_ptr(), guide.data_ptr(), 600, 500, 129,
                                                       out.data_ptr()))
-        after = stage.run()
+        after = _run(stage)
         assert after[2] == 0
-        gpu_ctx.check(lib.chiaro_depth_set_stage_graph(h, 0))
-        _same(after, stage.run())
+        stage.graph = False
+        _same(after, _run(stage))
     finally:
-        gpu_ctx.check(lib.chiaro_depth_set_stage_graph(h, 0))
+        stage.graph = False
