@@ -371,7 +371,9 @@ class DeviceStage:
         self.options = options
         device = torch.device("cuda", self.ctx.device)
         n = len(inputs)
-        self.views, self._keep = pack_views(inputs, alignments)
+        # the views' host pointers are replaced by device ones below, so the host copies
+        # pack_views keeps alive are not needed past this point
+        self.views, _ = pack_views(inputs, alignments)
         self.planes, self.warp_points, self.warp_confidence = [], [], []
         for i, (inp, al) in enumerate(zip(inputs, alignments)):
             plane = torch.from_numpy(np.ascontiguousarray(inp.luminance.data, dtype=np.float32).reshape(-1))
@@ -384,7 +386,6 @@ class DeviceStage:
             self.views[i].luminance = C.cast(C.c_void_p(plane.data_ptr()), C.POINTER(C.c_float))
             self.views[i].warp.points = C.cast(C.c_void_p(points.data_ptr()), C.POINTER(C.c_float))
             self.views[i].warp.confidence = C.cast(C.c_void_p(conf.data_ptr()), C.POINTER(C.c_float))
-        self._keep = None  # the host copies are no longer referenced by the views
         ref = inputs[reference_index]
         (columns, rows, _), _ = output_shape(ref.width, ref.height, options)
         self.shape = (ref.width, ref.height)
