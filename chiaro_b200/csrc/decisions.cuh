@@ -104,28 +104,67 @@ __device__ __forceinline__ int list_items(const DecisionSlot &d, int count, bool
     return count + __popc(mask);
 }
 
+// Scores the pooled lists of the CTA's nodes (node k's count[k] entries of its
+// d.list / d.disp, node after node), so the lanes of all warps share the
+// correlations of one phase. Phase 1 items are (target, offset k < 5 or baseline
+// k = 5), phase 2 items (target, shift j < 8). A failed correlation of an offset
+// or shift marks its target's refinement as failed.
+__device__ inline void decision_pool_scores(const DecisionParams &p, unsigned char *smem_raw, size_t slot_bytes,
+                                            const RefPatch *patches, const int *count, int nodes, int taps,
+                                            bool shifts) {
+    const int V = p.n_targets;
+    int pooled = 0;
+    for (int k = 0; k < nodes; ++k) pooled += count[k];
+    for (int j = threadIdx.x; j < pooled; j += blockDim.x) {
+        int k = 0, at = j;
+        while (at >= count[k]) at -= count[k++];
+        const DecisionSlot d = carve_decision_slot(smem_raw + (size_t)k * slot_bytes, V, taps);
+        const int item = d.list[at];
+        const int v = shifts ? item >> 3 : item / 6;
+        const DevView &tv = p.views[p.targets[v]];
+        const double2 dd = d.disp[at];
+        float score;
+        const bool ok = zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patches[k], taps,
+                                 dd.x, dd.y, score);
+        const int kk = shifts ? 6 + (item & 7) : item - v * 6;
+        if (ok)
+            d.sc[v * 16 + kk] = score;
+        else if (shifts || kk < 5)
+            atomicOr(&d.flags[v], 1);
+    }
+}
+
 // A warp per fine node, every target (depth.rs:420-485 with refine_one_view,
 // depth.rs:1634-1708). Each phase first settles which correlations run, lists
 // them, and runs the list from one call site, so the lanes stay converged.
+// POOLED (for one or two targets, whose phases list at most 12 and 16 items per
+// node): the CTA scores the pooled lists of all its nodes instead, so few warps
+// issue each phase's correlations; nodes without work stay for the CTA's
+// barriers.
+template <bool POOLED>
 __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(DecisionParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patches[DECISION_WARPS];
+    __shared__ int count[DECISION_WARPS];
     const unsigned full = 0xffffffffu;
     const int slot = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int node = blockIdx.x * (blockDim.x >> 5) + slot;
-    if (node >= p.columns * p.rows) return;  // whole warp
+    const int nodes = blockDim.x >> 5;
+    const int node = blockIdx.x * nodes + slot;
+    const bool in_grid = node < p.columns * p.rows;  // whole warp
+    if (!POOLED && !in_grid) return;
     const int V = p.n_targets;
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
-    DecisionSlot d = carve_decision_slot(smem_raw + (size_t)slot * decision_slot_bytes(V, taps), V, taps);
+    const size_t slot_bytes = decision_slot_bytes(V, taps);
+    DecisionSlot d = carve_decision_slot(smem_raw + (size_t)slot * slot_bytes, V, taps);
     RefPatch &patch = patches[slot];
     const DevView &rv = p.views[p.reference];
     const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
-    const bool has = p.field.has[node];
+    const bool has = in_grid && p.field.has[node];
     // the global warp at the node: Undefined, or Global without a depth (depth.rs:433-440);
     // lane v holds target v's mapping
     unsigned defined = 0u;
     float2 gq = make_float2(0.0f, 0.0f);
-    if (lane < V) {
+    if (in_grid && lane < V) {
         float gx = 0.0f, gy = 0.0f;
         const bool ok = warp_map(p.views[p.targets[lane]].warp, (float)cx, (float)cy, gx, gy);
         gq = make_float2(gx, gy);
@@ -135,16 +174,19 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
         d.flags[lane] = 0;
     }
     defined = __reduce_or_sync(full, defined);
-    if (!has || !defined) return;  // whole warp
-    const unsigned undefined_taps = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, p.radius,
-                                                     p.spatial, d.rr, d.wt, d.gh, d.box, patch, p.lattice);
-    const bool patch_ok = patch.ok;
+    const bool active = has && defined;  // whole warp
+    if (!POOLED && !active) return;
+    unsigned undefined_taps = 0u;
+    if (active)
+        undefined_taps = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, p.radius, p.spatial, d.rr,
+                                          d.wt, d.gh, d.box, patch, p.lattice);
+    const bool patch_ok = active && patch.ok;
     const D3 origin = camera_origin(rv.cam);
-    const double shared_inverse = 1.0 / p.field.depth[node];
+    const double shared_inverse = active ? 1.0 / p.field.depth[node] : 0.0;
     const double min_inverse = 1.0 / p.far_depth, max_inverse = 1.0 / p.near_depth;
     // phase 1: per target, five inverse-depth offsets (k < 5) and the baseline (k = 5)
     int listed = 0;
-    for (int base = 0; base < 6 * V; base += 32) {
+    for (int base = 0; active && base < 6 * V; base += 32) {
         const int item = base + lane;
         const int v = item / 6, k = item - v * 6;
         const int vs = v < V ? v : 0;
@@ -180,23 +222,30 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
         }
         listed = list_items(d, listed, zncc, item, ddx, ddy);
     }
-    __syncwarp();
-    for (int j = lane; j < listed; j += 32) {
-        const int item = d.list[j];
-        const int v = item / 6, k = item - v * 6;
-        const DevView &tv = p.views[p.targets[v]];
-        const double2 dd = d.disp[j];
-        float score;
-        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, dd.x, dd.y,
-                     score))
-            d.sc[v * 16 + k] = score;
-        else if (k < 5)
-            atomicOr(&d.flags[v], 1);
+    if constexpr (POOLED) {
+        if (lane == 0) count[slot] = listed;
+        __syncthreads();
+        decision_pool_scores(p, smem_raw, slot_bytes, patches, count, nodes, taps, false);
+        __syncthreads();
+    } else {
+        __syncwarp();
+        for (int j = lane; j < listed; j += 32) {
+            const int item = d.list[j];
+            const int v = item / 6, k = item - v * 6;
+            const DevView &tv = p.views[p.targets[v]];
+            const double2 dd = d.disp[j];
+            float score;
+            if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, dd.x, dd.y,
+                         score))
+                d.sc[v * 16 + k] = score;
+            else if (k < 5)
+                atomicOr(&d.flags[v], 1);
+        }
+        __syncwarp();
     }
-    __syncwarp();
     // best offset per target: in order, strict improvement
-    const unsigned failed = __ballot_sync(full, lane < V && d.flags[lane < V ? lane : 0]);
-    if (lane < V && ((defined >> lane) & 1u) && !((failed >> lane) & 1u)) {
+    const unsigned failed = __ballot_sync(full, active && lane < V && d.flags[lane < V ? lane : 0]);
+    if (active && lane < V && ((defined >> lane) & 1u) && !((failed >> lane) & 1u)) {
         float *sc = d.sc + lane * 16;
         float2 *pts = d.pts + lane * 16;
         float best_objective = 0.0f;
@@ -212,7 +261,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
     __syncwarp();
     // phase 2: per target, eight residual shifts (dy outer, dx inner, centre skipped)
     listed = 0;
-    for (int base = 0; base < 8 * V; base += 32) {
+    for (int base = 0; active && base < 8 * V; base += 32) {
         const int item = base + lane;
         const int v = item >> 3, j = item & 7;
         const int vs = v < V ? v : 0;
@@ -233,22 +282,30 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
         }
         listed = list_items(d, listed, zncc, item, ddx, ddy);
     }
-    __syncwarp();
-    for (int j = lane; j < listed; j += 32) {
-        const int item = d.list[j];
-        const int v = item >> 3;
-        const DevView &tv = p.views[p.targets[v]];
-        const double2 dd = d.disp[j];
-        float score;
-        if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, dd.x, dd.y,
-                     score))
-            d.sc[v * 16 + 6 + (item & 7)] = score;
-        else
-            atomicOr(&d.flags[v], 1);
+    if constexpr (POOLED) {
+        __syncwarp();
+        if (lane == 0) count[slot] = listed;
+        __syncthreads();
+        decision_pool_scores(p, smem_raw, slot_bytes, patches, count, nodes, taps, true);
+        __syncthreads();
+    } else {
+        __syncwarp();
+        for (int j = lane; j < listed; j += 32) {
+            const int item = d.list[j];
+            const int v = item >> 3;
+            const DevView &tv = p.views[p.targets[v]];
+            const double2 dd = d.disp[j];
+            float score;
+            if (zncc_any(TargetRef{tv.luma, tv.quads}, d.gh + v * taps, d.box[v], d.wt, patch, taps, dd.x, dd.y,
+                         score))
+                d.sc[v * 16 + 6 + (item & 7)] = score;
+            else
+                atomicOr(&d.flags[v], 1);
+        }
+        __syncwarp();
     }
-    __syncwarp();
     // classification (depth.rs:458-485), lane v for target v
-    if (lane >= V || !((defined >> lane) & 1u)) return;
+    if (!active || lane >= V || !((defined >> lane) & 1u)) return;
     const Decisions o = p.out[lane];
     const float *sc = d.sc + lane * 16;
     const float2 *pts = d.pts + lane * 16;

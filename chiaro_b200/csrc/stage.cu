@@ -190,7 +190,8 @@ void set_smem_limits() {
     CK(cudaFuncSetAttribute(cost_volume_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(direct_depth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(direct_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    CK(cudaFuncSetAttribute(target_decision_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(target_decision_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(target_decision_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(align_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done_devices.push_back(device);
 }
@@ -1479,8 +1480,11 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         int taps = (2 * radius + 1) * (2 * radius + 1);
         const size_t slot = decision_slot_bytes(V, taps);
         if (slot > 200 * 1024) throw CudaError{cudaErrorInvalidValue, "decision shared memory exceeds 200 KiB"};
-        const int warps = warps_per_cta(target_decision_kernel, slot, DECISION_WARPS);
-        target_decision_kernel<<<blocks_for(M, warps), 32 * warps, warps * slot, s>>>(p);
+        // one or two targets leave most lanes of a node's warp idle in both phases (6 V and
+        // 8 V items): the CTA then pools its nodes' correlations
+        const auto decision_kernel = V <= 2 ? target_decision_kernel<true> : target_decision_kernel<false>;
+        const int warps = warps_per_cta(decision_kernel, slot, DECISION_WARPS);
+        decision_kernel<<<blocks_for(M, warps), 32 * warps, warps * slot, s>>>(p);
         CK(cudaGetLastError());
         Decisions dec2 = decision_bufs(ctx, "dec_consensus", M), dec3 = decision_bufs(ctx, "dec_boundary", M);
         for (int v = 0; v < V; ++v) {
