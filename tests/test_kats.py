@@ -5,7 +5,7 @@ Each test restates one of the reference's own unit tests for the depth path
 geometry.rs:367-393, math.rs:141-160) and runs it against the CPU oracle and,
 where the operator exists on the device, against the CUDA library too. These
 pin the oracle: it must reproduce every known answer the reference's tests
-hold before it may judge the GPU.
+hold before it may serve as the GPU path's checker.
 """
 import ctypes as C
 
