@@ -98,11 +98,15 @@ __global__ void components_union_kernel(const uint8_t *__restrict__ has, const d
     }
 }
 
+// Component sizes: the lanes of a warp that share a root add their count with one
+// atomic (a large component would otherwise serialise one atomic per node on its root).
 __global__ void components_size_kernel(const uint8_t *__restrict__ has, int *parent, int *size, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !has[i]) return;
+    const unsigned active = __activemask();
     int root = uf_find(parent, i);
-    atomicAdd(size + root, 1);
+    const unsigned peers = __match_any_sync(active, root);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(size + root, __popc(peers));
 }
 
 __global__ void components_mark_kernel(const uint8_t *__restrict__ src_has, int *parent, const int *__restrict__ size,
