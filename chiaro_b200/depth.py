@@ -347,7 +347,7 @@ class DeviceStage:
     runs the stage on what they hold and writes the outputs this object owns: ``depth``
     (f64), ``confidence`` (f32) and ``provenance`` (u8) over the M output nodes, and for
     each target t (accepted, calibrated, not the reference) ``points[t]`` (f32 [M, 2]) and
-    ``point_confidence[t]`` (f32 [M]); ``reports[t]`` is the stage's report of target t.
+    ``point_confidence[t]`` (f32 [M]); ``report(t)`` is the stage's report of target t.
     The call returns False where the reference returns None.
 
     ``graph=True`` enables the whole-stage CUDA graph: with unchanged views, options and
@@ -423,6 +423,12 @@ class DeviceStage:
     def graph(self, enabled: bool):
         self.ctx.check(self.ctx.lib.chiaro_depth_set_stage_graph(self.ctx.handle, 1 if enabled else 0))
         self._graph = bool(enabled)
+
+    def report(self, t: int) -> Optional[DepthAlignmentReport]:
+        """The last call's report of module t (the reference's ``report.depth``), or None
+        when the call did not rewrite t."""
+        r = self.reports[t]
+        return DepthAlignmentReport.from_c(r) if r.present else None
 
     @property
     def graph_state(self) -> int:

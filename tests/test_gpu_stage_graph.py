@@ -50,6 +50,8 @@ def test_device_stage_matches_the_host_api(gpu_ctx):
     for k, t in enumerate(stage.targets):
         assert np.array_equal(outputs[3 + 2 * k], alignments[t].warp.points.reshape(-1).view(np.uint32))
         assert np.array_equal(outputs[4 + 2 * k], alignments[t].warp.confidence.view(np.uint32))
+        assert stage.report(t) == alignments[t].report.depth
+    assert stage.report(sc.reference_index) is None
 
 
 def test_setting_the_same_graph_state_keeps_the_graph(gpu_ctx):
