@@ -41,10 +41,12 @@ __global__ void reject_isolated_kernel(const uint8_t *__restrict__ src_has, cons
 }
 
 // ---- connected components ------------------------------------------------------
+// parent[] is read through L2 (__ldcg), where the atomicCAS of uf_union resolves: a
+// thread never retries a union on a stale L1 copy of a root it has just lost.
 __device__ inline int uf_find(int *parent, int x) {
-    int p = parent[x];
+    int p = __ldcg(parent + x);
     while (p != x) {
-        int gp = parent[p];
+        int gp = __ldcg(parent + p);
         if (gp != p) parent[x] = gp;  // path halving (benign races: any ancestor is a valid parent)
         x = p;
         p = gp;
@@ -52,8 +54,16 @@ __device__ inline int uf_find(int *parent, int x) {
     return x;
 }
 
-__device__ inline void uf_union(int *parent, int a, int b) {
-    for (int guard = 0; guard < (1 << 20); ++guard) {
+// Bit set in the status word when a union gave up (UNION_GAVE_UP): the host turns it
+// into CHIARO_ERR_TIMEOUT instead of returning components with an edge left out.
+constexpr int UNION_GAVE_UP = 1;
+
+// Lock-free union. Each failed compare-and-swap means another thread attached root b,
+// and at most n - 1 attachments happen in all, so with retries >= n the loop always
+// ends by joining or finding a == b; a smaller bound (a caller's choice) can run out,
+// which is reported, never silent.
+__device__ inline void uf_union(int *parent, int a, int b, int retries, int *status) {
+    for (int attempt = 0; attempt < retries; ++attempt) {
         a = uf_find(parent, a);
         b = uf_find(parent, b);
         if (a == b) return;
@@ -66,6 +76,7 @@ __device__ inline void uf_union(int *parent, int a, int b) {
         int old = atomicCAS(parent + b, b, a);
         if (old == b) return;
     }
+    atomicOr(status, UNION_GAVE_UP);
 }
 
 __device__ inline bool component_edge(const uint8_t *has, const double *depth, const float *guidance, int i, int j,
@@ -85,7 +96,7 @@ __global__ void components_init_kernel(int *parent, int n) {
 // (together with the mirrored pairs this covers all eight directions).
 __global__ void components_union_kernel(const uint8_t *__restrict__ has, const double *__restrict__ depth,
                                         const float *__restrict__ guidance, int *parent, int columns, int rows,
-                                        double tolerance) {
+                                        double tolerance, int retries, int *status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= columns * rows || !has[i]) return;
     int column = i % columns, row = i / columns;
@@ -94,7 +105,7 @@ __global__ void components_union_kernel(const uint8_t *__restrict__ has, const d
         int x = column + off[k][0], y = row + off[k][1];
         if (x < 0 || y < 0 || x >= columns || y >= rows) continue;
         int j = y * columns + x;
-        if (component_edge(has, depth, guidance, i, j, tolerance)) uf_union(parent, i, j);
+        if (component_edge(has, depth, guidance, i, j, tolerance)) uf_union(parent, i, j, retries, status);
     }
 }
 

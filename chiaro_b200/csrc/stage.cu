@@ -64,6 +64,11 @@ struct chiaro_depth_ctx {
     int stage_graph_state = 0;  // last call: 0 launched, 1 captured, 2 replayed
     float timings[7] = {};
     int launches = 0;  // this library's kernel launches in the last stage call
+    // bounds set by the caller: attempts of one union-find join (negative: the node count
+    // plus one, which cannot run out) and the bytes the context's buffers may hold (0: no limit)
+    int union_retries = -1;
+    uint64_t memory_limit = 0;
+    uint64_t memory_held = 0;
 };
 
 namespace {
@@ -85,13 +90,24 @@ T *dbuf(chiaro_depth_ctx *ctx, const std::string &name, size_t count) {
     size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
     auto &b = ctx->buffers[name];
     if (b.bytes < bytes) {
+        if (ctx->memory_limit && ctx->memory_held - b.bytes + bytes > ctx->memory_limit)
+            throw CudaError{cudaErrorMemoryAllocation, "a context buffer beyond the context's memory limit"};
         if (b.ptr) CK(cudaFree(b.ptr));
+        ctx->memory_held -= b.bytes;
         b.ptr = nullptr;
+        b.bytes = 0;
         CK(cudaMalloc(&b.ptr, bytes));
         b.bytes = bytes;
+        ctx->memory_held += bytes;
         ++ctx->alloc_epoch;  // a captured stage graph holding the old pointer is void
     }
     return static_cast<T *>(b.ptr);
+}
+
+// Retry bound of the union-find joins for a grid of n nodes (see uf_union).
+int union_retries(const chiaro_depth_ctx *ctx, size_t n) {
+    if (ctx->union_retries >= 0) return ctx->union_retries;
+    return (int)std::min<size_t>(n + 1, INT32_MAX);
 }
 
 int fail(chiaro_depth_ctx *ctx, const CudaError &e) {
@@ -938,6 +954,7 @@ struct HostTransfers {
 };
 
 struct Results {  // read back once at the end
+    int status;  // UNION_GAVE_UP when a component join ran out of retries
     unsigned long long tested, measured, regularized;
     unsigned long long target_counts[MAX_VIEWS][3];
     double median_depth;
@@ -1409,7 +1426,8 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     components_init_kernel<<<blocks_for(M, 256), 256, 0, s>>>(parent, (int)M);
     CK(cudaMemsetAsync(csize, 0, M * sizeof(int), s));
     components_union_kernel<<<blocks_for(M, 256), 256, 0, s>>>(has_a, direct.depth, fguidance, parent, (int)g.columns,
-                                                               (int)g.rows, inverse_step * 2.5);
+                                                               (int)g.rows, inverse_step * 2.5,
+                                                               union_retries(ctx, M), &d_results->status);
     components_size_kernel<<<blocks_for(M, 256), 256, 0, s>>>(has_a, parent, csize, (int)M);
     Field fin = field_bufs(ctx, "final", M);
     components_mark_kernel<<<blocks_for(M, 256), 256, 0, s>>>(has_a, parent, csize, fin.has, (int)M,
@@ -1685,6 +1703,10 @@ int refine(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views, size
             refined[t].columns = g.columns;
             refined[t].rows = g.rows;
         }
+        if (h_results.status & UNION_GAVE_UP) {
+            ctx->error = "reject_small_direct_components: a union-find join ran out of retries";
+            return CHIARO_ERR_TIMEOUT;
+        }
         fill_reports(h_results, rewritten, n_views, reports);
     } catch (const CudaError &e) {
         return fail(ctx, e);
@@ -1821,6 +1843,20 @@ int chiaro_depth_set_stage_graph(chiaro_depth_ctx *ctx, int32_t enabled) {
 
 int chiaro_depth_stage_graph_state(const chiaro_depth_ctx *ctx) { return ctx ? ctx->stage_graph_state : -1; }
 
+int chiaro_depth_set_union_retry_limit(chiaro_depth_ctx *ctx, int32_t retries) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    ctx->union_retries = retries < 0 ? -1 : retries;
+    return CHIARO_OK;
+}
+
+int chiaro_depth_set_memory_limit(chiaro_depth_ctx *ctx, uint64_t bytes) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    ctx->memory_limit = bytes;
+    return CHIARO_OK;
+}
+
+uint64_t chiaro_depth_memory_held(const chiaro_depth_ctx *ctx) { return ctx ? ctx->memory_held : 0; }
+
 int chiaro_depth_last_timings(const chiaro_depth_ctx *ctx, float *ms, int capacity) {
     if (!ctx || !ms) return 0;
     int n = std::min(capacity, 7);
@@ -1933,7 +1969,9 @@ int chiaro_reject_isolated(chiaro_depth_ctx *ctx, uint8_t *has, const double *de
 
 int chiaro_reject_small_components(chiaro_depth_ctx *ctx, uint8_t *has, const double *depth, const float *guidance,
                                    uint64_t columns, uint64_t rows, double inverse_tolerance, uint64_t minimum_nodes) {
-    if (!ctx || !has || !depth || !guidance) return CHIARO_ERR_ARGUMENT;
+    if (!ctx || !has || !depth || !guidance || columns < 1 || rows < 1) return CHIARO_ERR_ARGUMENT;
+    // node indices are 32-bit: refuse each side before the product can wrap
+    if (columns >= (1ull << 31) || rows >= (1ull << 31) || columns * rows >= (1ull << 31)) return CHIARO_ERR_ARGUMENT;
     if (minimum_nodes <= 1) return CHIARO_OK;  // depth.rs:941-943
     try {
         CK(cudaSetDevice(ctx->device));
@@ -1943,16 +1981,26 @@ int chiaro_reject_small_components(chiaro_depth_ctx *ctx, uint8_t *has, const do
         double *dd = dbuf<double>(ctx, "op.depth", n);
         float *dg = dbuf<float>(ctx, "op.guid", n);
         int *parent = dbuf<int>(ctx, "op.parent", n), *size = dbuf<int>(ctx, "op.size", n);
+        int *status = dbuf<int>(ctx, "op.status", 1);
         upload(ctx, dh, has, n);
         upload(ctx, dd, depth, n);
         upload(ctx, dg, guidance, n);
+        CK(cudaMemsetAsync(status, 0, sizeof(int), s));
         components_init_kernel<<<blocks_for(n, 256), 256, 0, s>>>(parent, (int)n);
         CK(cudaMemsetAsync(size, 0, n * sizeof(int), s));
         components_union_kernel<<<blocks_for(n, 256), 256, 0, s>>>(dh, dd, dg, parent, (int)columns, (int)rows,
-                                                                   inverse_tolerance);
+                                                                   inverse_tolerance, union_retries(ctx, n), status);
         components_size_kernel<<<blocks_for(n, 256), 256, 0, s>>>(dh, parent, size, (int)n);
-        components_mark_kernel<<<blocks_for(n, 256), 256, 0, s>>>(dh, parent, size, dh2, (int)n, (int)minimum_nodes);
+        components_mark_kernel<<<blocks_for(n, 256), 256, 0, s>>>(dh, parent, size, dh2, (int)n,
+                                                                  (int)std::min<uint64_t>(minimum_nodes, INT32_MAX));
         CK(cudaGetLastError());
+        int h_status = 0;
+        CK(cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (h_status & UNION_GAVE_UP) {
+            ctx->error = "reject_small_components: a union-find join ran out of retries";
+            return CHIARO_ERR_TIMEOUT;
+        }
         download(ctx, has, dh2, n);
         CK(cudaStreamSynchronize(s));
     } catch (const CudaError &e) {
@@ -2454,16 +2502,19 @@ int chiaro_refine_resolution_warp(chiaro_depth_ctx *ctx, const float *reference,
 // size per node) in a file-scope device array, so it calls no cudaMalloc,
 // cudaFree or allocating library routine.
 //
-// The array holds NOALLOC_MAX_NODES nodes (2 x 4 MiB); every GPU that loads
-// the library keeps it until the process exits. All calls share it, so calls
-// that overlap on the GPU (different streams, or host threads) race; the
-// scratch keeps the previous call's contents and is reinitialised on every call.
+// The array holds NOALLOC_MAX_NODES nodes (2 x 4 MiB, plus a status word); every
+// GPU that loads the library keeps it until the process exits. All calls share
+// it, so calls that overlap on the GPU (different streams, or host threads)
+// race; the scratch keeps the previous call's contents and is reinitialised on
+// every call. Its device address is looked up once per device index and kept:
+// after cudaDeviceReset the kept address is stale, so the entry point must not
+// be used across a device reset.
 // ---------------------------------------------------------------------------------
 namespace {
 
 constexpr uint64_t NOALLOC_MAX_NODES = 1u << 20;
 
-static __device__ __align__(256) int g_component_scratch[2 * NOALLOC_MAX_NODES];  // [parent | size]
+static __device__ __align__(256) int g_component_scratch[2 * NOALLOC_MAX_NODES + 64];  // [parent | size | status]
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_scratch_mutex;
@@ -2494,6 +2545,8 @@ extern "C" int chiaro_reject_small_components_noalloc(void *stream, const uint8_
                                                       double inverse_tolerance, uint64_t minimum_nodes,
                                                       uint8_t *has_out) {
     if (!has || !depth || !guidance || !has_out || columns < 1 || rows < 1) return CHIARO_ERR_ARGUMENT;
+    // each side first, so that the product below cannot wrap
+    if (columns > NOALLOC_MAX_NODES || rows > NOALLOC_MAX_NODES) return CHIARO_ERR_CAPACITY;
     const uint64_t n = columns * rows;
     if (n > NOALLOC_MAX_NODES) return CHIARO_ERR_CAPACITY;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -2503,12 +2556,14 @@ extern "C" int chiaro_reject_small_components_noalloc(void *stream, const uint8_
     }
     int *scratch = nullptr;
     if (component_scratch(&scratch) != cudaSuccess) return CHIARO_ERR_CUDA;
-    int *parent = scratch, *size = scratch + NOALLOC_MAX_NODES;
+    int *parent = scratch, *size = scratch + NOALLOC_MAX_NODES, *status = scratch + 2 * NOALLOC_MAX_NODES;
     const unsigned blocks = blocks_for(n, 256);
     components_init_kernel<<<blocks, 256, 0, s>>>(parent, (int)n);
     if (cudaMemsetAsync(size, 0, n * sizeof(int), s) != cudaSuccess) return CHIARO_ERR_CUDA;
+    if (cudaMemsetAsync(status, 0, sizeof(int), s) != cudaSuccess) return CHIARO_ERR_CUDA;
+    // n + 1 retries: a join cannot run out (see uf_union), so the status word stays clear
     components_union_kernel<<<blocks, 256, 0, s>>>(has, depth, guidance, parent, (int)columns, (int)rows,
-                                                   inverse_tolerance);
+                                                   inverse_tolerance, (int)n + 1, status);
     components_size_kernel<<<blocks, 256, 0, s>>>(has, parent, size, (int)n);
     components_mark_kernel<<<blocks, 256, 0, s>>>(has, parent, size, has_out, (int)n,
                                                   (int)std::min<uint64_t>(minimum_nodes, INT32_MAX));

@@ -53,6 +53,9 @@ SIGNATURES = {
                                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "chiaro_depth_set_stage_graph": (C.c_int, [C.c_void_p, C.c_int32]),
     "chiaro_depth_stage_graph_state": (C.c_int, [C.c_void_p]),
+    "chiaro_depth_set_union_retry_limit": (C.c_int, [C.c_void_p, C.c_int32]),
+    "chiaro_depth_set_memory_limit": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "chiaro_depth_memory_held": (C.c_uint64, [C.c_void_p]),
     "chiaro_align_options_default": (None, [P(abi.AlignOptionsC)]),
     "chiaro_align_module": (C.c_int, [C.c_void_p, P(abi.AlignInputC), P(abi.AlignInputC), C.c_int32,
                                       P(abi.AlignOptionsC), P(abi.WarpC), P(abi.WarpC), P(C.c_float),
@@ -199,6 +202,18 @@ class DepthContext:
 
     def stream_handle(self) -> int:
         return int(self.lib.chiaro_depth_ctx_stream(self.handle) or 0)
+
+    def set_union_retry_limit(self, retries: int = -1) -> None:
+        """Bound the union-find joins' attempts (negative: the node count plus one, which
+        cannot run out; 0: every join gives up at once)."""
+        self.check(self.lib.chiaro_depth_set_union_retry_limit(self.handle, int(retries)))
+
+    def set_memory_limit(self, nbytes: int = 0) -> None:
+        """Cap the device memory the context's buffers may hold (0: no cap)."""
+        self.check(self.lib.chiaro_depth_set_memory_limit(self.handle, int(nbytes)))
+
+    def memory_held(self) -> int:
+        return int(self.lib.chiaro_depth_memory_held(self.handle))
 
     def make_debug(self, arrays: dict) -> DepthDebugC:
         dbg = DepthDebugC()

@@ -270,6 +270,25 @@ int chiaro_depth_set_stage_graph(chiaro_depth_ctx *ctx, int32_t enabled);
  * launched the graph, 2 replayed it. */
 int chiaro_depth_stage_graph_state(const chiaro_depth_ctx *ctx);
 
+/* No counterpart in the reference (whose CPU union-find is a depth-first search
+ * with no retries): the bound on the compare-and-swap attempts of one union-find
+ * join in the connected-components filter (depth.rs:933-989), on the GPU. A
+ * negative value, the default, bounds a join by the grid's node count plus one,
+ * which cannot run out (each failed attempt means another join succeeded). A
+ * smaller bound may run out (0 allows no attempt, so every join gives up); the
+ * call then returns CHIARO_ERR_TIMEOUT instead of a result with a join left out,
+ * and the context stays usable. */
+int chiaro_depth_set_union_retry_limit(chiaro_depth_ctx *ctx, int32_t retries);
+
+/* No counterpart in the reference: a cap on the device memory the context's
+ * buffers may hold (0, the default: no cap), for hosts that give this library a
+ * fixed budget. A call that would grow its buffers past the cap returns
+ * CHIARO_ERR_CUDA (out of memory, with the message in chiaro_depth_last_error)
+ * before allocating; buffers already held are kept, and the context stays usable.
+ * chiaro_depth_memory_held reports the bytes held now. */
+int chiaro_depth_set_memory_limit(chiaro_depth_ctx *ctx, uint64_t bytes);
+uint64_t chiaro_depth_memory_held(const chiaro_depth_ctx *ctx);
+
 /* Device time in milliseconds of each stage of the last call on this context:
  * [0] cost volume, [1] SGM, [2] select, [3] direct pass, [4] filters,
  * [5] per-target decisions, [6] whole stage. Returns the count written. */
@@ -634,8 +653,10 @@ int chiaro_refine_resolution_warp_device(chiaro_depth_ctx *ctx, const float *ref
  * call returns without synchronising. Its union-find scratch lives in a static
  * device array of 2^20 nodes (8 MiB per GPU, held until exit): grids with more
  * nodes return CHIARO_ERR_CAPACITY. The first call on a device looks up that
- * array's address; make it before any stream capture. Calls share the array,
- * so calls that overlap on the GPU race. Nothing here calls cudaMalloc. */
+ * array's address; make it before any stream capture. That address is kept
+ * per device index for the life of the process, so do not use this call across
+ * cudaDeviceReset. Calls share the array, so calls that overlap on the GPU race.
+ * Nothing here calls cudaMalloc. */
 int chiaro_reject_small_components_noalloc(void *stream, const uint8_t *has, const double *depth,
                                            const float *guidance, uint64_t columns, uint64_t rows,
                                            double inverse_tolerance, uint64_t minimum_nodes,
