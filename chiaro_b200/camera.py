@@ -58,6 +58,39 @@ def rotation_about_axis(axis, angle_radians: float) -> np.ndarray:
     ])
 
 
+def rotation_from_axis_angle(vector) -> np.ndarray:
+    """math.rs:111-118: rotation by |vector| radians about vector; identity below 1e-18."""
+    v = np.asarray(vector, dtype=np.float64)
+    angle = float(np.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]))
+    if angle < 1e-18:
+        return IDENTITY.copy()
+    return rotation_about_axis(v, angle)
+
+
+def reflection(normal) -> np.ndarray:
+    """math.rs:120-129: Householder reflection across the plane with unit normal ``normal``."""
+    x, y, z = _normalize_one(np.asarray(normal, dtype=np.float64))
+    return np.array([
+        [1.0 - 2.0 * x * x, -2.0 * x * y, -2.0 * x * z],
+        [-2.0 * x * y, 1.0 - 2.0 * y * y, -2.0 * y * z],
+        [-2.0 * x * z, -2.0 * y * z, 1.0 - 2.0 * z * z],
+    ])
+
+
+def mirror_pose(real_camera_location, real_camera_orientation_cw, mirror_normal, plane_point):
+    """The Mirror pose of ResolvedCamera::new (geometry.rs:86-104) from a mirror's unit
+    normal and a point on its plane: (real_cw, reflect, virtual_center), the virtual
+    centre being the real centre reflected across the mirror plane."""
+    normal = np.asarray(mirror_normal, dtype=np.float64)
+    location = np.asarray(real_camera_location, dtype=np.float64)
+    plane = np.asarray(plane_point, dtype=np.float64)
+    reflect = reflection(normal)
+    rel = location - plane
+    distance = normal[0] * rel[0] + normal[1] * rel[1] + normal[2] * rel[2]
+    virtual_center = location - normal * (2.0 * distance)
+    return np.asarray(real_camera_orientation_cw, dtype=np.float64), reflect, virtual_center
+
+
 def _dot3(a, b):
     # ((a0*b0 + a1*b1) + a2*b2), broadcasting over a leading axis
     return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]

@@ -33,7 +33,8 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 
 from .align import AlignInput, ModuleAlignment, AlignmentReport, Warp
-from .camera import PolynomialDistortion, ResolvedCamera, rotation_about_axis
+from .camera import (PolynomialDistortion, ResolvedCamera, mirror_pose, reflection, rotation_about_axis,
+                     rotation_from_axis_angle)
 from .depth import DepthOptions
 from .image import Plane
 
@@ -147,6 +148,39 @@ def _camera(width, height, k, rotation_wc, centre, distortion=None) -> ResolvedC
     t = -(rotation_wc @ centre)
     return ResolvedCamera(width=width, height=height, k=k, distortion=distortion,
                           rotation_wc=rotation_wc, translation_wc=t)
+
+
+_FLIP_AXIS = {True: np.diag([1.0, -1.0, 1.0]), False: np.diag([-1.0, 1.0, 1.0])}
+
+
+def _mirror_camera(width, height, k, rotation_wc, centre, flip: bool, rng: np.random.Generator,
+                   distortion=None, orientation=None) -> ResolvedCamera:
+    """A module behind a 45-degree fold mirror (the L16's mid and tele modules) whose
+    virtual camera sits at ``centre`` and looks along ``rotation_wc``.
+
+    The mirror's normal is tilted about 45 degrees from the viewing axis (towards a
+    random side), and its plane lies a few millimetres in front of the virtual centre.
+    The physical module sits at the virtual centre reflected across that plane and
+    looks into the mirror; its orientation real_cw makes reflect . real_cw . F equal the
+    virtual camera's camera-to-world rotation, F being the image-axis flip that
+    flip_img_around_x restores (geometry.rs:129-136). The pose itself comes from the
+    reference's construction (geometry.rs:86-104) through ``mirror_pose``.
+    ``orientation`` is an axis-angle offset in degrees (CameraRefinement's
+    orientation_offset_degrees, geometry.rs:22-28, applied at geometry.rs:111-114).
+    """
+    rotation_cw = rotation_wc.T
+    axis = rotation_cw[:, 2]
+    side = rotation_cw[:, 0] * np.cos(rng.uniform(0, 2 * np.pi)) + rotation_cw[:, 1] * np.sin(rng.uniform(0, 2 * np.pi))
+    side = _unit(side - axis * float(side @ axis))
+    tilt = np.deg2rad(45.0 + rng.uniform(-3.0, 3.0))
+    normal = _unit(-axis * np.cos(tilt) + side * np.sin(tilt))
+    plane_point = centre + axis * rng.uniform(4.0, 8.0)
+    location = centre - normal * (2.0 * float(normal @ (centre - plane_point)))
+    real_cw = reflection(normal) @ rotation_cw @ _FLIP_AXIS[flip]
+    real_cw, reflect, virtual_center = mirror_pose(location, real_cw, normal, plane_point)
+    oc = np.eye(3) if orientation is None else rotation_from_axis_angle(np.asarray(orientation) * (np.pi / 180.0))
+    return ResolvedCamera(width=width, height=height, k=k, distortion=distortion, flip=flip, real_cw=real_cw,
+                          reflect=reflect, virtual_center=virtual_center, orientation_correction=oc)
 
 
 def _random_plane(rng, ref: ResolvedCamera, depth_mm: float, coverage: Tuple[float, float],
@@ -290,8 +324,18 @@ def luminance_half(raw: np.ndarray, black: float = 0.0, white: float = 4095.0) -
 def make_scene(name: str, width: int, height: int, n_sources: int, n_planes: int, n_spheres: int,
                depth_range: Tuple[float, float], baseline_range: Tuple[float, float],
                max_rotation_deg: float, options: DepthOptions, seed: int,
-               distortion: bool = False, horizontal_only: bool = False, texel_px: float = 3.0) -> Scene:
+               distortion: bool = False, horizontal_only: bool = False, texel_px: float = 3.0,
+               mirrors: Optional[Dict[int, bool]] = None,
+               orientation: Optional[Dict[int, Tuple[float, float, float]]] = None) -> Scene:
+    """``mirrors`` maps module indices (0 = the reference) to the flip_img_around_x value
+    of a module behind a fold mirror (Pose::Mirror); ``orientation`` maps module indices
+    to an axis-angle orientation offset in degrees. Both leave the random draws of the
+    canonical scene unchanged (their own draws come from a separate generator), so a
+    mirrored scene sees the same surfaces from the same virtual positions."""
     rng = np.random.default_rng(seed)
+    mirror_rng = np.random.default_rng((seed, 271828))
+    mirrors = mirrors or {}
+    orientation = orientation or {}
     tiles = [_noise_tile(np.random.default_rng(seed * 7919 + i)) for i in range(4)]
     ref_k = _intrinsics(width, height)
     ref_dist = None
@@ -299,7 +343,7 @@ def make_scene(name: str, width: int, height: int, n_sources: int, n_planes: int
         ref_dist = PolynomialDistortion(((width - 1) / 2.0, (height - 1) / 2.0), (width * 0.8, width * 0.8),
                                         (0.02, -0.01, 0.0, 0.0, 0.002))
     ref = _camera(width, height, ref_k, np.eye(3), np.zeros(3), ref_dist)
-    cams = [ref]
+    canonical = [ref]
     for _ in range(n_sources):
         b = rng.uniform(*baseline_range)
         if horizontal_only:
@@ -315,7 +359,21 @@ def make_scene(name: str, width: int, height: int, n_sources: int, n_planes: int
             dist = PolynomialDistortion(((width - 1) / 2.0 + rng.uniform(-5, 5), (height - 1) / 2.0 + rng.uniform(-5, 5)),
                                         (width * 0.8, width * 0.8),
                                         (rng.uniform(0.0, 0.04), rng.uniform(-0.02, 0.0), 0.0, 0.0, 0.002))
-        cams.append(_camera(width, height, k, rot, centre, dist))
+        canonical.append(_camera(width, height, k, rot, centre, dist))
+    cams = []
+    for i, cam in enumerate(canonical):
+        if i in mirrors or i in orientation:
+            centre = cam.center()
+            if i in mirrors:
+                cam = _mirror_camera(width, height, cam.k, cam.rotation_wc, centre, mirrors[i], mirror_rng,
+                                     cam.distortion, orientation.get(i))
+            else:
+                cam = ResolvedCamera(width=width, height=height, k=cam.k, distortion=cam.distortion,
+                                     rotation_wc=cam.rotation_wc, translation_wc=cam.translation_wc,
+                                     orientation_correction=rotation_from_axis_angle(
+                                         np.asarray(orientation[i]) * (np.pi / 180.0)))
+        cams.append(cam)
+    ref = cams[0]
     near, far = depth_range
     surfaces = [_background(rng, ref, far, texel_px, 0)]
     for i in range(n_planes - 1):

@@ -288,3 +288,20 @@ def test_no_targets_gives_unsupported_map():
     assert dmap is not None
     assert np.all(dmap.provenance == abi.UNSUPPORTED)
     assert all(a.report.depth is None for a in al)
+
+
+@pytest.mark.parametrize("name,seed,mirrors,orientation", [
+    ("small", 5, {1: True, 2: False}, None),                              # both flip kinds as targets
+    ("tiny", 11, {0: True}, {1: (0.03, -0.02, 0.04)}),                    # mirrored reference
+    ("small", 6, {2: False}, {2: (-0.02, 0.05, 0.01), 1: (0.01, 0.01, -0.03)}),  # mirror + orientation
+    ("tiny", 12, {0: False, 1: True, 2: False}, {0: (0.02, 0.0, -0.01)}),  # every module mirrored
+], ids=["targets-both-flips", "mirrored-reference", "orientation-corrections", "all-mirrored"])
+def test_stage_with_mirrored_modules_bit_exact(name, seed, mirrors, orientation):
+    """Modules behind fold mirrors (Pose::Mirror with flip_img_around_x Some(true) and
+    Some(false), geometry.rs:86-104, 129-136) and orientation corrections
+    (geometry.rs:111-114): the camera branches of the L16's mid and tele modules."""
+    sc = scenes.workload(name, seed=seed, mirrors=mirrors, orientation=orientation)
+    assert any(c.pose_kind == 1 for c in sc.cameras)
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+    assert (dmap.provenance == abi.MEASURED).sum() > 0.2 * dmap.provenance.size
