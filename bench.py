@@ -15,7 +15,11 @@ API with pinned host inputs (e2e). With N > 1 (torchrun) every rank processes
 its own replica of the workload (the stage shards by capture; no collective on
 the data path): value is the total over ranks, timed as the maximum over ranks.
 The reference arm times the CPU oracle (a C++ restatement of the reference's
-Rust code) on a bounded band of the same workload and scales by node count.
+Rust code): each step is the whole stage on a bounded sample of the same
+workload (one coarse row in each of the reference's worker bands, with the
+fine rows they seed; the steps step through the bands, top to bottom), or the
+whole workload where it takes seconds (two_view). Its value is the SGM cells of
+what it processed over the time it took: measured, not extrapolated.
 """
 from __future__ import annotations
 
@@ -53,7 +57,8 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", default="five_view", choices=sorted(WORKLOAD_TEXT))
     p.add_argument("--seed", type=int, default=0)
-    p.add_argument("--band", type=int, default=0, help="coarse rows per CPU sample (0 = automatic)")
+    p.add_argument("--rows-per-band", type=int, default=1,
+                   help="coarse rows per worker band in each CPU sample step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (0 = --steps)")
     p.add_argument("--band-train", type=int, default=24, help="1040x780 scenes the band network trains on")
@@ -61,6 +66,7 @@ def parse_args():
     p.add_argument("--band-train-full", type=int, default=2,
                    help="full-resolution five-view scenes added to the third band network's training")
     p.add_argument("--no-learned-band", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the per-config sub-objects (two_view, ...)")
     return p.parse_args()
 
 
@@ -253,7 +259,23 @@ def run_ours(args, rank, world, local):
                                                             for w in scene.warps)
     d2h = M * (8 + 4 + 1) + targets * M * (8 + 4)
     e2e_value = whole_job_rate(world, work["cells"], e2e_steps, e2e_s)
+    # the same public call with the scene's own (pageable) numpy planes, as a caller that
+    # hands ordinary host vectors makes it
+    pageable = scene.inputs()
+    for _ in range(max(args.warmup, 2)):
+        refine_multiview_depth(pageable, scene.reference_index, scene.alignments(), scene.options, context=ctx)
+    e2e_pageable = []
+    for _ in range(e2e_steps):
+        alignments = scene.alignments()
+        t0 = time.perf_counter()
+        result = refine_multiview_depth(pageable, scene.reference_index, alignments, scene.options, context=ctx)
+        e2e_pageable.append(time.perf_counter() - t0)
+        assert result is not None
+    e2e_pageable_s = max_over_ranks(float(sum(e2e_pageable)), world, device)
 
+    configs = {}
+    if args.workload == "five_view" and not args.no_configs:
+        configs["two_view"] = two_view_config(args, ctx, torch, stream, flush, rank == 0 and world == 1)
     graph = stage_graph(args, torch, stream, flush, stage)
     finest = finest_coarse_grid(args, scene, stage, torch, stream, flush)
     resolution = resolution_warp(args, scene, ctx)
@@ -307,17 +329,27 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(1e3 * e2e_s / e2e_steps, 3),
                 "api": "chiaro_b200.depth.refine_multiview_depth (host buffers, pinned inputs)"},
+        "e2e_pageable": {"value": round(whole_job_rate(world, work["cells"], e2e_steps, e2e_pageable_s), 3),
+                         "unit": UNIT, "ms_per_step": round(1e3 * e2e_pageable_s / e2e_steps, 3),
+                         "api": "chiaro_b200.depth.refine_multiview_depth (host buffers: the scene's own pageable "
+                                "numpy planes, as a caller passing ordinary host vectors)"},
+        **({"configs": configs} if configs else {}),
         "gpu_launches": launches * args.steps,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline
-        band = args.band or 4
-        r = cpu_baseline.run_sample(scene, band=band)
-        line["cpu_baseline"] = {"value": round(r["gcells_per_s"], 6), "unit": UNIT, "cores": r["threads"],
-                                "kind": "port", "sample": r["sample"],
-                                "estimated_stage_s": round(r["total_seconds"], 2),
-                                "stage_s": {k: round(v, 3) for k, v in r["stage_seconds"].items()}}
+        if args.workload == "two_view":
+            r = cpu_baseline.run_whole(scene)
+            line["cpu_baseline"] = {"value": round(r["gcells_per_s"], 6), "unit": UNIT, "cores": r["threads"],
+                                    "kind": "port", "sample": r["sample"], "seconds": round(r["seconds"], 2)}
+        else:
+            r = cpu_baseline.run_samples(scene, (6, 18), rows_per_band=args.rows_per_band)
+            line["cpu_baseline"] = {"value": round(r["gcells_per_s"], 6), "unit": UNIT, "cores": r["threads"],
+                                    "kind": "port", "sample": r["sample"], "samples": r["samples"],
+                                    "cells": r["cells"], "seconds": round(r["seconds"], 2),
+                                    "spread": {k: round(v, 6) for k, v in r["spread"].items()},
+                                    "stage_s": {k: round(v, 3) for k, v in r["stage_seconds"].items()}}
         # refine_resolution_warp of every target through the oracle, one host thread as the reference runs it
         from oracle import oracle as oracle_module
         ref = scene.luminance[scene.reference_index]
@@ -448,6 +480,71 @@ def finest_coarse_grid(args, scene, stage, torch, stream, flush):
             "sgm_cells_per_step": work["cells"], "ms_per_step": round(ms, 3),
             "gcells_s": round(work["cells"] / (ms / 1e3) / 1e9, 3),
             "stage_ms": {k: round(statistics.median(s[k] for s in stages), 4) for k in stages[0]}}
+
+
+def timed_stage(args, torch, stream, flush, fn, ctx, steps=None):
+    """Device time (ms) per call of ``fn`` with the main leg's method (L2 flushed, CUDA
+    events on the library's stream) and the median per-stage times."""
+    for _ in range(max(args.warmup, 2)):
+        fn()
+    steps = steps or max(1, args.steps)
+    total, stages = 0.0, []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        fn()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+        stages.append(ctx.timings())
+    return total / steps, {k: statistics.median(s[k] for s in stages) for k in stages[0]}
+
+
+def stage_rooflines(work, ms, stage_ms, sm_mhz):
+    """The SGM's HBM fraction and the cost volume's FP32 fraction for one workload."""
+    peaks = measured_peaks()
+    sgm_gbs = work["sgm_bytes"] / (stage_ms["sgm"] / 1e3) / 1e9
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    cost_tflops = work["cost_flop"] / (stage_ms["cost_volume"] / 1e3) / 1e12
+    return {"sgm": {"bound": "hbm", "achieved": round(sgm_gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": round(sgm_gbs / peaks["hbm_gbs"], 4), "algorithmic_bytes": work["sgm_bytes"],
+                    "peak_source": peaks["source"]},
+            "cost_volume": {"bound": "fp32", "achieved": round(cost_tflops, 3), "peak": round(fp32_peak, 1),
+                            "unit": "TFLOP/s", "frac": round(cost_tflops / fp32_peak, 4),
+                            "taps": work["cost_taps"], "flop_per_tap": 16}}
+
+
+def two_view_config(args, ctx, torch, stream, flush, with_cpu):
+    """Config 0 (two_view: 1040x780 reference + 1 source at 25 mm, 64 planes): the whole
+    stage on device buffers, timed like the main leg, with its SGM and cost-volume
+    rooflines, and the oracle's whole stage on the host cores (measured once, whole)."""
+    from chiaro_b200 import scenes
+    from chiaro_b200.depth import DeviceStage
+    scene = scenes.workload("two_view", seed=args.seed)
+    work = stage_bytes(scene)
+    stage = DeviceStage(scene.inputs(), scene.reference_index, scene.alignments(), scene.options, context=ctx)
+
+    def step():
+        if not stage():
+            raise RuntimeError("the stage returned None on two_view")
+
+    ms, stage_ms = timed_stage(args, torch, stream, flush, step, ctx)
+    sm_mhz = 1965.0
+    out = {"workload": WORKLOAD_TEXT["two_view"], "value": round(work["cells"] / (ms / 1e3) / 1e9, 3),
+           "unit": UNIT, "ms_per_step": round(ms, 4), "sgm_cells_per_step": work["cells"],
+           "coarse_nodes": work["coarse_nodes"], "labels": work["labels"],
+           "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+           "roofline": stage_rooflines(work, ms, stage_ms, sm_mhz)}
+    if with_cpu:
+        from oracle import cpu_baseline
+        r = cpu_baseline.run_whole(scene)
+        out["cpu_baseline"] = {"value": round(r["gcells_per_s"], 6), "unit": UNIT, "cores": r["threads"],
+                               "kind": "port", "sample": r["sample"], "seconds": round(r["seconds"], 3)}
+    del stage
+    return out
 
 
 def stage_graph(args, torch, stream, flush, stage):
@@ -742,7 +839,14 @@ def learned_band(args, scene, ctx, torch, device, stream, flush):
 
 
 def run_reference(args, rank, world):
-    """The reference's CPU path (the oracle restatement) on a bounded band."""
+    """The reference's CPU path (the oracle restatement, all host threads), measured.
+
+    five_view: each step is the whole stage on one sample (one coarse row in each of
+    the reference's worker bands and the fine rows they seed, oracle/cpu_baseline.py);
+    the timed steps' offsets spread over the bands, so together they cover the image
+    from top to bottom. two_view: each step is the whole stage on the whole workload.
+    value = SGM cells processed / seconds taken, over the timed steps.
+    """
     if rank != 0:
         return None
     from chiaro_b200 import scenes
@@ -750,28 +854,53 @@ def run_reference(args, rank, world):
 
     scene = scenes.workload(args.workload, seed=args.seed)
     work = stage_bytes(scene)
-    band = args.band or 2
-    for _ in range(args.warmup):
-        cpu_baseline.run_sample(scene, band=band)
-    estimates, last = [], None
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        last = cpu_baseline.run_sample(scene, band=band)
-        estimates.append(last["total_seconds"])
-    wall = time.perf_counter() - t0
-    mean_s = statistics.mean(estimates)
-    value = work["cells"] / mean_s / 1e9
+    threads = os.cpu_count() or 1
+    if args.workload == "two_view":
+        def one(_):
+            r = cpu_baseline.run_whole(scene, threads)
+            return r["cells"], r["seconds"], r
+
+        offsets = [None] * args.steps
+    else:
+        from chiaro_b200.depth import output_shape
+        _, (_, coarse_rows, _) = output_shape(scene.width, scene.height, scene.options)
+        band = min(b - a for a, b in cpu_baseline.worker_bands(coarse_rows, threads))
+
+        def one(offset):
+            r = cpu_baseline.run_sample(scene, offset, threads, args.rows_per_band)
+            return r["cells"], r["wall_seconds"], r
+
+        offsets = [(i * band) // max(args.steps, 1) for i in range(args.steps)]
+    for i in range(args.warmup):
+        one(offsets[i % len(offsets)] if offsets else None)
+    cells = seconds = 0.0
+    rates, last = [], None
+    for k in offsets:
+        c, t, last = one(k)
+        cells += c
+        seconds += t
+        rates.append(c / t / 1e9)
+    value = cells / seconds / 1e9
+    sample = last["sample"] if args.workload == "two_view" else (
+        f"whole stage on {args.rows_per_band} coarse row(s) in each of the reference's {threads}-worker row bands "
+        f"(offsets {offsets[0]}..{offsets[-1]} within the bands, top to bottom over the steps) with the fine rows "
+        f"they seed; cost volume and direct pass threaded as the reference threads them, SGM, winner-take-all, "
+        f"filters and per-target decisions on one thread; measured, not extrapolated")
     return {
         "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(mean_s * 1e3, 1), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": round(seconds * 1e3 / args.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (costs, scores) + f64 (geometry, depths)",
         "data": "synthetic (seeded ray-cast scenes, Poisson-Gaussian noise)",
         "config": {"workload": WORKLOAD_TEXT[args.workload], "seed": args.seed,
-                   "sgm_cells_per_step": work["cells"], "parallelism": "host threads (rank 0 only)"},
+                   "sgm_cells_per_step": work["cells"], "sgm_cells_per_timed_step": int(cells / args.steps),
+                   "parallelism": f"{threads} host threads (rank 0 only)"},
         "impl": "reference",
-        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": last["threads"], "kind": "port",
-                         "sample": last["sample"], "sample_wall_s_per_step": round(wall / args.steps, 2),
-                         "stage_s": {k: round(v, 3) for k, v in last["stage_seconds"].items()}},
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample,
+                         "spread": {"min_gcells_s": round(min(rates), 6), "max_gcells_s": round(max(rates), 6),
+                                    "stdev_over_mean": round(statistics.pstdev(rates) / statistics.mean(rates), 4)
+                                    if len(rates) > 1 else 0.0},
+                         "last_step_stage_s": {k: round(v, 3) for k, v in last.get("stage_seconds", {}).items()}},
         "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

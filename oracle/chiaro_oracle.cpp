@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -513,9 +514,12 @@ struct CostVolume {  // depth.rs:291-299
 };
 
 // build_cost_volume (depth.rs:1187-1277)
+// row_mask (optional, one byte per row) restricts the work to the marked rows; the
+// rows are still split into the reference's worker bands, so a mask that marks rows
+// in every band keeps every worker busy (the benchmark's bounded samples).
 static CostVolume build_cost_volume(const std::vector<Input> &inputs, size_t reference_index, size_t columns,
                                     size_t rows, size_t step, const Options &options, int threads,
-                                    size_t row_begin = 0, size_t row_end = SIZE_MAX) {
+                                    const uint8_t *row_mask = nullptr) {
     auto finite_depths = inverse_depth_samples(options.near_depth, options.far_depth, options.planes);
     std::reverse(finite_depths.begin(), finite_depths.end());
     CostVolume v;
@@ -527,9 +531,9 @@ static CostVolume build_cost_volume(const std::vector<Input> &inputs, size_t ref
     v.costs.assign(node_count * label_count, 0.0f);
     v.guidance.assign(node_count, 0.0f);
     v.tested.assign(node_count, 0);
-    row_end = std::min(row_end, rows);
     for_row_bands(rows, threads, [&](size_t first_row, size_t last_row) {
-        for (size_t row = std::max(first_row, row_begin); row < std::min(last_row, row_end); ++row) {
+        for (size_t row = first_row; row < last_row; ++row) {
+            if (row_mask && !row_mask[row]) continue;
             for (size_t column = 0; column < columns; ++column) {
                 size_t node = row * columns + column;
                 Vec2 p = {(double)(column * step), (double)(row * step)};
@@ -881,7 +885,7 @@ struct DirectField {  // depth.rs:301-308
 static DirectField measure_direct_depths(const std::vector<Input> &inputs, size_t reference_index,
                                          const Field &coarse, size_t coarse_columns, size_t coarse_rows,
                                          size_t coarse_step, double inverse_step, const Options &options,
-                                         int threads, size_t row_begin = 0, size_t row_end = SIZE_MAX) {
+                                         int threads, const uint8_t *row_mask = nullptr) {
     DirectField out;
     out.step = std::max<size_t>(coarse_step / 2, 4);
     out.columns = div_ceil(inputs[reference_index].width, out.step) + 1;
@@ -892,9 +896,9 @@ static DirectField measure_direct_depths(const std::vector<Input> &inputs, size_
     out.tested.assign(columns * rows, 0);
     size_t direct_radius = std::max<size_t>(options.patch_radius, 3);
     size_t wide_radius = std::max<size_t>(options.patch_radius * 2, 8);
-    row_end = std::min(row_end, rows);
     for_row_bands(rows, threads, [&](size_t first_row, size_t last_row) {
-        for (size_t row = std::max(first_row, row_begin); row < std::min(last_row, row_end); ++row) {
+        for (size_t row = first_row; row < last_row; ++row) {
+            if (row_mask && !row_mask[row]) continue;
             for (size_t column = 0; column < columns; ++column) {
                 size_t index = row * columns + column;
                 Vec2 p = {(double)(column * step), (double)(row * step)};
@@ -1236,17 +1240,19 @@ struct Result {
 
 // Per-target decisions for one target (depth.rs:427-489), returning the
 // filtered decision list.
+// row_of (optional) gives the raster row index of each grid row, for a grid of
+// sampled rows stacked together.
 static std::vector<NodeWarp> target_decisions(const std::vector<Input> &inputs, size_t reference_index,
                                               size_t target_index, const Field &field, const float *guidance,
                                               size_t columns, size_t rows, size_t step, double inverse_step,
-                                              const Options &options) {
+                                              const Options &options, const size_t *row_of = nullptr) {
     const Input &reference = inputs[reference_index];
     const Warp &global = inputs[target_index].warp;
     std::vector<NodeWarp> decisions(columns * rows);
     for (size_t row = 0; row < rows; ++row)
         for (size_t column = 0; column < columns; ++column) {
             size_t index = row * columns + column;
-            Vec2 p = {(double)(column * step), (double)(row * step)};
+            Vec2 p = {(double)(column * step), (double)((row_of ? row_of[row] : row) * step)};
             NodeWarp &d = decisions[index];
             auto global_q = global.map((float)p[0], (float)p[1]);
             if (!global_q) {
@@ -1830,9 +1836,11 @@ int oracle_build_cost_volume(const chiaro_view *views, size_t n_views, size_t re
     size_t step = std::max<size_t>(options.grid_step, 4);
     size_t columns = div_ceil(inputs[reference_index].width, step) + 1;
     size_t rows = div_ceil(inputs[reference_index].height, step) + 1;
-    auto v = build_cost_volume(inputs, reference_index, columns, rows, step, options, threads, row_begin, row_end);
-    size_t nl = v.labels.size();
     row_end = std::min(row_end, rows);
+    std::vector<uint8_t> mask(rows, 0);
+    for (size_t row = row_begin; row < row_end; ++row) mask[row] = 1;
+    auto v = build_cost_volume(inputs, reference_index, columns, rows, step, options, threads, mask.data());
+    size_t nl = v.labels.size();
     for (size_t row = row_begin; row < row_end; ++row)
         for (size_t column = 0; column < columns; ++column) {
             size_t node = row * columns + column;
@@ -1862,9 +1870,13 @@ int oracle_measure_direct_depths(const chiaro_view *views, size_t n_views, size_
     Field coarse =
         arrays_to_field(cc * cr, coarse_has, coarse_depth, coarse_confidence, coarse_improvement, coarse_regularized);
     double inverse_step = (1.0 / options.near_depth - 1.0 / options.far_depth) / (double)(options.planes - 1);
+    size_t fine_step = std::max<size_t>(cstep / 2, 4);
+    size_t fine_rows = div_ceil(inputs[reference_index].height, fine_step) + 1;
+    row_end = std::min(row_end, fine_rows);
+    std::vector<uint8_t> mask(fine_rows, 0);
+    for (size_t row = row_begin; row < row_end; ++row) mask[row] = 1;
     auto d = measure_direct_depths(inputs, reference_index, coarse, cc, cr, cstep, inverse_step, options, threads,
-                                   row_begin, row_end);
-    row_end = std::min(row_end, d.rows);
+                                   mask.data());
     for (size_t row = row_begin; row < row_end; ++row)
         for (size_t column = 0; column < d.columns; ++column) {
             size_t i = row * d.columns + column;
@@ -1935,6 +1947,101 @@ int oracle_target_decisions(const chiaro_view *views, size_t n_views, size_t ref
     enforce_warp_consensus(decisions, columns, band_rows);
     suppress_warp_boundaries(decisions, guidance + off, columns, band_rows);
     for (size_t i = 0; i < n; ++i) kind_out[i] = (uint8_t)decisions[i].kind;
+    return CHIARO_OK;
+}
+
+// The whole stage on a sample of coarse rows, timed per stage (the benchmark's CPU
+// baseline). coarse_row_mask marks the sampled coarse rows; the direct pass, the
+// filters and the decisions take the fine rows those nodes seed (fine rows 2r - 1 and
+// 2r round to coarse row r in nearest_coarse_depth, depth.rs:1062-1076). Each stage
+// runs as the reference runs it over the full grid:
+//   cost volume and direct pass: the reference's worker bands over all rows, each
+//     worker working on its own marked rows (depth.rs:1204-1206, 729-731);
+//   SGM, winner-take-all, filters and per-target decisions: one thread, over the
+//     sampled rows stacked into a grid of their own (the work per node and label is
+//     that of the full grid; depth.rs:359-392, 420-547).
+// seconds[6] receives the wall time of cost volume, SGM, select, direct, filters and
+// decisions; counts[2] the sampled coarse and fine nodes.
+int oracle_stage_sample(const chiaro_view *views, size_t n_views, size_t reference_index,
+                        const chiaro_depth_options *opt, const uint8_t *coarse_row_mask, int threads,
+                        double *seconds, uint64_t *counts) {
+    using clock = std::chrono::steady_clock;
+    auto since = [](clock::time_point t) { return std::chrono::duration<double>(clock::now() - t).count(); };
+    Options options(*opt);
+    if (!valid_options(options) || reference_index >= n_views || !views[reference_index].has_camera)
+        return CHIARO_INVALID;
+    auto inputs = make_inputs(views, n_views);
+    const Input &reference = inputs[reference_index];
+    size_t cstep = std::max<size_t>(options.grid_step, 4);
+    size_t cc = div_ceil(reference.width, cstep) + 1, cr = div_ceil(reference.height, cstep) + 1;
+    std::vector<size_t> coarse_rows;
+    for (size_t r = 0; r < cr; ++r)
+        if (coarse_row_mask[r]) coarse_rows.push_back(r);
+    if (coarse_rows.empty()) return CHIARO_INVALID;
+    auto t = clock::now();
+    CostVolume volume = build_cost_volume(inputs, reference_index, cc, cr, cstep, options, threads, coarse_row_mask);
+    seconds[0] = since(t);
+    size_t nl = volume.labels.size(), sr = coarse_rows.size(), sn = sr * cc;
+    std::vector<float> costs(sn * nl), scores(sn * nl), guidance(sn);
+    std::vector<uint8_t> tested(sn);
+    for (size_t i = 0; i < sr; ++i) {
+        size_t from = coarse_rows[i] * cc, to = i * cc;
+        std::memcpy(costs.data() + to * nl, volume.costs.data() + from * nl, cc * nl * 4);
+        std::memcpy(scores.data() + to * nl, volume.scores.data() + from * nl, cc * nl * 4);
+        std::memcpy(guidance.data() + to, volume.guidance.data() + from, cc * 4);
+        std::memcpy(tested.data() + to, volume.tested.data() + from, cc);
+    }
+    t = clock::now();
+    std::vector<float> regularised = semi_global_costs(costs.data(), guidance.data(), cc, sr, nl);
+    seconds[1] = since(t);
+    Field sampled;
+    std::vector<uint8_t> fillable;
+    t = clock::now();
+    select_depths(volume.labels, scores.data(), tested.data(), sn, regularised.data(), options, sampled, fillable);
+    seconds[2] = since(t);
+    Field coarse(cc * cr);
+    for (size_t i = 0; i < sr; ++i)
+        for (size_t c = 0; c < cc; ++c) coarse[coarse_rows[i] * cc + c] = sampled[i * cc + c];
+    double inverse_step = (1.0 / options.near_depth - 1.0 / options.far_depth) / (double)(options.planes - 1);
+    size_t step = std::max<size_t>(cstep / 2, 4);
+    size_t columns = div_ceil(reference.width, step) + 1, rows = div_ceil(reference.height, step) + 1;
+    std::vector<uint8_t> fine_mask(rows, 0);
+    for (size_t r : coarse_rows) {
+        if (2 * r >= 1 && 2 * r - 1 < rows) fine_mask[2 * r - 1] = 1;
+        if (2 * r < rows) fine_mask[2 * r] = 1;
+    }
+    t = clock::now();
+    DirectField direct = measure_direct_depths(inputs, reference_index, coarse, cc, cr, cstep, inverse_step, options,
+                                               threads, fine_mask.data());
+    seconds[3] = since(t);
+    std::vector<size_t> fine_rows;
+    for (size_t r = 0; r < rows; ++r)
+        if (fine_mask[r]) fine_rows.push_back(r);
+    size_t fr = fine_rows.size(), fn = fr * columns;
+    Field field(fn);
+    std::vector<float> fine_guidance(fn);
+    for (size_t i = 0; i < fr; ++i)
+        for (size_t c = 0; c < columns; ++c) {
+            field[i * columns + c] = direct.nodes[fine_rows[i] * columns + c];
+            fine_guidance[i * columns + c] = direct.guidance[fine_rows[i] * columns + c];
+        }
+    t = clock::now();
+    reject_isolated_direct_depths(field, fine_guidance.data(), columns, fr, inverse_step * 2.5);
+    reject_small_direct_components(field, fine_guidance.data(), columns, fr, inverse_step * 2.5,
+                                   MINIMUM_DIRECT_COMPONENT_NODES);
+    fit_local_depth_planes(field, fine_guidance.data(), columns, fr, inverse_step * 4.0);
+    seconds[4] = since(t);
+    t = clock::now();
+    for (size_t target_index = 0; target_index < n_views; ++target_index) {
+        if (target_index == reference_index || !inputs[target_index].accepted || !inputs[target_index].camera)
+            continue;
+        auto decisions = target_decisions(inputs, reference_index, target_index, field, fine_guidance.data(),
+                                          columns, fr, step, inverse_step, options, fine_rows.data());
+        (void)decisions;
+    }
+    seconds[5] = since(t);
+    counts[0] = sn;
+    counts[1] = fn;
     return CHIARO_OK;
 }
 

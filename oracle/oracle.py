@@ -118,6 +118,8 @@ def lib():
                                                 C.c_size_t, C.c_size_t, P(C.c_float), P(C.c_float), P(C.c_float)]),
             "oracle_sgm_u16": (None, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, C.c_size_t,
                                       P(C.c_uint16), P(C.c_uint16)]),
+            "oracle_stage_sample": (C.c_int, [P(ViewC), C.c_size_t, C.c_size_t, P(DepthOptionsC), P(C.c_uint8),
+                                              C.c_int, P(C.c_double), P(C.c_uint64)]),
             "oracle_luminance_half_mesh": (None, [P(C.c_uint16), C.c_size_t, C.c_size_t, C.c_float, C.c_float,
                                                   P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_float),
                                                   P(C.c_float)]),
