@@ -81,6 +81,34 @@ class CameraC(C.Structure):
     ]
 
 
+class BandOptionsC(C.Structure):
+    """chiaro_band_options: the learned-band form of the coarse search."""
+
+    _fields_ = [
+        ("params", C.c_void_p),
+        ("tile", C.c_uint64),
+        ("band", C.c_uint64),
+        ("margin", C.c_uint64),
+        ("contradicted_fraction", C.c_float),
+        ("_pad0", C.c_int32),
+    ]
+
+
+class BandReportC(C.Structure):
+    """chiaro_band_report: what a coarse search did."""
+
+    _fields_ = [
+        ("tiles", C.c_uint64),
+        ("edge_tiles", C.c_uint64),
+        ("consistency_tiles", C.c_uint64),
+        ("fallback_tiles", C.c_uint64),
+        ("windows", C.c_uint64),
+        ("window_nodes", C.c_uint64),
+        ("ms", C.c_float * 7),
+        ("_pad0", C.c_int32),
+    ]
+
+
 class SgmInstanceC(C.Structure):
     """chiaro_sgm_instance: one SGM instance of a batch (device pointers)."""
 

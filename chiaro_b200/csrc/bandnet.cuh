@@ -49,36 +49,28 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
     return *reinterpret_cast<const unsigned *>(&v);
 }
 
+// The band proposal's sampled labels: 16 finite labels spread evenly over
+// 1..labels-1, the first and the last included.
+__host__ __device__ inline int net_sample_label(int b, int labels) { return 1 + (b * (labels - 2) + 7) / 15; }
+
 // Input features of one node: the reference luminance at the node (guidance / 8);
-// per bin of the finite labels, the bin's minimum cost minus the node's; the
-// first cost argmin over the finite labels, as (argmin - 1) / (labels - 2); and
-// the node's minimum cost. A warp per node: lanes read consecutive labels, the
-// minima are reduced by shuffles (a minimum does not depend on its order) and the
-// argmin is the smallest label holding the minimum; lane k writes channel k.
-__global__ void net_features_kernel(const float *__restrict__ costs, const float *__restrict__ guidance, int nodes,
-                                    int labels, __nv_bfloat16 *__restrict__ features) {
+// the costs of the 16 sampled labels minus the lowest of them; the first sampled
+// label holding that lowest cost, as (label - 1) / (labels - 2); and the lowest cost.
+// Rows of `costs` hold `stride` values: the full volume (stride == labels, a label's
+// cost at its index) or the pre-pass's compact rows (label 0, then the sampled labels
+// in order). A warp per node: lane b < 16 reads sampled label b; the minimum and its
+// first label come from shuffles; lane k writes channel k.
+__global__ void net_features_kernel(const float *__restrict__ costs, int stride, const float *__restrict__ guidance,
+                                    int nodes, int labels, __nv_bfloat16 *__restrict__ features) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int node = (int)(((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (node >= nodes) return;  // whole warp
-    const float *c = costs + (size_t)node * labels;
-    const int finite = labels - 1;
-    float bins[NET_BINS];
-#pragma unroll
-    for (int b = 0; b < NET_BINS; ++b) bins[b] = INFINITY;
-    float lowest = INFINITY;
-    int argmin = labels;
-    for (int l = 1 + lane; l < labels; l += 32) {
-        const float v = __ldcs(c + l);
-        const int bin = (NET_BINS * l + finite - 1) / finite - 1;  // l0(bin) <= l < l0(bin + 1)
-#pragma unroll
-        for (int b = 0; b < NET_BINS; ++b)
-            if (b == bin) bins[b] = fminf(bins[b], v);
-        if (v < lowest) {  // a lane's labels rise, so this keeps its first minimum
-            lowest = v;
-            argmin = l;
-        }
-    }
+    const int label = lane < NET_BINS ? net_sample_label(lane, labels) : labels;
+    const float v = lane < NET_BINS ? __ldg(costs + (size_t)node * stride + (stride == labels ? label : 1 + lane))
+                                    : INFINITY;
+    float lowest = v;
+    int argmin = label;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         const float ov = __shfl_xor_sync(full, lowest, off);
@@ -87,15 +79,12 @@ __global__ void net_features_kernel(const float *__restrict__ costs, const float
             lowest = ov;
             argmin = oa;
         }
-#pragma unroll
-        for (int b = 0; b < NET_BINS; ++b) bins[b] = fminf(bins[b], __shfl_xor_sync(full, bins[b], off));
     }
-    if (argmin == labels) argmin = 1;  // no finite label at all: the first
+    if (argmin == labels) argmin = 1;  // every sampled cost NaN: the first label
+    const float bin = __shfl_sync(full, v, (lane + 31) & 31);  // lane 1 + b: sampled label b
     float value = 0.0f;
     if (lane == 0) value = guidance[node] * 0.125f;
-#pragma unroll
-    for (int b = 0; b < NET_BINS; ++b)
-        if (lane == 1 + b) value = bins[b] - lowest;
+    if (lane >= 1 && lane <= NET_BINS) value = bin - lowest;
     if (lane == NET_INPUTS - 2) value = (float)(argmin - 1) / (float)(labels - 2);
     if (lane == NET_INPUTS - 1) value = lowest;
     features[(size_t)node * NET_CH + lane] = __float2bfloat16_rn(value);

@@ -10,6 +10,14 @@
 // and the D = planes + 1 labels leave no nearly empty warp. Last, a thread per
 // label aggregates the views (depth.rs:1761-1770) and writes the label-minor
 // score and cost rows (node-major [N][D], as the reference lays them out).
+//
+// The same kernel scores a subset of the labels for the learned band: each node
+// scores `slots` labels, slot 0 being label 0 (the global warp) and the others
+// either one label list shared by every node (the band proposal's sampled labels)
+// or its tile's band [O, O + slots - 1); rows are then [N][slots]. A node list
+// restricts the CTAs to some nodes (the fallback windows), each writing the row
+// of its list position. A label's score and cost do not depend on which other
+// labels a node scores, so every subset holds the full volume's values bit for bit.
 #pragma once
 
 #include "zncc.cuh"
@@ -31,7 +39,24 @@ struct CostParams {
     int minimum_support, best_view_count;
     float *scores, *costs, *guidance;
     uint8_t *tested;
+    // label subsets (slots == labels with no list and no bands: the full volume)
+    int slots;                  // labels scored per node; rows of the outputs
+    const int *label_list;      // [slots]: slot -> label, or nullptr
+    const int *band_first;      // [tiles_y][tiles_x]: slot s > 0 -> label band_first[tile] + s - 1, or nullptr
+    int band_tile, band_tiles_x;
+    const int *node_list;       // CTA b scores node node_list[b] into output row b, or nullptr
 };
+
+// The label of a slot of `node` (see CostParams).
+__device__ __forceinline__ int cost_slot_label(const CostParams &p, int node, int slot) {
+    if (p.label_list) return __ldg(p.label_list + slot);
+    if (p.band_first) {
+        if (slot == 0) return 0;
+        const int row = node / p.columns, column = node - row * p.columns;
+        return __ldg(p.band_first + (row / p.band_tile) * p.band_tiles_x + column / p.band_tile) + slot - 1;
+    }
+    return slot;
+}
 
 constexpr int COST_THREADS = 128;
 constexpr int COST_MAX_CHUNKS = 32;  // item chunks listed per barrier pair
@@ -88,8 +113,9 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
     const unsigned full = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int warps = COST_THREADS / 32;
-    const int node = blockIdx.x;
-    const int V = p.n_targets, D = p.labels;
+    const int out_row = blockIdx.x;
+    const int node = p.node_list ? __ldg(p.node_list + out_row) : out_row;
+    const int V = p.n_targets, D = p.slots, full_labels = p.labels;
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
     const int total = V * D;
     const int chunks = (total + COST_THREADS - 1) / COST_THREADS;
@@ -148,9 +174,9 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         }
         s.gh[i] = make_double2((double)qx * 0.5, (double)qy * 0.5);
     }
-    // displacement of every (target, label) item, view-major: item = v * D + label
+    // displacement of every (target, slot) item, view-major: item = v * D + slot
     for (int item = tid; item < total; item += COST_THREADS) {
-        const int v = item / D, label = item - v * D;
+        const int v = item / D, label = cost_slot_label(p, node, item - v * D);
         ViewGeom g;
         geom_from_rec(p.geometry[(size_t)node * V + v], origin, g);
         double ddx = 0.0, ddy = 0.0;
@@ -259,27 +285,29 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
 
     // ---- aggregate the views per label and price the label (depth.rs:1233-1246)
     int any_finite = 0;
-    for (int label = tid; label < D; label += COST_THREADS) {
+    for (int slot = tid; slot < D; slot += COST_THREADS) {
+        const int label = cost_slot_label(p, node, slot);
         float sc[MAX_VIEWS];
-        for (int v = 0; v < V; ++v) sc[v] = s.score[v * D + label];
+        for (int v = 0; v < V; ++v) sc[v] = s.score[v * D + slot];
         float agg;
         float score = aggregate_scores(sc, V, p.minimum_support, p.best_view_count, agg) ? agg : NAN;
         float cost;
         if (isfinite(score)) {
             any_finite = 1;
-            float near_prior = label == 0 ? 0.0f : NEAR_DEPTH_PRIOR * (float)(label - 1) / (float)(D - 2);
+            float near_prior =
+                label == 0 ? 0.0f : NEAR_DEPTH_PRIOR * (float)(label - 1) / (float)(full_labels - 2);
             cost = clampf_r(1.0f - score, 0.0f, 2.0f) + near_prior;
         } else {
             cost = MISSING_COST;
         }
-        size_t o = (size_t)node * D + label;
+        size_t o = (size_t)out_row * D + slot;
         p.scores[o] = score;
         p.costs[o] = cost;
     }
     const bool tested = __syncthreads_or(any_finite);
     if (tid == 0) {
-        p.tested[node] = tested;
-        p.guidance[node] = patch.centre;  // reference_guidance (depth.rs:1824-1832)
+        p.tested[out_row] = tested;
+        p.guidance[out_row] = patch.centre;  // reference_guidance (depth.rs:1824-1832)
     }
 }
 

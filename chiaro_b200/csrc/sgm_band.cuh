@@ -36,9 +36,11 @@ __device__ __forceinline__ int band_offset_at(const BandGrid &b, int row, int co
 // Banded path costs of every path of every direction; pass k writes paths + k * pitch ([N][band]).
 // Each step loads its own costs: the kernel stays small enough (registers) for all paths of
 // a full-resolution grid to be resident at once, and the other warps hide the load.
+// Cost rows are either full ([N][labels]: label l at l) or the banded cost volume's
+// compact rows ([N][1 + band]: label 0, then the node's band in order; compact != 0).
 __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_band_paths_kernel(
     const float *__restrict__ data, const float *__restrict__ guidance, BandGrid grid, float *__restrict__ paths,
-    size_t pitch, int columns, int rows, int labels) {
+    size_t pitch, int columns, int rows, int labels, int compact) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
@@ -59,7 +61,8 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_band_paths_kernel(
     const long node0 = (long)r0 * columns + c0;
     float *wp = paths + (size_t)pass * pitch + (size_t)node0 * band + lane;
     int offset = band_offset_at(grid, r0, c0);
-    float prev = valid ? __ldg(data + (size_t)node0 * labels + offset + lane) : INFINITY;
+    const int stride = compact ? 1 + band : labels;
+    float prev = valid ? __ldg(data + (size_t)node0 * stride + (compact ? 1 : offset) + lane) : INFINITY;
     if (valid) *wp = prev;
     float p1s = 0.0f, p2s = 0.0f;
     int offsets = 0;
@@ -80,7 +83,7 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_band_paths_kernel(
             const long node = node0 + (long)(base + j) * node_step;
             const int o = __shfl_sync(full, offsets, j);
             const float p1 = __shfl_sync(full, p1s, j), p2 = __shfl_sync(full, p2s, j);
-            const float cur = valid ? __ldg(data + (size_t)node * labels + o + lane) : INFINITY;
+            const float cur = valid ? __ldg(data + (size_t)node * stride + (compact ? 1 : o) + lane) : INFINITY;
             const float minimum_previous = warp_min_f32(prev);
             const int s = lane + (o - offset);  // this label's slot in the previous band
             const float same = __shfl_sync(full, prev, s & 31);

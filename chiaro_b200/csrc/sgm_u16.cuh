@@ -9,7 +9,14 @@
 // values quantised the same way (at most 922). A path cost is then at most
 // 4608 + 922 = 5530 and the sum of the 8 paths at most 44240, so the recurrence
 // and the sum are exact in 16 bits: no saturation ever applies to a real label.
-// Integer addition is associative, so the 8 directions need no summation order.
+// Integer addition is associative, so the 8 directions need no summation order:
+// every path adds its costs straight into one packed aggregate with a 32-bit
+// atomic add (a red.global.add, resolved in L2). A real label's 8-path sum never
+// exceeds 16 bits, so no carry crosses into the pair's high half; the pad label
+// of an odd count (0xFFFF on every path) sits in the high half, where its carry
+// leaves the word, and no one reads it. No per-direction buffer is written: the
+// cells cross DRAM about once each way (quantised costs in, aggregate out) while
+// the 8 walks read the costs and add into the aggregate in L2.
 //
 // Labels travel in pairs, (2j, 2j + 1) packed in one 32-bit word, and the
 // recurrence runs on both halves at once with __vaddus2 / __vminu2 / __vsub2.
@@ -39,8 +46,9 @@ __device__ __forceinline__ unsigned quantise_sgm_cost(float c) {
 __device__ __forceinline__ unsigned quantise_penalty(float p) { return (unsigned)rintf(p * SGM_Q); }
 
 // f32 [N][D] costs -> u16 pairs [N][pairs], pairs = ceil(D / 2); the pad label is 0xFFFF.
+// The aggregate's words are cleared in the same pass.
 __global__ void sgm_quantise_kernel(const float *__restrict__ costs, int nodes, int labels,
-                                    unsigned *__restrict__ quantised) {
+                                    unsigned *__restrict__ quantised, unsigned *__restrict__ aggregate) {
     const int pairs = (labels + 1) / 2;
     const long total = (long)nodes * pairs;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
@@ -49,16 +57,17 @@ __global__ void sgm_quantise_kernel(const float *__restrict__ costs, int nodes, 
         const unsigned lo = quantise_sgm_cost(c[0]);
         const unsigned hi = 2 * j + 1 < labels ? quantise_sgm_cost(c[1]) : SGM_U16_PAD;
         quantised[i] = lo | (hi << 16);
+        aggregate[i] = 0u;
     }
 }
 
-// Path costs of every path of every direction; pass k writes paths + k * pitch (words).
+// Every path of every direction, each adding its path costs into the packed
+// aggregate [N][pairs] (cleared beforehand).
 template <int K>
 __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_u16_paths_kernel(const unsigned *__restrict__ data,
                                                                               const float *__restrict__ guidance,
-                                                                              unsigned *__restrict__ paths,
-                                                                              size_t pitch, int columns, int rows,
-                                                                              int labels) {
+                                                                              unsigned *__restrict__ aggregate,
+                                                                              int columns, int rows, int labels) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
@@ -83,13 +92,13 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_u16_paths_kernel(c
     const int node0 = r0 * columns + c0;
     const size_t e0 = (size_t)node0 * pairs + lane;
     const unsigned *pf = data + e0;
-    unsigned *wp = paths + (size_t)pass * pitch + e0;
+    unsigned *wp = aggregate + e0;
     const float *gp = guidance + node0;
     unsigned prev[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         prev[k] = valid[k] ? __ldg(pf + 32 * k) : full;
-        if (valid[k]) wp[32 * k] = prev[k];
+        if (valid[k]) atomicAdd(wp + 32 * k, prev[k]);
     }
     unsigned ring[P][K];
 #pragma unroll
@@ -148,18 +157,17 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_u16_paths_kernel(c
                     best = __vminu2(best, jump);
                     const unsigned v = __vaddus2(cur[k], __vsub2(best, floor2));
                     prev[k] = v;
-                    if (valid[k]) wp[32 * k] = v;
+                    if (valid[k]) atomicAdd(wp + 32 * k, v);
                 }
             }
         }
     }
 }
 
-// The 8 path costs summed per cell, the u16 aggregate written unpadded ([N][D],
-// optional) and the winner over labels 1..D-1 (first minimum, optional). A warp per node.
-__global__ void __launch_bounds__(256) sgm_u16_select_kernel(const unsigned *__restrict__ paths, size_t pitch,
-                                                             int nodes, int labels, uint16_t *aggregate,
-                                                             uint16_t *best) {
+// The packed aggregate written unpadded ([N][D], optional) and the winner over
+// labels 1..D-1 (first minimum, optional). A warp per node.
+__global__ void __launch_bounds__(256) sgm_u16_select_kernel(const unsigned *__restrict__ packed, int nodes,
+                                                             int labels, uint16_t *aggregate, uint16_t *best) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -167,10 +175,7 @@ __global__ void __launch_bounds__(256) sgm_u16_select_kernel(const unsigned *__r
     const int pairs = (labels + 1) / 2;
     unsigned key = full;  // (cost << 16) | label: the minimum is the first minimum
     for (int j = lane; j < pairs; j += 32) {
-        const size_t e = (size_t)node * pairs + j;
-        unsigned s = 0u;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) s = __vaddus2(s, __ldcs(paths + k * pitch + e));
+        const unsigned s = __ldcs(packed + (size_t)node * pairs + j);
         const int lo = 2 * j, hi = 2 * j + 1;
         if (aggregate) {
             aggregate[(size_t)node * labels + lo] = (uint16_t)(s & 0xFFFFu);

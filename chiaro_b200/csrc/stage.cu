@@ -32,6 +32,7 @@
 #include "resolution.cuh"
 #include "align.cuh"
 #include "consumers.cuh"
+#include "coarse.cuh"
 
 using namespace chiaro;
 
@@ -261,33 +262,34 @@ void launch_sgm(chiaro_depth_ctx *ctx, const float *data, const float *guidance,
 }
 
 template <int K>
-void sgm_u16_paths(chiaro_depth_ctx *ctx, const unsigned *data, const float *guidance, unsigned *paths, size_t pitch,
+void sgm_u16_paths(chiaro_depth_ctx *ctx, const unsigned *data, const float *guidance, unsigned *aggregate,
                    int columns, int rows, int labels) {
     const unsigned blocks = (unsigned)div_ceil(sgm_total_paths(columns, rows), SGM_PATHS_PER_CTA);
-    sgm_u16_paths_kernel<K><<<blocks, 32 * SGM_PATHS_PER_CTA, 0, ctx->stream>>>(data, guidance, paths, pitch,
-                                                                                columns, rows, labels);
+    sgm_u16_paths_kernel<K><<<blocks, 32 * SGM_PATHS_PER_CTA, 0, ctx->stream>>>(data, guidance, aggregate, columns,
+                                                                                rows, labels);
     CK(cudaGetLastError());
 }
 
-// The quantised SGM (sgm_u16.cuh): quantise, every direction's path costs, sum and winner.
+// The quantised SGM (sgm_u16.cuh): quantise (and clear the aggregate), every direction's
+// paths adding into the one packed aggregate, then the unpacked aggregate and the winner.
 void launch_sgm_u16(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, int columns, int rows,
                     int labels, uint16_t *aggregate, uint16_t *best) {
     const size_t nodes = (size_t)columns * rows, pairs = (size_t)(labels + 1) / 2;
-    const size_t words = nodes * pairs, pitch = (words + 63) / 64 * 64;
+    const size_t words = nodes * pairs;
     unsigned *quantised = dbuf<unsigned>(ctx, "sgm16.costs", words);
-    unsigned *paths = dbuf<unsigned>(ctx, "sgm16.paths", 8 * pitch);
+    unsigned *packed = dbuf<unsigned>(ctx, "sgm16.aggregate", words);
     const unsigned qblocks = (unsigned)std::min<size_t>(div_ceil(words, 256), (size_t)ctx->sm_count * 16);
-    sgm_quantise_kernel<<<qblocks, 256, 0, ctx->stream>>>(costs, (int)nodes, labels, quantised);
+    sgm_quantise_kernel<<<qblocks, 256, 0, ctx->stream>>>(costs, (int)nodes, labels, quantised, packed);
     CK(cudaGetLastError());
     switch ((int)((pairs + 31) / 32)) {
-        case 1: sgm_u16_paths<1>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
-        case 2: sgm_u16_paths<2>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
-        case 3: sgm_u16_paths<3>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
-        case 4: sgm_u16_paths<4>(ctx, quantised, guidance, paths, pitch, columns, rows, labels); break;
+        case 1: sgm_u16_paths<1>(ctx, quantised, guidance, packed, columns, rows, labels); break;
+        case 2: sgm_u16_paths<2>(ctx, quantised, guidance, packed, columns, rows, labels); break;
+        case 3: sgm_u16_paths<3>(ctx, quantised, guidance, packed, columns, rows, labels); break;
+        case 4: sgm_u16_paths<4>(ctx, quantised, guidance, packed, columns, rows, labels); break;
         default: throw CudaError{cudaErrorInvalidValue, "labels exceed 256"};
     }
-    sgm_u16_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, ctx->stream>>>(paths, pitch, (int)nodes,
-                                                                                       labels, aggregate, best);
+    sgm_u16_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, ctx->stream>>>(packed, (int)nodes, labels,
+                                                                                       aggregate, best);
     CK(cudaGetLastError());
 }
 
@@ -516,38 +518,19 @@ int run_batch(chiaro_depth_ctx *ctx, const chiaro_sgm_instance *in, size_t n, si
 }
 
 // ---- banded SGM with windowed fallback (sgm_band.cuh) ----------------------------------
-int run_band(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, int columns, int rows, int labels,
-             const int *tile_offset, int tile, int band, int margin, int *winner, uint8_t *fallback) {
-    cudaStream_t s = ctx->stream;
-    const int tiles_x = (columns + tile - 1) / tile, tiles_y = (rows + tile - 1) / tile, tiles = tiles_x * tiles_y;
-    int *bad = dbuf<int>(ctx, "band.bad", 1);
-    CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
-    band_check_kernel<<<(unsigned)div_ceil(tiles, 256), 256, 0, s>>>(tile_offset, tiles, labels, band, bad);
-    CK(cudaGetLastError());
-    int h_bad = 0;
-    CK(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (h_bad) return CHIARO_ERR_ARGUMENT;
-    const BandGrid grid{tile_offset, tile, tiles_x, band};
-    const size_t nodes = (size_t)columns * rows, pitch = (nodes * band + 63) / 64 * 64;
-    float *paths = dbuf<float>(ctx, "band.paths", 8 * pitch);
-    CK(cudaMemsetAsync(fallback, 0, tiles, s));
-    sgm_band_paths_kernel<<<(unsigned)div_ceil(sgm_total_paths(columns, rows), SGM_PATHS_PER_CTA),
-                            32 * SGM_PATHS_PER_CTA, 0, s>>>(costs, guidance, grid, paths, pitch, columns, rows, labels);
-    CK(cudaGetLastError());
-    sgm_band_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, s>>>(paths, pitch, grid, columns, rows,
-                                                                               labels, winner, fallback);
-    CK(cudaGetLastError());
-    std::vector<uint8_t> flags(tiles);
-    CK(cudaMemcpyAsync(flags.data(), fallback, tiles, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    // fallback tiles as greedy rectangles in raster order (widest run, then as many
-    // rows of it as are all flagged), each with its window of margin nodes around it
+// Fallback tiles as greedy rectangles in raster order (the widest run, then as many rows
+// of it as are all flagged), each with its window of `margin` nodes around it; the
+// windows' cost and node offsets pack them one after another ([cells][labels], [cells]).
+// Where the windows would cover at least the grid, one window, the whole grid, decides
+// every fallback tile instead. most = the largest rectangle's node count.
+std::vector<BandWindow> fallback_windows(const std::vector<uint8_t> &flags, int tiles_x, int tiles_y, int tile,
+                                         int columns, int rows, int margin, int labels, size_t &cost_floats,
+                                         size_t &node_floats, int &most) {
     std::vector<BandWindow> windows;
-    std::vector<uint8_t> taken(tiles, 0);
+    std::vector<uint8_t> taken(flags.size(), 0);
     auto open = [&](int x, int y) { return flags[y * tiles_x + x] && !taken[y * tiles_x + x]; };
-    size_t cost_floats = 0, node_floats = 0;
-    int most = 0;
+    cost_floats = node_floats = 0;
+    most = 0;
     for (int ty = 0; ty < tiles_y; ++ty)
         for (int tx = 0; tx < tiles_x; ++tx) {
             if (!open(tx, ty)) continue;
@@ -575,15 +558,47 @@ int run_band(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, i
             most = std::max(most, win.tc * win.tr);
             windows.push_back(win);
         }
-    if (node_floats >= nodes) {
-        // the windows would cover at least the grid: one full-range SGM over the whole
-        // grid decides the fallback tiles' nodes instead
+    if (node_floats >= (size_t)columns * rows) {
         BandWindow whole{};
         whole.wc = whole.tc = columns;
         whole.wr = whole.tr = rows;
         windows.assign(1, whole);
         most = columns * rows;
+        cost_floats = (size_t)columns * rows * labels;
+        node_floats = (size_t)columns * rows;
     }
+    return windows;
+}
+
+int run_band(chiaro_depth_ctx *ctx, const float *costs, const float *guidance, int columns, int rows, int labels,
+             const int *tile_offset, int tile, int band, int margin, int *winner, uint8_t *fallback) {
+    cudaStream_t s = ctx->stream;
+    const int tiles_x = (columns + tile - 1) / tile, tiles_y = (rows + tile - 1) / tile, tiles = tiles_x * tiles_y;
+    int *bad = dbuf<int>(ctx, "band.bad", 1);
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    band_check_kernel<<<(unsigned)div_ceil(tiles, 256), 256, 0, s>>>(tile_offset, tiles, labels, band, bad);
+    CK(cudaGetLastError());
+    int h_bad = 0;
+    CK(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h_bad) return CHIARO_ERR_ARGUMENT;
+    const BandGrid grid{tile_offset, tile, tiles_x, band};
+    const size_t nodes = (size_t)columns * rows, pitch = (nodes * band + 63) / 64 * 64;
+    float *paths = dbuf<float>(ctx, "band.paths", 8 * pitch);
+    CK(cudaMemsetAsync(fallback, 0, tiles, s));
+    sgm_band_paths_kernel<<<(unsigned)div_ceil(sgm_total_paths(columns, rows), SGM_PATHS_PER_CTA),
+                            32 * SGM_PATHS_PER_CTA, 0, s>>>(costs, guidance, grid, paths, pitch, columns, rows, labels, 0);
+    CK(cudaGetLastError());
+    sgm_band_select_kernel<<<(unsigned)div_ceil(nodes * 32, 256), 256, 0, s>>>(paths, pitch, grid, columns, rows,
+                                                                               labels, winner, fallback);
+    CK(cudaGetLastError());
+    std::vector<uint8_t> flags(tiles);
+    CK(cudaMemcpyAsync(flags.data(), fallback, tiles, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    size_t cost_floats = 0, node_floats = 0;
+    int most = 0;
+    std::vector<BandWindow> windows =
+        fallback_windows(flags, tiles_x, tiles_y, tile, columns, rows, margin, labels, cost_floats, node_floats, most);
     ctx->band_windows = (int)windows.size();
     if (!windows.empty()) {
         BandWindow *d_windows = dbuf<BandWindow>(ctx, "band.windows", windows.size());
@@ -863,10 +878,12 @@ NetState net_state(chiaro_depth_ctx *ctx, int images, int height, int width) {
     return s;
 }
 
-void net_features(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, const float *guidance, int labels) {
+// Features from full-volume rows (stride == labels) or the pre-pass's compact rows (stride 17).
+void net_features(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, const float *guidance, int labels,
+                  int stride) {
     const int nodes = (int)s.pixels;
-    net_features_kernel<<<(unsigned)div_ceil((size_t)nodes * 32, 256), 256, 0, ctx->stream>>>(costs, guidance, nodes,
-                                                                                               labels, s.act[0]);
+    net_features_kernel<<<(unsigned)div_ceil((size_t)nodes * 32, 256), 256, 0, ctx->stream>>>(costs, stride, guidance,
+                                                                                               nodes, labels, s.act[0]);
     CK(cudaGetLastError());
 }
 
@@ -927,6 +944,278 @@ __global__ void net_targets_kernel(const int *__restrict__ winners, long pixels,
 }
 
 // ---- the stage ------------------------------------------------------------------------
+// ---- the coarse depth search (coarse.cuh): plain, or with the learned band -----------
+struct BandSpec {
+    const float *params;  // the network's parameters (device), or nullptr for the naive band
+    int tile, band, margin;
+    float fraction;  // cross-view fallback above this fraction of contradicted nodes (>= 1: off)
+};
+
+// The coarse grid's cost volume for `slots` labels per node (see CostParams), over all
+// nodes or the `n_rows` nodes of node_list; rows [n_rows][slots].
+struct CoarseGrid {
+    std::vector<int> targets;
+    int V, D, columns, rows, step;
+    double *labels;
+    float *spatial;
+    GeomRec *geometry;
+    TapLattice lattice;
+    DevView *views;
+};
+
+void coarse_cost(chiaro_depth_ctx *ctx, const CoarseGrid &g, int reference, const chiaro_depth_options &o, int slots,
+                 const int *label_list, const BandGrid *band, const int *node_list, size_t n_rows, float *scores,
+                 float *costs, float *guidance, uint8_t *tested) {
+    if (n_rows == 0) return;
+    CostParams p{};
+    p.geometry = g.geometry;
+    p.views = g.views;
+    p.reference = reference;
+    p.n_targets = g.V;
+    for (int v = 0; v < g.V; ++v) p.targets[v] = g.targets[v];
+    p.columns = g.columns;
+    p.rows = g.rows;
+    p.step = g.step;
+    p.labels = g.D;
+    p.slots = slots;
+    p.label_list = label_list;
+    if (band) {
+        p.band_first = band->tile_offset;
+        p.band_tile = band->tile;
+        p.band_tiles_x = band->tiles_x;
+    }
+    p.node_list = node_list;
+    p.label_depth = g.labels;
+    p.spatial = g.spatial;
+    p.radius = (int)o.patch_radius;
+    p.lattice = g.lattice;
+    p.minimum_support = (int)o.minimum_support;
+    p.best_view_count = (int)std::min<uint64_t>(o.best_view_count, MAX_VIEWS);
+    p.scores = scores;
+    p.costs = costs;
+    p.guidance = guidance;
+    p.tested = tested;
+    const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
+    const size_t smem = node_smem_bytes(g.V, taps, slots);
+    if ((size_t)g.V * slots > 65535 || smem > 200 * 1024)
+        throw CudaError{cudaErrorInvalidValue, "cost volume: targets x labels exceed the node CTA's shared memory"};
+    cost_volume_kernel<<<(unsigned)n_rows, COST_THREADS, smem, ctx->stream>>>(p);
+    CK(cudaGetLastError());
+}
+
+// The coarse search of the stage's reference grid (depth.rs:1187-1467 up to the winner):
+// spec == nullptr runs the plain form (full cost volume, SGM, first minimum over labels
+// 1..D-1, bit-identical to the stage's); otherwise the learned-band form (coarse.cuh).
+// prepass_only stops after the pre-pass and writes its rows and guidance out.
+int run_coarse(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, int reference, const chiaro_depth_options &o,
+               const BandSpec *spec, int *winner, uint8_t *tested_out, int *offsets_out, uint8_t *fallback_out,
+               chiaro_band_report *report, float *prepass_out, float *guidance_out) {
+    cudaStream_t s = ctx->stream;
+    set_smem_limits();
+    CoarseGrid g{};
+    const int n_views = (int)h_views.size();
+    for (int i = 0; i < n_views; ++i)
+        if (i != reference && h_views[i].accepted && h_views[i].has_camera) g.targets.push_back(i);
+    g.V = (int)g.targets.size();
+    g.D = (int)o.planes + 1;
+    g.step = (int)std::max<uint64_t>(o.grid_step, 4);
+    g.columns = (int)div_ceil(h_views[reference].width, g.step) + 1;
+    g.rows = (int)div_ceil(h_views[reference].height, g.step) + 1;
+    const int D = g.D, radius = (int)o.patch_radius;
+    const size_t N = (size_t)g.columns * g.rows;
+    if (spec && (g.V < 1 || D < PREPASS_SLOTS + 2)) return CHIARO_ERR_ARGUMENT;
+    auto finite_depths = inverse_depth_samples(o.near_depth, o.far_depth, o.planes);
+    std::vector<double> labels(D);
+    labels[0] = NAN;
+    for (int l = 1; l < D; ++l) labels[l] = finite_depths[o.planes - l];
+    auto sp = spatial_weights(radius);
+    g.labels = dbuf<double>(ctx, "coarse.labels", D);
+    g.spatial = dbuf<float>(ctx, "coarse.spatial", sp.size());
+    upload(ctx, g.labels, labels.data(), D);
+    upload(ctx, g.spatial, sp.data(), sp.size());
+    for (int t : g.targets) {
+        const PlaneRef &lp = h_views[t].luma;
+        h_views[t].quads = dbuf<float4>(ctx, "quads" + std::to_string(t),
+                                        (size_t)quad_pair_stride(lp.width) * ((lp.height + 1) / 2));
+    }
+    g.views = dbuf<DevView>(ctx, "coarse.views", n_views);
+    upload(ctx, g.views, h_views.data(), n_views);
+    g.geometry = dbuf<GeomRec>(ctx, "coarse_geometry", N * std::max(g.V, 1));
+    if (g.V > 0 && g.step % 2 == 0) {
+        g.lattice.margin = radius;
+        g.lattice.columns = (int)((size_t)(g.columns - 1) * g.step / 2 + 2 * (size_t)radius + 1);
+        g.lattice.rows = (int)((size_t)(g.rows - 1) * g.step / 2 + 2 * (size_t)radius + 1);
+        g.lattice.planes = dbuf<float2>(ctx, "coarse.lattice", (size_t)(g.V + 1) * g.lattice.columns * g.lattice.rows);
+    }
+    CK(cudaEventRecord(ctx->events[0], s));
+    launch_geometry(ctx, g.views, reference, g.targets, g.columns, g.rows, g.step, g.geometry);
+    if (g.lattice.planes) {
+        LatticeParams p{};
+        p.views = g.views;
+        p.reference = reference;
+        p.n_targets = g.V;
+        for (int v = 0; v < g.V; ++v) p.targets[v] = g.targets[v];
+        p.columns = g.lattice.columns;
+        p.rows = g.lattice.rows;
+        p.margin = g.lattice.margin;
+        p.out = const_cast<float2 *>(g.lattice.planes);
+        tap_lattice_kernel<<<blocks_for((size_t)g.lattice.columns * g.lattice.rows, 256), 256, 0, s>>>(p);
+        CK(cudaGetLastError());
+    }
+    for (int t : g.targets) {
+        const PlaneRef &lp = h_views[t].luma;
+        quad_plane_kernel<<<blocks_for((size_t)lp.width * lp.height, 256), 256, 0, s>>>(
+            lp.data, lp.width, lp.height, quad_pair_stride(lp.width), const_cast<float4 *>(h_views[t].quads));
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(ctx->events[1], s));
+    uint8_t *tested = dbuf<uint8_t>(ctx, "coarse.tested", N);
+    float *guidance = dbuf<float>(ctx, "coarse.guidance", N);
+    chiaro_band_report rep{};
+    if (!spec) {
+        CK(cudaEventRecord(ctx->events[2], s));
+        CK(cudaEventRecord(ctx->events[3], s));
+        float *scores = dbuf<float>(ctx, "coarse.scores", N * D), *costs = dbuf<float>(ctx, "coarse.costs", N * D);
+        CK(cudaMemsetAsync(tested, 0, N, s));
+        coarse_cost(ctx, g, reference, o, D, nullptr, nullptr, nullptr, N, scores, costs, guidance, tested);
+        CK(cudaEventRecord(ctx->events[4], s));
+        float *aggregate = dbuf<float>(ctx, "coarse.aggregate", N * D);
+        launch_sgm(ctx, costs, guidance, aggregate, g.columns, g.rows, D);
+        aggregate_winner_kernel<<<(unsigned)div_ceil(N * 32, 256), 256, 0, s>>>(aggregate, (int)N, D, winner);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ctx->events[5], s));
+        CK(cudaEventRecord(ctx->events[6], s));
+    } else {
+        const int tile = spec->tile, band = spec->band;
+        const int tiles_x = (g.columns + tile - 1) / tile, tiles_y = (g.rows + tile - 1) / tile;
+        const int tiles = tiles_x * tiles_y;
+        // pre-pass: label 0 and the 16 sampled labels
+        std::vector<int> list(PREPASS_SLOTS, 0);
+        for (int b = 0; b < NET_BINS; ++b) list[1 + b] = net_sample_label(b, D);
+        int *d_list = dbuf<int>(ctx, "coarse.prepass_labels", PREPASS_SLOTS);
+        upload(ctx, d_list, list.data(), PREPASS_SLOTS);
+        float *pre_scores = dbuf<float>(ctx, "coarse.prepass_scores", N * PREPASS_SLOTS);
+        float *pre_costs = dbuf<float>(ctx, "coarse.prepass_costs", N * PREPASS_SLOTS);
+        CK(cudaMemsetAsync(tested, 0, N, s));
+        coarse_cost(ctx, g, reference, o, PREPASS_SLOTS, d_list, nullptr, nullptr, N, pre_scores, pre_costs, guidance,
+                    tested);
+        CK(cudaEventRecord(ctx->events[2], s));
+        if (prepass_out) {
+            CK(cudaMemcpyAsync(prepass_out, pre_costs, N * PREPASS_SLOTS * sizeof(float), cudaMemcpyDeviceToDevice, s));
+            if (guidance_out) CK(cudaMemcpyAsync(guidance_out, guidance, N * sizeof(float), cudaMemcpyDeviceToDevice, s));
+            if (tested_out) CK(cudaMemcpyAsync(tested_out, tested, N, cudaMemcpyDeviceToDevice, s));
+            CK(cudaStreamSynchronize(s));
+            return CHIARO_OK;
+        }
+        // the band proposal: the network on the pre-pass's costs, or the naive band
+        int *offsets = dbuf<int>(ctx, "coarse.band_offsets", tiles);
+        if (spec->params) {
+            NetState ns = net_state(ctx, 1, g.rows, g.columns);
+            net_features(ctx, ns, pre_costs, guidance, D, PREPASS_SLOTS);
+            net_forward(ctx, ns, spec->params);
+            net_tile_offsets_kernel<<<(unsigned)div_ceil(tiles, 128), 128, 0, s>>>(ns.y, g.columns, g.rows, D, tile,
+                                                                                   band, offsets);
+        } else {
+            naive_band_offsets_kernel<<<(unsigned)div_ceil(tiles, 128), 128, 0, s>>>(pre_costs, g.columns, g.rows, D,
+                                                                                     tile, band, offsets);
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ctx->events[3], s));
+        // the banded cost volume: label 0 and each tile's band
+        const BandGrid grid{offsets, tile, tiles_x, band};
+        float *band_scores = dbuf<float>(ctx, "coarse.band_scores", N * (1 + band));
+        float *band_costs = dbuf<float>(ctx, "coarse.band_costs", N * (1 + band));
+        uint8_t *band_tested = dbuf<uint8_t>(ctx, "coarse.band_tested", N);
+        float *band_guidance = dbuf<float>(ctx, "coarse.band_guidance", N);
+        CK(cudaMemsetAsync(band_tested, 0, N, s));
+        coarse_cost(ctx, g, reference, o, 1 + band, nullptr, &grid, nullptr, N, band_scores, band_costs,
+                    band_guidance, band_tested);
+        CK(cudaEventRecord(ctx->events[4], s));
+        // the banded SGM, its winners, the edge and cross-view fallback flags
+        const size_t pitch = (N * band + 63) / 64 * 64;
+        float *paths = dbuf<float>(ctx, "coarse.band_paths", 8 * pitch);
+        uint8_t *fallback = dbuf<uint8_t>(ctx, "coarse.band_fallback", tiles);
+        uint8_t *consistency = dbuf<uint8_t>(ctx, "coarse.band_consistency", tiles);
+        uint8_t *edge = dbuf<uint8_t>(ctx, "coarse.band_edge", tiles);
+        CK(cudaMemsetAsync(fallback, 0, tiles, s));
+        CK(cudaMemsetAsync(consistency, 0, tiles, s));
+        sgm_band_paths_kernel<<<(unsigned)div_ceil(sgm_total_paths(g.columns, g.rows), SGM_PATHS_PER_CTA),
+                                32 * SGM_PATHS_PER_CTA, 0, s>>>(band_costs, guidance, grid, paths, pitch, g.columns,
+                                                                g.rows, D, 1);
+        CK(cudaGetLastError());
+        sgm_band_select_kernel<<<(unsigned)div_ceil(N * 32, 256), 256, 0, s>>>(paths, pitch, grid, g.columns, g.rows,
+                                                                               D, winner, fallback);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(edge, fallback, tiles, cudaMemcpyDeviceToDevice, s));
+        if (spec->fraction < 1.0f) {
+            band_consistency_kernel<<<(unsigned)div_ceil(tiles, 128), 128, 0, s>>>(
+                band_scores, band_tested, winner, grid, g.columns, g.rows, spec->fraction, consistency, fallback);
+            CK(cudaGetLastError());
+        }
+        CK(cudaEventRecord(ctx->events[5], s));
+        std::vector<uint8_t> flags(tiles), edges(tiles), crossed(tiles);
+        CK(cudaMemcpyAsync(flags.data(), fallback, tiles, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(edges.data(), edge, tiles, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(crossed.data(), consistency, tiles, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        size_t cost_floats = 0, node_count = 0;
+        int most = 0;
+        std::vector<BandWindow> windows = fallback_windows(flags, tiles_x, tiles_y, tile, g.columns, g.rows,
+                                                           spec->margin, D, cost_floats, node_count, most);
+        if (!windows.empty()) {
+            // full-range costs of every window's nodes, window after window, in row-major order
+            std::vector<int> nodes(node_count);
+            for (const BandWindow &w : windows)
+                for (int r = 0; r < w.wr; ++r)
+                    for (int c = 0; c < w.wc; ++c)
+                        nodes[w.node_offset + (size_t)r * w.wc + c] = (w.r0 + r) * g.columns + (w.c0 + c);
+            int *d_nodes = dbuf<int>(ctx, "coarse.window_nodes", node_count);
+            upload(ctx, d_nodes, nodes.data(), node_count);
+            BandWindow *d_windows = dbuf<BandWindow>(ctx, "coarse.windows", windows.size());
+            upload(ctx, d_windows, windows.data(), windows.size());
+            float *wscores = dbuf<float>(ctx, "coarse.window_scores", cost_floats);
+            float *wcosts = dbuf<float>(ctx, "coarse.window_costs", cost_floats);
+            float *wguid = dbuf<float>(ctx, "coarse.window_guidance", node_count);
+            uint8_t *wtested = dbuf<uint8_t>(ctx, "coarse.window_tested", node_count);
+            float *wagg = dbuf<float>(ctx, "coarse.window_aggregate", cost_floats);
+            coarse_cost(ctx, g, reference, o, D, nullptr, nullptr, d_nodes, node_count, wscores, wcosts, wguid,
+                        wtested);
+            if (windows.size() == 1 && windows[0].wc == g.columns && windows[0].wr == g.rows) {
+                launch_sgm(ctx, wcosts, wguid, wagg, g.columns, g.rows, D);
+            } else {
+                std::vector<chiaro_sgm_instance> instances(windows.size());
+                for (size_t i = 0; i < windows.size(); ++i) {
+                    const BandWindow &w = windows[i];
+                    instances[i] = chiaro_sgm_instance{wcosts + w.cost_offset, wguid + w.node_offset,
+                                                       wagg + w.cost_offset, (uint64_t)w.wc, (uint64_t)w.wr,
+                                                       (uint64_t)D};
+                }
+                if (int st = run_batch(ctx, instances.data(), instances.size(), 0, 0)) return st;
+            }
+            band_window_winner_kernel<<<dim3((unsigned)div_ceil((size_t)most * 32, 256), (unsigned)windows.size()),
+                                        256, 0, s>>>(wagg, g.columns, D, d_windows, grid, fallback, winner);
+            CK(cudaGetLastError());
+        }
+        CK(cudaEventRecord(ctx->events[6], s));
+        for (int t = 0; t < tiles; ++t) {
+            rep.edge_tiles += edges[t] != 0;
+            rep.consistency_tiles += crossed[t] != 0;
+            rep.fallback_tiles += flags[t] != 0;
+        }
+        rep.tiles = (uint64_t)tiles;
+        rep.windows = windows.size();
+        rep.window_nodes = node_count;
+        if (offsets_out) CK(cudaMemcpyAsync(offsets_out, offsets, tiles * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        if (fallback_out) CK(cudaMemcpyAsync(fallback_out, fallback, tiles, cudaMemcpyDeviceToDevice, s));
+    }
+    if (tested_out) CK(cudaMemcpyAsync(tested_out, tested, N, cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&rep.ms[i], ctx->events[i], ctx->events[i + 1]));
+    CK(cudaEventElapsedTime(&rep.ms[6], ctx->events[0], ctx->events[6]));
+    if (report) *report = rep;
+    return CHIARO_OK;
+}
+
 struct StageOutputs {  // device pointers
     double *depth;
     float *confidence;
@@ -1289,6 +1578,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         p.rows = (int)g.coarse_rows;
         p.step = (int)g.coarse_step;
         p.labels = D;
+        p.slots = D;
         p.label_depth = d_labels;
         p.spatial = d_sp;
         p.radius = radius;
@@ -2195,6 +2485,62 @@ int chiaro_sgm_banded(chiaro_depth_ctx *ctx, const float *costs, const float *gu
     return CHIARO_OK;
 }
 
+// The coarse search's views: device-memory views as the device-buffer stage takes them.
+static int coarse_views(const chiaro_view *views, size_t n_views, size_t reference_index,
+                        const chiaro_depth_options *options, std::vector<DevView> &h_views) {
+    int st = validate(views, n_views, reference_index, options);
+    if (st != CHIARO_OK) return st;
+    h_views.resize(n_views);
+    for (size_t i = 0; i < n_views; ++i)
+        h_views[i] = dev_view(views[i], views[i].luminance, reinterpret_cast<const float2 *>(views[i].warp.points));
+    return CHIARO_OK;
+}
+
+int chiaro_coarse_depth_device(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views,
+                               size_t reference_index, const chiaro_depth_options *options,
+                               const chiaro_band_options *band, int32_t *winner, uint8_t *tested,
+                               int32_t *tile_offsets, uint8_t *tile_fallback, chiaro_band_report *report) {
+    if (!ctx || !winner) return CHIARO_ERR_ARGUMENT;
+    std::vector<DevView> h_views;
+    int st = coarse_views(views, n_views, reference_index, options, h_views);
+    if (st != CHIARO_OK) return st;
+    BandSpec spec{};
+    if (band) {
+        if (band->tile < 1 || band->tile > (uint64_t)NAIVE_MAX_TILE || band->band < 1 || band->band > 32 ||
+            band->band > options->planes || band->margin > 4096 ||
+            !(band->contradicted_fraction >= 0.0f))
+            return CHIARO_ERR_ARGUMENT;
+        spec = BandSpec{band->params, (int)band->tile, (int)band->band, (int)band->margin,
+                        band->contradicted_fraction};
+    }
+    try {
+        CK(cudaSetDevice(ctx->device));
+        return run_coarse(ctx, h_views, (int)reference_index, *options, band ? &spec : nullptr, winner, tested,
+                          tile_offsets, tile_fallback, report, nullptr, nullptr);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+}
+
+int chiaro_band_prepass_device(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views,
+                               size_t reference_index, const chiaro_depth_options *options, float *sampled_costs,
+                               float *guidance, uint8_t *tested) {
+    if (!ctx || !sampled_costs) return CHIARO_ERR_ARGUMENT;
+    std::vector<DevView> h_views;
+    int st = coarse_views(views, n_views, reference_index, options, h_views);
+    if (st != CHIARO_OK) return st;
+    if (options->planes + 1 < (uint64_t)PREPASS_SLOTS + 2) return CHIARO_ERR_ARGUMENT;
+    BandSpec spec{nullptr, 4, 1, 0, 1.0f};
+    try {
+        CK(cudaSetDevice(ctx->device));
+        int scratch = 0;
+        return run_coarse(ctx, h_views, (int)reference_index, *options, &spec, &scratch, tested, nullptr, nullptr,
+                          nullptr, sampled_costs, guidance);
+    } catch (const CudaError &e) {
+        return fail(ctx, e);
+    }
+}
+
 uint64_t chiaro_bandnet_parameter_count(void) { return NET_PARAMS; }
 
 static int bandnet_args(const void *ctx, uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels) {
@@ -2207,8 +2553,8 @@ static int bandnet_args(const void *ctx, uint64_t images, uint64_t columns, uint
 // Batch setup shared by training and the gradient: features, targets, and
 // 1 / (number of scored nodes) from the mask.
 static float bandnet_batch(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, const float *guidance,
-                           const int32_t *winners, const uint8_t *mask, int labels, float **targets) {
-    net_features(ctx, s, costs, guidance, labels);
+                           const int32_t *winners, const uint8_t *mask, int labels, int stride, float **targets) {
+    net_features(ctx, s, costs, guidance, labels, stride);
     *targets = dbuf<float>(ctx, "net.targets", (size_t)s.pixels);
     net_targets_kernel<<<(unsigned)div_ceil((size_t)s.pixels, 256), 256, 0, ctx->stream>>>(winners, s.pixels, labels,
                                                                                            *targets);
@@ -2223,14 +2569,15 @@ static float bandnet_batch(chiaro_depth_ctx *ctx, const NetState &s, const float
 
 int chiaro_bandnet_propose_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
                                   const float *guidance, uint64_t columns, uint64_t rows, uint64_t labels,
-                                  uint64_t tile, uint64_t band, int32_t *tile_offsets, float *centres) {
+                                  uint64_t cost_stride, uint64_t tile, uint64_t band, int32_t *tile_offsets,
+                                  float *centres) {
     if (bandnet_args(ctx, 1, columns, rows, labels) || !params || !costs || !guidance || !tile_offsets || tile < 1 ||
-        band < 1 || band > 32 || labels < band + 1)
+        band < 1 || band > 32 || labels < band + 1 || (cost_stride != labels && cost_stride != PREPASS_SLOTS))
         return CHIARO_ERR_ARGUMENT;
     try {
         CK(cudaSetDevice(ctx->device));
         NetState s = net_state(ctx, 1, (int)rows, (int)columns);
-        net_features(ctx, s, costs, guidance, (int)labels);
+        net_features(ctx, s, costs, guidance, (int)labels, (int)cost_stride);
         net_forward(ctx, s, params);
         const size_t tiles = ((columns + tile - 1) / tile) * ((rows + tile - 1) / tile);
         net_tile_offsets_kernel<<<(unsigned)div_ceil(tiles, 128), 128, 0, ctx->stream>>>(
@@ -2247,16 +2594,17 @@ int chiaro_bandnet_propose_device(chiaro_depth_ctx *ctx, const float *params, co
 
 int chiaro_bandnet_gradient_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
                                    const float *guidance, const int32_t *winners, const uint8_t *mask,
-                                   uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels, float *grads,
-                                   float *loss) {
+                                   uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels,
+                                   uint64_t cost_stride, float *grads, float *loss) {
     if (bandnet_args(ctx, images, columns, rows, labels) || !params || !costs || !guidance || !winners || !mask ||
-        !grads || !loss)
+        !grads || !loss || (cost_stride != labels && cost_stride != PREPASS_SLOTS))
         return CHIARO_ERR_ARGUMENT;
     try {
         CK(cudaSetDevice(ctx->device));
         NetState s = net_state(ctx, (int)images, (int)rows, (int)columns);
         float *targets = nullptr;
-        const float inverse = bandnet_batch(ctx, s, costs, guidance, winners, mask, (int)labels, &targets);
+        const float inverse =
+            bandnet_batch(ctx, s, costs, guidance, winners, mask, (int)labels, (int)cost_stride, &targets);
         float *d_loss = dbuf<float>(ctx, "net.loss", 1);
         CK(cudaMemsetAsync(d_loss, 0, sizeof(float), ctx->stream));
         net_backward(ctx, s, params, targets, mask, inverse, grads, d_loss);
@@ -2271,15 +2619,18 @@ int chiaro_bandnet_gradient_device(chiaro_depth_ctx *ctx, const float *params, c
 int chiaro_bandnet_train_device(chiaro_depth_ctx *ctx, float *params, float *adam_m, float *adam_v,
                                 uint64_t first_step, uint64_t steps, const float *costs, const float *guidance,
                                 const int32_t *winners, const uint8_t *mask, uint64_t images, uint64_t columns,
-                                uint64_t rows, uint64_t labels, float learning_rate, float *losses) {
+                                uint64_t rows, uint64_t labels, uint64_t cost_stride, float learning_rate,
+                                float *losses) {
     if (bandnet_args(ctx, images, columns, rows, labels) || !params || !adam_m || !adam_v || !costs || !guidance ||
-        !winners || !mask || !(learning_rate > 0.0f) || steps > 100000)
+        !winners || !mask || !(learning_rate > 0.0f) || steps > 100000 ||
+        (cost_stride != labels && cost_stride != PREPASS_SLOTS))
         return CHIARO_ERR_ARGUMENT;
     try {
         CK(cudaSetDevice(ctx->device));
         NetState s = net_state(ctx, (int)images, (int)rows, (int)columns);
         float *targets = nullptr;
-        const float inverse = bandnet_batch(ctx, s, costs, guidance, winners, mask, (int)labels, &targets);
+        const float inverse =
+            bandnet_batch(ctx, s, costs, guidance, winners, mask, (int)labels, (int)cost_stride, &targets);
         float *grads = dbuf<float>(ctx, "net.grads", NET_PARAMS);
         float *d_losses = dbuf<float>(ctx, "net.losses", std::max<uint64_t>(steps, 1));
         CK(cudaMemsetAsync(d_losses, 0, sizeof(float) * std::max<uint64_t>(steps, 1), ctx->stream));

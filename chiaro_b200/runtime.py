@@ -72,15 +72,20 @@ SIGNATURES = {
                                            C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p]),
     "chiaro_bandnet_parameter_count": (C.c_uint64, []),
     "chiaro_bandnet_propose_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
-                                                C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
-                                                C.c_void_p]),
+                                                C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                                                C.c_void_p, C.c_void_p]),
     "chiaro_bandnet_train_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
                                               C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                              C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_float,
-                                              P(C.c_float)]),
+                                              C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                                              C.c_float, P(C.c_float)]),
     "chiaro_bandnet_gradient_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                  C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
-                                                 C.c_void_p, P(C.c_float)]),
+                                                 C.c_uint64, C.c_void_p, P(C.c_float)]),
+    "chiaro_coarse_depth_device": (C.c_int, [C.c_void_p, P(ViewC), C.c_size_t, C.c_size_t, P(DepthOptionsC),
+                                             P(abi.BandOptionsC), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             P(abi.BandReportC)]),
+    "chiaro_band_prepass_device": (C.c_int, [C.c_void_p, P(ViewC), C.c_size_t, C.c_size_t, P(DepthOptionsC),
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
     "chiaro_host_alloc": (C.c_int, [C.c_uint64, P(C.c_void_p)]),
     "chiaro_host_free": (None, [C.c_void_p]),
     "chiaro_luminance_half": (C.c_int, [C.c_void_p, P(C.c_uint16), C.c_uint64, C.c_uint64, C.c_float, C.c_float,

@@ -310,6 +310,126 @@ def render_module(camera: ResolvedCamera, surfaces: List[Surface], tiles: List[n
     return raw, depth
 
 
+# ---- GPU rendering (benchmark workloads) ------------------------------------------
+# The same scene model ray cast with torch on a CUDA device, for workloads of many
+# full-resolution modules (the batched captures, the band network's training and
+# evaluation sets), where the numpy renderer would take minutes. Rays, hits and
+# texture follow the numpy path; the noise comes from torch's generator, so an image
+# differs from the numpy renderer's for the same seed (neither is a reference output).
+def _torch_normalize(v):
+    import torch
+    n = torch.sqrt((v * v).sum(-1, keepdim=True))
+    return torch.where(n == 0, v, v / n)
+
+
+def _torch_rays(camera: ResolvedCamera, pix):
+    """pixel_to_ray (geometry.rs:139-166) on a [n, 2] float64 tensor: (origin [3], directions [n, 3])."""
+    import torch
+    dev = pix.device
+    t64 = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev)
+    ideal = pix
+    d = camera.distortion
+    if d is not None:
+        centre, norm = t64(d.center), t64(d.normalization)
+        k1, k2, p1, p2, k3 = (d.coeff(i) for i in range(5))
+        observed = (pix - centre) / norm
+        est = observed.clone()
+        for _ in range(20):
+            x, y = est[:, 0], est[:, 1]
+            r2 = x * x + y * y
+            radial = 1.0 + k1 * r2 + k2 * r2 * r2 + k3 * r2 * r2 * r2
+            dx = x * radial + 2.0 * p1 * x * y + p2 * (r2 + 2.0 * x * x)
+            dy = y * radial + p1 * (r2 + 2.0 * y * y) + 2.0 * p2 * x * y
+            est = est + (observed - torch.stack([dx, dy], -1))
+        ideal = est * norm + centre
+    ones = torch.ones(len(pix), dtype=torch.float64, device=dev)
+    direction = _torch_normalize(torch.stack([ideal[:, 0], ideal[:, 1], ones], -1) @ t64(camera.k_inverse).T)
+    if camera.flip is not None:
+        sign = t64([1.0, -1.0, 1.0] if camera.flip else [-1.0, 1.0, 1.0])
+        direction = _torch_normalize(direction * sign)
+    if camera.pose_kind == 0:
+        world = direction @ t64(camera.rotation_cw).T
+    else:
+        world = direction @ (t64(camera.reflect) @ t64(camera.real_cw)).T
+    world = _torch_normalize(_torch_normalize(world) @ t64(camera.orientation_correction).T)
+    return t64(camera.center()), world
+
+
+def _torch_cast(surfaces: List[Surface], tiles, origin, direction):
+    """_cast on tensors: (intensity in [0, 1], distance) of the nearest hit along each ray."""
+    import torch
+    dev = direction.device
+    n = direction.shape[0]
+    best_t = torch.full((n,), float("inf"), dtype=torch.float64, device=dev)
+    value = torch.zeros(n, dtype=torch.float64, device=dev)
+    t64 = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=dev)
+    for s in surfaces:
+        if s.kind == "plane":
+            normal = t64(s.normal)
+            denom = direction @ normal
+            t = float(np.dot(s.origin - origin.cpu().numpy(), s.normal)) / denom
+            o_rel = origin - t64(s.origin)
+            uu = float(o_rel @ t64(s.axis_u)) + t * (direction @ t64(s.axis_u))
+            vv = float(o_rel @ t64(s.axis_v)) + t * (direction @ t64(s.axis_v))
+            hit = torch.isfinite(t) & (t > 1.0) & (t < best_t) & (uu.abs() <= s.half_u) & (vv.abs() <= s.half_v)
+        else:
+            oc = origin - t64(s.origin)
+            b = direction @ oc
+            c = float(oc @ oc) - s.radius * s.radius
+            disc = b * b - c
+            t = -b - torch.sqrt(torch.clamp(disc, min=0.0))
+            hit = (disc > 0) & (t > 1.0) & (t < best_t)
+            rel = _torch_normalize(oc + direction * t[:, None])
+            uu = torch.atan2(rel[:, 0], -rel[:, 2]) * s.radius
+            vv = torch.asin(torch.clamp(rel[:, 1], -1, 1)) * s.radius
+        tile = tiles[s.tex_index]
+        size = tile.shape[0]
+        u = uu / s.texel_mm + s.tex_offset[0]
+        v = vv / s.texel_mm + s.tex_offset[1]
+        u0, v0 = torch.floor(u), torch.floor(v)
+        fu, fv = u - u0, v - v0
+        iu = torch.remainder(torch.nan_to_num(u0, 0.0).long(), size)
+        iv = torch.remainder(torch.nan_to_num(v0, 0.0).long(), size)
+        iu1, iv1 = (iu + 1) % size, (iv + 1) % size
+        top = tile[iv, iu] * (1 - fu) + tile[iv, iu1] * fu
+        bottom = tile[iv1, iu] * (1 - fu) + tile[iv1, iu1] * fu
+        value = torch.where(hit, top * (1 - fv) + bottom * fv, value)
+        best_t = torch.where(hit, t, best_t)
+    return value, best_t
+
+
+def render_module_gpu(camera: ResolvedCamera, surfaces: List[Surface], tiles, seed: int, device,
+                      chunk_rows: int = 512):
+    """Ray cast one module on the GPU: its u16 raster [h, w] as an int32 device tensor."""
+    import torch
+    h, w = camera.height, camera.width
+    raw = torch.empty((h, w), dtype=torch.int32, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed) & 0x7FFFFFFFFFFFFFFF)
+    xs = torch.arange(w, dtype=torch.float64, device=device)
+    for y0 in range(0, h, chunk_rows):
+        y1 = min(h, y0 + chunk_rows)
+        yy = torch.arange(y0, y1, dtype=torch.float64, device=device)
+        pix = torch.stack(torch.meshgrid(yy, xs, indexing="ij")[::-1], -1).reshape(-1, 2)
+        origin, direction = _torch_rays(camera, pix)
+        value, _ = _torch_cast(surfaces, tiles, origin, direction)
+        signal = 4095.0 * (0.04 + 0.92 * value)
+        electrons = torch.poisson(signal / 0.5, generator=gen)
+        noisy = 0.5 * electrons + torch.randn(signal.shape, generator=gen, device=device, dtype=torch.float64) * 4.0
+        raw[y0:y1] = torch.clamp(torch.round(noisy), 0, 4095).to(torch.int32).reshape(y1 - y0, w)
+    return raw
+
+
+def luminance_half_gpu(raw, black: float = 0.0, white: float = 4095.0) -> Plane:
+    """luminance_half on a device raster (f32 on the GPU; the log is torch's)."""
+    import torch
+    h, w = raw.shape[0] // 2, raw.shape[1] // 2
+    r = raw[: 2 * h, : 2 * w].to(torch.float32)
+    s = ((r[0::2, 0::2] + r[0::2, 1::2]) + r[1::2, 0::2]) + r[1::2, 1::2]
+    linear = torch.clamp((s * 0.25 - black) / max(white - black, 1.0), min=0.0)
+    return Plane(w, h, torch.log(1.0 + 1000.0 * linear).cpu().numpy())
+
+
 def luminance_half(raw: np.ndarray, black: float = 0.0, white: float = 4095.0) -> Plane:
     """image.rs:401-428 with flat field 1 (f32 arithmetic, host numpy log)."""
     h, w = raw.shape[0] // 2, raw.shape[1] // 2
@@ -326,18 +446,24 @@ def make_scene(name: str, width: int, height: int, n_sources: int, n_planes: int
                max_rotation_deg: float, options: DepthOptions, seed: int,
                distortion: bool = False, horizontal_only: bool = False, texel_px: float = 3.0,
                mirrors: Optional[Dict[int, bool]] = None,
-               orientation: Optional[Dict[int, Tuple[float, float, float]]] = None) -> Scene:
+               orientation: Optional[Dict[int, Tuple[float, float, float]]] = None,
+               render_device=None, focal_px: Optional[float] = None) -> Scene:
     """``mirrors`` maps module indices (0 = the reference) to the flip_img_around_x value
     of a module behind a fold mirror (Pose::Mirror); ``orientation`` maps module indices
     to an axis-angle orientation offset in degrees. Both leave the random draws of the
     canonical scene unchanged (their own draws come from a separate generator), so a
-    mirrored scene sees the same surfaces from the same virtual positions."""
+    mirrored scene sees the same surfaces from the same virtual positions.
+    ``render_device``: a CUDA device to ray cast on (render_module_gpu) instead of numpy.
+    ``focal_px``: the modules' focal length in pixels (default: the 3 mm lens scaled to
+    the raster width, the same field of view at every size)."""
     rng = np.random.default_rng(seed)
     mirror_rng = np.random.default_rng((seed, 271828))
     mirrors = mirrors or {}
     orientation = orientation or {}
     tiles = [_noise_tile(np.random.default_rng(seed * 7919 + i)) for i in range(4)]
     ref_k = _intrinsics(width, height)
+    if focal_px is not None:
+        ref_k[0, 0] = ref_k[1, 1] = focal_px
     ref_dist = None
     if distortion:
         ref_dist = PolynomialDistortion(((width - 1) / 2.0, (height - 1) / 2.0), (width * 0.8, width * 0.8),
@@ -354,6 +480,10 @@ def make_scene(name: str, width: int, height: int, n_sources: int, n_planes: int
         centre = direction * b
         rot = _random_rotation(rng, max_rotation_deg)
         k = _intrinsics(width, height, rng, 0.01) if distortion else ref_k
+        if focal_px is not None and distortion:
+            k = k.copy()
+            k[0, 0] *= focal_px / _intrinsics(width, height)[0, 0]
+            k[1, 1] *= focal_px / _intrinsics(width, height)[0, 0]
         dist = None
         if distortion:
             dist = PolynomialDistortion(((width - 1) / 2.0 + rng.uniform(-5, 5), (height - 1) / 2.0 + rng.uniform(-5, 5)),
@@ -382,7 +512,16 @@ def make_scene(name: str, width: int, height: int, n_sources: int, n_planes: int
     for i in range(n_spheres):
         surfaces.append(_random_sphere(rng, ref, (max(near, 1000.0), min(far, 8000.0)), texel_px, (i + 2) % 4))
     raws, lumas, truth = [], [], None
+    gpu_tiles = None
+    if render_device is not None:
+        import torch
+        gpu_tiles = [torch.as_tensor(t, device=render_device) for t in tiles]
     for i, cam in enumerate(cams):
+        if gpu_tiles is not None:  # the raster stays on the device; Scene.raw is left empty
+            raw = render_module_gpu(cam, surfaces, gpu_tiles, seed * 104729 + i, render_device)
+            lumas.append(luminance_half_gpu(raw))
+            del raw
+            continue
         raw, depth = render_module(cam, surfaces, tiles, seed * 104729 + i)
         raws.append(raw)
         lumas.append(luminance_half(raw))
@@ -412,6 +551,35 @@ WORKLOADS: Dict[str, dict] = {
                  baseline_range=(20.0, 40.0), max_rotation_deg=0.3, distortion=False,
                  options=dict(planes=16, near_depth=400.0, far_depth=20000.0)),
 }
+
+# One synthetic 16-module capture as the depth stage sees it: 10 reference/source
+# groupings of 5 wide modules (canonical poses), 5 mid and 6 tele modules (behind fold
+# mirrors, alternating flip_img_around_x). Every module is resampled to the wide
+# modules' angular pixel size (a common bandwidth: the 3 mm lens at 1.12 um), so a
+# grouping's raster is its field of view at that size: 4160x3120 for the wide modules
+# down to 1040x780 for the tele ones. (width, height, planes, kind, sources)
+CAPTURE_GROUPINGS = [(4160, 3120, 128, "wide", 4), (4160, 3120, 192, "wide", 4), (3120, 2340, 64, "mid", 3),
+                     (3120, 2340, 128, "mid", 4), (2080, 1560, 192, "mid", 3), (2080, 1560, 64, "tele", 2),
+                     (2080, 1560, 128, "tele", 3), (1560, 1170, 192, "tele", 3), (1040, 780, 64, "tele", 2),
+                     (1040, 780, 128, "tele", 3)]
+
+
+def make_capture(seed: int, render_device=None, planes=None, surfaces: Tuple[int, int] = (12, 3),
+                 groupings=CAPTURE_GROUPINGS) -> List[Scene]:
+    """The groupings of one seeded capture, each a Scene of its raster size, plane count and
+    module kind (mid and tele modules behind mirrors). ``planes`` (optional) replaces each
+    grouping's plane count, e.g. drawn per capture; ``surfaces`` = (slanted planes, spheres)."""
+    out = []
+    for g, (width, height, default_planes, kind, sources) in enumerate(groupings):
+        flip = (seed + g) % 2 == 0
+        mirrors = {} if kind == "wide" else {i: (flip if i % 2 == 0 else not flip) for i in range(sources + 1)}
+        opt = DepthOptions(planes=(planes[g] if planes is not None else default_planes), near_depth=400.0,
+                           far_depth=50000.0)
+        out.append(make_scene(f"capture{seed}.{g}.{kind}", width, height, sources, surfaces[0], surfaces[1],
+                              (500.0, 20000.0), (20.0, 60.0), 0.5, opt, seed * 1000 + g, distortion=True,
+                              mirrors=mirrors, render_device=render_device, focal_px=FOCAL_MM / PIXEL_PITCH_MM))
+    return out
+
 
 _CACHE: Dict[tuple, Scene] = {}
 

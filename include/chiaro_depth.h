@@ -434,14 +434,15 @@ int chiaro_sgm_banded_report(const chiaro_depth_ctx *ctx, int *windows);
 /* No counterpart in the reference (which uses no learned model): the band
  * proposal network of the banded SGM. Six 3x3 convolutions of 32 channels on
  * the coarse grid (one pixel per node), bf16 tensor-core kernels with fp32
- * accumulation. Inputs per node: the reference luminance (guidance), 16
- * cost-bin minima over the finite labels (labels >= 19), the first cost argmin
- * and the minimum cost. Parameters are
+ * accumulation. Inputs per node: the reference luminance (guidance), the costs
+ * of 16 sampled labels spread over the finite ones (labels >= 19), the first
+ * sampled label at their minimum and that minimum cost. Parameters are
  * chiaro_bandnet_parameter_count() fp32 values: per layer the weights
  * [tap][co][ci] then the 32 biases. All arrays below are device memory; costs
- * [images][nodes][labels], guidance [images][nodes], winners (the target
- * labels, e.g. the full-range SGM's) and mask (1 for nodes to learn from)
- * [images][nodes]. */
+ * [images][nodes][cost_stride]: full rows (cost_stride = labels) or the
+ * pre-pass's rows (cost_stride = 17, chiaro_band_prepass_device); guidance
+ * [images][nodes], winners (the target labels, e.g. the full-range SGM's) and
+ * mask (1 for nodes to learn from) [images][nodes]. */
 uint64_t chiaro_bandnet_parameter_count(void);
 
 /* Band offsets per tile (as chiaro_sgm_banded takes them): the band centred on
@@ -449,7 +450,7 @@ uint64_t chiaro_bandnet_parameter_count(void);
  * centres (optional, [nodes]) receives each node's normalised prediction. */
 int chiaro_bandnet_propose_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
                                   const float *guidance, uint64_t columns, uint64_t rows,
-                                  uint64_t labels, uint64_t tile, uint64_t band,
+                                  uint64_t labels, uint64_t cost_stride, uint64_t tile, uint64_t band,
                                   int32_t *tile_offsets, float *centres);
 
 /* `steps` full-batch Adam steps (numbered from first_step + 1) of the Huber loss
@@ -460,14 +461,78 @@ int chiaro_bandnet_train_device(chiaro_depth_ctx *ctx, float *params, float *ada
                                 uint64_t first_step, uint64_t steps, const float *costs,
                                 const float *guidance, const int32_t *winners, const uint8_t *mask,
                                 uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels,
-                                float learning_rate, float *losses);
+                                uint64_t cost_stride, float learning_rate, float *losses);
 
 /* One forward and backward pass: the loss (host) and its gradient (device,
  * the parameters' layout). */
 int chiaro_bandnet_gradient_device(chiaro_depth_ctx *ctx, const float *params, const float *costs,
                                    const float *guidance, const int32_t *winners, const uint8_t *mask,
                                    uint64_t images, uint64_t columns, uint64_t rows, uint64_t labels,
-                                   float *grads, float *loss);
+                                   uint64_t cost_stride, float *grads, float *loss);
+
+/* ---- coarse depth search ------------------------------------------------------- */
+
+/* The learned-band form of the coarse search (no counterpart in the reference, which
+ * searches every label). params: the band network's parameters in device memory
+ * (chiaro_bandnet_parameter_count() floats), or NULL for the band without learning
+ * (per tile, the median of its nodes' lowest sampled labels). A tile is tile x tile
+ * coarse nodes (1..8); band finite labels per tile (1..32, at most planes); margin nodes
+ * of full-range context around each fallback rectangle; a tile also falls back when
+ * more than contradicted_fraction of its tested nodes fail the cross-view check (1 or
+ * more: never). */
+typedef struct chiaro_band_options {
+    const float *params;
+    uint64_t tile;
+    uint64_t band;
+    uint64_t margin;
+    float contradicted_fraction;
+    int32_t _pad0;
+} chiaro_band_options;
+
+/* What a coarse search did. Tiles whose winner sat on a band edge (edge_tiles), that
+ * failed the cross-view check (consistency_tiles), either (fallback_tiles); the fallback
+ * windows and the nodes whose full-range costs they computed; device milliseconds of
+ * [0] the shared set-up (geometry, tap lattice, quad planes), [1] the pre-pass, [2] the
+ * band proposal, [3] the cost volume (banded or full), [4] the SGM and winners (with the
+ * fallback flags), [5] the fallback (host round trip included), [6] the whole search. */
+typedef struct chiaro_band_report {
+    uint64_t tiles;
+    uint64_t edge_tiles;
+    uint64_t consistency_tiles;
+    uint64_t fallback_tiles;
+    uint64_t windows;
+    uint64_t window_nodes;
+    float ms[7];
+    int32_t _pad0;
+} chiaro_band_report;
+
+/* The coarse depth search of refine_multiview_depth on the reference's coarse grid
+ * (depth.rs:326-328): build_cost_volume (depth.rs:1187-1277), semi_global_costs
+ * (depth.rs:1279-1383) and each node's winning label over the finite labels, the first
+ * minimum as select_depths takes it (depth.rs:1406-1413). views as for
+ * chiaro_refine_multiview_depth_device (device memory). winner [N] (device) receives
+ * each coarse node's label; tested [N] (device, optional) the cost volume's tested flags.
+ * band == NULL: the plain search, bit-identical to the stage's. Otherwise the learned-band
+ * search (no counterpart in the reference): a pre-pass scores label 0 and 16 sampled
+ * labels at every node, the band proposal picks each tile's band, the cost volume scores
+ * label 0 and the band, the banded SGM picks winners, and tiles whose winner sits on a
+ * band edge or that fail the cross-view check (a node's aggregated score at its winner
+ * more than 0.12 below its score under the global warp, the threshold of depth.rs:
+ * 458-485) are searched again at full range in windows around them. tile_offsets and
+ * tile_fallback ([tiles], device, optional) receive each tile's band start and fallback
+ * flag; report (host, optional) what the search did. */
+int chiaro_coarse_depth_device(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views,
+                               size_t reference_index, const chiaro_depth_options *options,
+                               const chiaro_band_options *band, int32_t *winner, uint8_t *tested,
+                               int32_t *tile_offsets, uint8_t *tile_fallback, chiaro_band_report *report);
+
+/* The learned-band search's pre-pass alone (no counterpart in the reference): per coarse
+ * node, the costs of label 0 and of the 16 sampled labels ([N][17], device), the
+ * guidance and the tested flag ([N], device, optional): the band network's inputs, for
+ * training it. The sampled labels are 1 + (b (planes - 1) + 7) / 15, b = 0..15. */
+int chiaro_band_prepass_device(chiaro_depth_ctx *ctx, const chiaro_view *views, size_t n_views,
+                               size_t reference_index, const chiaro_depth_options *options, float *sampled_costs,
+                               float *guidance, uint8_t *tested);
 
 /* ---- input plane --------------------------------------------------------- */
 

@@ -2348,26 +2348,38 @@ int oracle_sgm_banded(const float *costs, const float *guidance, size_t columns,
 // 32 biases.
 static const int NET_CH_O = 32, NET_LAYERS_O = 6, NET_W_O = 9 * 32 * 32;
 
-void oracle_bandnet_features(const float *costs, const float *guidance, size_t nodes, size_t labels, float *features) {
-    const int bins = 16, finite = (int)labels - 1;
+// The band proposal's sampled labels: 16 finite labels spread evenly over 1..labels-1
+// (the first and the last included), label(b) = 1 + (b (labels - 2) + 7) / 15.
+static int net_sample_label(int b, int labels) { return 1 + (b * (labels - 2) + 7) / 15; }
+
+void oracle_net_sample_labels(size_t labels, int *out) {
+    for (int b = 0; b < 16; ++b) out[b] = net_sample_label(b, (int)labels);
+}
+
+// Features of the band network per node: the reference luminance at the node
+// (guidance / 8); the costs of the 16 sampled labels minus the lowest of them; the
+// first of the sampled labels holding that lowest cost, as (label - 1) / (labels - 2);
+// and the lowest cost. costs rows hold `stride` values: the full volume (stride =
+// labels, a label's cost at its index) or the pre-pass's rows (stride = 17, label 0
+// then the sampled labels in order).
+void oracle_bandnet_features(const float *costs, const float *guidance, size_t nodes, size_t labels, size_t stride,
+                             float *features) {
+    const int bins = 16;
     for (size_t node = 0; node < nodes; ++node) {
-        const float *c = costs + node * labels;
-        float m[16], lowest = std::numeric_limits<float>::infinity();
+        const float *c = costs + node * stride;
+        float v[16], lowest = std::numeric_limits<float>::infinity();
         int argmin = 1;
         for (int b = 0; b < bins; ++b) {
-            int l0 = 1 + b * finite / bins, l1 = 1 + (b + 1) * finite / bins;
-            m[b] = std::numeric_limits<float>::infinity();
-            for (int l = l0; l < l1; ++l) {
-                if (c[l] < lowest) {
-                    lowest = c[l];
-                    argmin = l;
-                }
-                m[b] = std::fmin(m[b], c[l]);
+            const int label = net_sample_label(b, (int)labels);
+            v[b] = c[stride == labels ? label : 1 + b];
+            if (v[b] < lowest) {
+                lowest = v[b];
+                argmin = label;
             }
         }
         float *f = features + node * NET_CH_O;
         f[0] = guidance[node] * 0.125f;
-        for (int b = 0; b < bins; ++b) f[1 + b] = m[b] - lowest;
+        for (int b = 0; b < bins; ++b) f[1 + b] = v[b] - lowest;
         f[1 + bins] = (float)(argmin - 1) / (float)(labels - 2);
         f[2 + bins] = lowest;
         for (int k = 3 + bins; k < NET_CH_O; ++k) f[k] = 0.0f;
@@ -2391,9 +2403,33 @@ static void net_conv_o(const float *in, int images, int h, int w, const float *w
                 }
 }
 
-// Loss and gradient of the network on a batch; y (optional) receives channel 0.
+// Round to the nearest bf16 (ties to even), as __float2bfloat16_rn does.
+static float bf16_round(float v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return v;  // inf and NaN stay
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+// Loss and gradient of the network on a batch; y (optional) receives channel 0. With
+// bf16_storage, every stored activation and pre-activation gradient is rounded to bf16,
+// as the GPU stores them (the last layer's channel 0, y, stays fp32 there too).
+void oracle_bandnet_loss_grad_mode(const float *params, const float *features, const float *targets,
+                                   const uint8_t *mask, size_t images, size_t height, size_t width, float *grads,
+                                   float *loss, float *y, int bf16_storage);
+
 void oracle_bandnet_loss_grad(const float *params, const float *features, const float *targets, const uint8_t *mask,
                               size_t images, size_t height, size_t width, float *grads, float *loss, float *y) {
+    oracle_bandnet_loss_grad_mode(params, features, targets, mask, images, height, width, grads, loss, y, 0);
+}
+
+void oracle_bandnet_loss_grad_mode(const float *params, const float *features, const float *targets,
+                                   const uint8_t *mask, size_t images, size_t height, size_t width, float *grads,
+                                   float *loss, float *y, int bf16_storage) {
     const int h = (int)height, w = (int)width, nimg = (int)images;
     const size_t pixels = images * height * width, act_n = pixels * NET_CH_O;
     std::vector<std::vector<float>> act(NET_LAYERS_O + 1, std::vector<float>(act_n));
@@ -2403,6 +2439,8 @@ void oracle_bandnet_loss_grad(const float *params, const float *features, const 
         net_conv_o(act[l].data(), nimg, h, w, p, p + NET_W_O, act[l + 1].data());
         if (l + 1 < NET_LAYERS_O)
             for (float &v : act[l + 1]) v = std::fmax(v, 0.0f);
+        if (bf16_storage && l + 1 < NET_LAYERS_O)
+            for (float &v : act[l + 1]) v = bf16_round(v);
     }
     size_t count = 0;
     for (size_t i = 0; i < pixels; ++i) count += mask[i] != 0;
@@ -2417,6 +2455,7 @@ void oracle_bandnet_loss_grad(const float *params, const float *features, const 
         float e = yi - targets[i], a = std::fabs(e);
         total += a <= delta ? 0.5 * e * e : delta * (a - 0.5 * delta);
         dpre[i * NET_CH_O] = (float)((a <= delta ? e : std::copysign(delta, e)) * inverse);
+        if (bf16_storage) dpre[i * NET_CH_O] = bf16_round(dpre[i * NET_CH_O]);
     }
     *loss = (float)(total * inverse);
     std::fill(grads, grads + (size_t)NET_LAYERS_O * (NET_W_O + NET_CH_O), 0.0f);
@@ -2461,6 +2500,8 @@ void oracle_bandnet_loss_grad(const float *params, const float *features, const 
                     }
                 }
         for (size_t i = 0; i < act_n; ++i) dpre[i] = act[l][i] > 0.0f ? dnext[i] : 0.0f;
+        if (bf16_storage)
+            for (float &v : dpre) v = bf16_round(v);
     }
 }
 

@@ -113,7 +113,12 @@ def lib():
             "oracle_sgm_banded": (C.c_int, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, C.c_size_t,
                                              P(C.c_int), C.c_size_t, C.c_size_t, C.c_size_t, P(C.c_int),
                                              P(C.c_uint8)]),
-            "oracle_bandnet_features": (None, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, P(C.c_float)]),
+            "oracle_bandnet_features": (None, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, C.c_size_t,
+                                               P(C.c_float)]),
+            "oracle_net_sample_labels": (None, [C.c_size_t, P(C.c_int)]),
+            "oracle_bandnet_loss_grad_mode": (None, [P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_uint8),
+                                                     C.c_size_t, C.c_size_t, C.c_size_t, P(C.c_float), P(C.c_float),
+                                                     P(C.c_float), C.c_int]),
             "oracle_bandnet_loss_grad": (None, [P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_uint8), C.c_size_t,
                                                 C.c_size_t, C.c_size_t, P(C.c_float), P(C.c_float), P(C.c_float)]),
             "oracle_sgm_u16": (None, [P(C.c_float), P(C.c_float), C.c_size_t, C.c_size_t, C.c_size_t,

@@ -38,7 +38,8 @@ def test_struct_layouts_match_the_header(tmp_path):
     structs = {"chiaro_depth_options": abi.DepthOptionsC, "chiaro_camera": abi.CameraC, "chiaro_warp": abi.WarpC,
                "chiaro_view": abi.ViewC, "chiaro_depth_map": abi.DepthMapC, "chiaro_depth_report": abi.DepthReportC,
                "chiaro_depth_debug": abi.DepthDebugC, "chiaro_vignetting": abi.VignettingC,
-               "chiaro_sgm_instance": abi.SgmInstanceC, "chiaro_resolution_report": abi.ResolutionReportC,
+               "chiaro_sgm_instance": abi.SgmInstanceC, "chiaro_band_options": abi.BandOptionsC,
+               "chiaro_band_report": abi.BandReportC, "chiaro_resolution_report": abi.ResolutionReportC,
                "chiaro_align_input": abi.AlignInputC, "chiaro_align_options": abi.AlignOptionsC,
                "chiaro_align_level": abi.AlignLevelC, "chiaro_alignment_report": abi.AlignmentReportC}
     lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]

@@ -45,18 +45,27 @@ def test_oracle_gradient_matches_finite_differences(oracle_lib):
 
 
 def test_oracle_features_of_a_node(oracle_lib):
-    labels = 49  # 48 finite labels: 16 bins of 3
+    """The 16 sampled labels spread over 1..D-1 (first and last included); the features
+    read them from a full row or from the pre-pass's compact row, with the same result."""
+    labels = 49
+    sampled = np.zeros(16, np.int32)
+    oracle_lib.oracle_net_sample_labels(labels, sampled.ctypes.data_as(C.POINTER(C.c_int)))
+    assert sampled[0] == 1 and sampled[-1] == labels - 1 and np.all(np.diff(sampled) > 0)
+    assert list(sampled) == [1 + (b * (labels - 2) + 7) // 15 for b in range(16)]
     costs = np.full(labels, 1.5, np.float32)
     costs[0] = 0.0  # label 0 is not a depth label and stays out of the summary
-    costs[[7, 20, 30]] = [0.4, 0.2, 0.2]
+    costs[sampled[[2, 6, 9]]] = [0.4, 0.2, 0.2]
+    costs[sampled[4] + 1] = 0.05  # not a sampled label: invisible to the features
     guidance = np.array([4.0], np.float32)
-    f = np.zeros(32, np.float32)
-    oracle_lib.oracle_bandnet_features(costs.ctypes.data_as(F), guidance.ctypes.data_as(F), 1, labels,
-                                       f.ctypes.data_as(F))
-    bins = np.full(16, 1.3, np.float32)
-    bins[2], bins[6], bins[9] = 0.2, 0.0, 0.0  # labels 7, 20 and 30 minus the minimum 0.2
-    assert f[0] == np.float32(0.5)
-    assert np.allclose(f[1:17], bins)
-    assert f[17] == np.float32(19 / 47)  # the first argmin (label 20), over labels 1..48
-    assert f[18] == np.float32(0.2)
-    assert not f[INPUTS:].any()
+    compact = np.concatenate([[costs[0]], costs[sampled]]).astype(np.float32)
+    expected = np.full(16, 1.3, np.float32)
+    expected[2], expected[6], expected[9] = 0.2, 0.0, 0.0  # minus the lowest sampled cost 0.2
+    for row, stride in ((costs, labels), (compact, 17)):
+        f = np.zeros(32, np.float32)
+        oracle_lib.oracle_bandnet_features(row.ctypes.data_as(F), guidance.ctypes.data_as(F), 1, labels, stride,
+                                           f.ctypes.data_as(F))
+        assert f[0] == np.float32(0.5)
+        assert np.allclose(f[1:17], expected)
+        assert f[17] == np.float32((sampled[6] - 1) / (labels - 2))  # the first sampled label at the minimum
+        assert f[18] == np.float32(0.2)
+        assert not f[INPUTS:].any()

@@ -46,7 +46,7 @@ def test_gpu_gradient_matches_fp32_oracle(gpu_ctx):
     n = 9 * 20
     features = np.zeros((2 * n, 32), np.float32)
     for i, s in enumerate(samples):
-        lib.oracle_bandnet_features(s.costs.ctypes.data_as(F), s.guidance.ctypes.data_as(F), n, s.labels,
+        lib.oracle_bandnet_features(s.costs.ctypes.data_as(F), s.guidance.ctypes.data_as(F), n, s.labels, s.labels,
                                     features[i * n:].ctypes.data_as(F))
     features = bf16_round(features)
     p = params.copy().reshape(6, -1)
@@ -56,13 +56,15 @@ def test_gpu_gradient_matches_fp32_oracle(gpu_ctx):
     mask = np.concatenate([s.mask for s in samples])
     grads = np.zeros_like(p)
     loss = C.c_float()
-    lib.oracle_bandnet_loss_grad(p.ctypes.data_as(F), features.ctypes.data_as(F), targets.ctypes.data_as(F),
-                                 mask.ctypes.data_as(C.POINTER(C.c_uint8)), 2, 9, 20, grads.ctypes.data_as(F),
-                                 C.byref(loss), None)
-    assert abs(loss_gpu - loss.value) <= 0.03 * loss.value
-    cos = float(np.dot(grads_gpu, grads) / (np.linalg.norm(grads_gpu) * np.linalg.norm(grads)))
+    # the oracle stores every activation and pre-activation gradient in bf16, as the GPU does;
+    # what remains is the accumulation order (fp32 tensor-core sums against f64 loops)
+    lib.oracle_bandnet_loss_grad_mode(p.ctypes.data_as(F), features.ctypes.data_as(F), targets.ctypes.data_as(F),
+                                      mask.ctypes.data_as(C.POINTER(C.c_uint8)), 2, 9, 20, grads.ctypes.data_as(F),
+                                      C.byref(loss), None, 1)
+    # stated tolerance: loss within 1e-3 relative, gradient within 1e-2 relative L2
+    assert abs(loss_gpu - loss.value) <= 1e-3 * loss.value, (loss_gpu, loss.value)
     rel = float(np.linalg.norm(grads_gpu - grads) / np.linalg.norm(grads))
-    assert cos > 0.98 and rel < 0.2, (cos, rel)
+    assert rel < 1e-2, rel
 
 
 def test_training_lowers_the_loss(gpu_ctx):
@@ -88,17 +90,19 @@ def test_proposals_are_valid_band_offsets(gpu_ctx):
 
 def test_trained_network_against_the_naive_band(gpu_ctx):
     """What training buys: the band network trained on the GPU (tile-median targets from
-    the exact stage's full-range SGM) against the naive band (each tile's median cost
-    argmin) on held-out 1040x780 scenes with 192 planes, the banded SGM with full-range
-    fallback scored against the full-range SGM over tested nodes."""
+    the exact plain search's winners, inputs from the pre-pass's 16 sampled labels)
+    against the naive band (each tile's median lowest sampled label) on held-out
+    1040x780 scenes with 192 planes: the learned-band coarse search scored against the
+    plain search over tested nodes."""
     from chiaro_b200 import bandnet
-    scenes = bandnet.render_scenes("band", list(range(300, 316)) + list(range(900, 906)))
-    samples = [bandnet.samples_from_stage(s, gpu_ctx) for s in scenes]
-    train, held = samples[:16], samples[16:]
+    from chiaro_b200.depth import DeviceStage
+    rendered = bandnet.render_scenes("band", list(range(300, 316)) + list(range(900, 906)))
+    stages = [DeviceStage(s.inputs(), 0, s.alignments(), s.options, context=gpu_ctx) for s in rendered]
+    samples = [bandnet.samples_from_prepass(st) for st in stages[:16]]
     net = BandNet(gpu_ctx, seed=0)
-    targets = [bandnet.tile_targets(s, 4, "median") for s in train]
+    targets = [bandnet.tile_targets(s, 4, "median") for s in samples]
     losses = np.concatenate([net.train(targets, 400, 2e-3), net.train(targets, 200, 5e-4)])
-    scores = bandnet.evaluate(gpu_ctx, held, {"learned": net}, 4, 24, 8)
+    scores = bandnet.evaluate_search(stages[16:], {"learned": net}, 4, 24, 8, 1.0)
     print(scores)
     assert losses[-1] < 0.2 * losses[0]
     learned, naive = scores["learned"], scores["naive"]
