@@ -61,10 +61,10 @@ def parse_args():
                    help="coarse rows per worker band in each CPU sample step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (0 = --steps)")
-    p.add_argument("--band-train", type=int, default=24, help="1040x780 scenes the band network trains on")
     p.add_argument("--band-eval", type=int, default=8, help="held-out 1040x780 scenes of the band evaluation")
-    p.add_argument("--band-train-full", type=int, default=2,
-                   help="full-resolution five-view scenes added to the third band network's training")
+    p.add_argument("--band-eval-full", type=int, default=2,
+                   help="held-out full-resolution five-view scenes of the band evaluation")
+    p.add_argument("--captures", type=int, default=32, help="captures of the config-4 stream")
     p.add_argument("--no-learned-band", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the per-config sub-objects (two_view, ...)")
     return p.parse_args()
@@ -155,6 +155,35 @@ def sgm_traffic():
         return None
     m = re.search(r"traffic_bytes_per_call = (\d+)", f.read_text())
     return int(m.group(1)) if m else None
+
+
+def correlation_instructions():
+    """Warp instructions per launch of the correlation kernels on five_view, from the
+    committed ncu capture (profiles/correlation_issue_five_view.md), or {}."""
+    import re
+    f = ROOT / "profiles" / "correlation_issue_five_view.md"
+    if not f.exists():
+        return {}
+    return {m.group(1): int(m.group(2)) for m in re.finditer(r"warp_instructions (\w+) = (\d+)", f.read_text())}
+
+
+def issue_roofline(stage_ms, sm_mhz):
+    """Instruction-issue fractions of the correlation stages: warp instructions per launch
+    (ncu) over the stage's event time at 148 SMs x 4 schedulers x one instruction per cycle."""
+    counts = correlation_instructions()
+    if not counts:
+        return None
+    peak = 148 * 4 * sm_mhz * 1e6
+    stages = {"cost_volume": ["cost_volume_kernel"], "direct": ["direct_depth_kernel", "direct_wide_kernel"],
+              "decisions": ["target_decision_kernel"]}
+    out = {"unit": "warp instructions / s", "peak": peak, "peak_source": f"148 SMs x 4 schedulers at {sm_mhz:.0f} MHz",
+           "instructions_source": "profiles/correlation_issue_five_view.md (ncu smsp__inst_executed.sum, one launch)"}
+    for stage, kernels in stages.items():
+        inst = sum(counts.get(k, 0) for k in kernels)
+        if inst and stage_ms.get(stage):
+            achieved = inst / (stage_ms[stage] / 1e3)
+            out[stage] = {"warp_instructions": inst, "achieved": round(achieved / 1e9, 1), "frac": round(achieved / peak, 4)}
+    return out
 
 
 def stage_bytes(scene):
@@ -284,7 +313,10 @@ def run_ours(args, rank, world, local):
     batched = batched_sgm(args, ctx, torch, device, stream, flush)
     band = None
     if world == 1 and not args.no_learned_band:
-        band = learned_band(args, scene, ctx, torch, device, stream, flush)
+        band = learned_band(args, ctx, torch, device)
+    if world == 1 and not args.no_configs:
+        configs["config2"] = config2_capture(args, ctx, torch, device)
+        configs["config4"] = config4_stream(args, ctx, torch, device)
 
     peaks = measured_peaks()
     sgm_s = stage_ms["sgm"] / 1e3
@@ -321,6 +353,7 @@ def run_ours(args, rank, world, local):
         "batched_sgm": dict(batched, note="SGM of many instances of uneven sizes and label counts: "
                             "per-instance calls (plain) against one persistent batch replayed from a CUDA graph"),
         **({"learned_band": band} if band else {}),
+        "issue_roofline": issue_roofline(stage_ms, sm_mhz) if args.workload == "five_view" else None,
         "compute_roofline": {"kernel": "cost_volume_kernel (build_cost_volume, the largest correlation kernel)",
                              "bound": "fp32", "achieved": round(cost_tflops, 2), "peak": round(fp32_peak, 1),
                              "unit": "TFLOP/s", "frac": round(cost_tflops / fp32_peak, 4),
@@ -722,120 +755,178 @@ def batched_sgm(args, ctx, torch, device, stream, flush):
     return result
 
 
-def learned_band(args, scene, ctx, torch, device, stream, flush):
-    """Config 3: the learned band proposal. Two networks (tile-median and tile-mid-range
-    targets) train on the GPU on seeded 1040x780 five-view scenes with 192 planes, labelled
-    by the exact GPU stage's full-range SGM; a third (tile-median) also sees a few
-    full-resolution five-view scenes of other seeds. On held-out scenes of that kind and on this
-    workload's own full-resolution scene at 192 planes, the banded SGM with full-range
-    fallback is scored against the
-    full-range SGM (agreement within one plane over tested nodes, fallback rate) beside the
-    naive band (each tile's median cost argmin), and timed against the full-range SGM."""
-    import numpy as np
+WEIGHTS = ROOT / "chiaro_b200" / "weights" / "bandnet.bin"
 
-    from chiaro_b200 import band as bandmod
-    from chiaro_b200 import bandnet
-    tile, width, margin = 4, 24, 8
-    t0 = time.perf_counter()
-    rendered = bandnet.render_scenes("band", list(range(1000, 1000 + args.band_train)) +
-                                     list(range(5000, 5000 + args.band_eval)))
-    render_s = time.perf_counter() - t0
-    samples = [bandnet.samples_from_stage(s, ctx) for s in rendered]
-    del rendered
-    train, held = samples[:args.band_train], samples[args.band_train:]
-    import dataclasses
-    full = bandnet.samples_from_stage(
-        dataclasses.replace(scene, options=dataclasses.replace(scene.options, planes=192)), ctx)
-    t0 = time.perf_counter()
-    full_train = [bandnet.samples_from_stage(s, ctx) for s in bandnet.render_scenes(
-        "five_view", range(7000, 7000 + args.band_train_full), options=dict(planes=192))]
-    render_s += time.perf_counter() - t0
-    nets, training = {}, {}
-    for kind, mixed in (("median", False), ("midrange", False), ("median", True)):
-        net = bandnet.BandNet(ctx, seed=args.seed)
-        targets = [bandnet.tile_targets(s, tile, kind) for s in train]
-        full_targets = [bandnet.tile_targets(s, tile, kind) for s in full_train] if mixed else []
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-        losses = []
-        for lr, rounds in ((2e-3, 10), (5e-4, 5)):  # 40 steps per round, a third of them full resolution
-            for _ in range(rounds):
-                if full_targets:
-                    losses.append(net.train(targets, 27, lr))
-                    losses.append(net.train(full_targets, 13, lr))
-                else:
-                    losses.append(net.train(targets, 40, lr))
-        with torch.cuda.stream(stream):
-            e1.record(stream)
-        e1.synchronize()
-        name = f"learned_{kind}" + ("_with_full_resolution" if mixed else "")
-        nets[name] = net
-        training[name] = {"steps": 600, "images": len(targets) + len(full_targets),
-                          "ms": round(e0.elapsed_time(e1), 1), "loss_first": float(losses[0][0]),
-                          "loss_last": float(losses[-1][-1])}
-    held_scores = bandnet.evaluate(ctx, held, nets, tile, width, margin)
-    full_scores = bandnet.evaluate(ctx, [full], nets, tile, width, margin)
 
-    # time on this workload's own cost volume: the full-range SGM against proposal + banded SGM + fallback
-    costs = torch.from_numpy(full.costs).to(device)
-    guidance = torch.from_numpy(full.guidance).to(device)
-    out = torch.empty_like(costs)
-    tx, ty = bandmod.tiles_of(full.columns, full.rows, tile)
-    winner = torch.empty(full.columns * full.rows, dtype=torch.int32, device=device)
-    fallback = torch.empty(tx * ty, dtype=torch.uint8, device=device)
-    lib = ctx.lib
+def band_network(ctx, device):
+    """The trained band network (chiaro_b200/weights/bandnet.bin, written by
+    chiaro_b200.train_band) and its metadata, or (None, None) without it."""
+    from chiaro_b200.bandnet import BandNet
+    if not WEIGHTS.exists():
+        return None, None
+    net = BandNet(ctx, device=device.index or 0)
+    meta = net.load(WEIGHTS)
+    return net, meta
 
-    def timed(fn):
+
+def learned_band(args, ctx, torch, device):
+    """Config 3: the learned-band coarse search (chiaro_coarse_depth_device with the band)
+    against the plain search on held-out scenes: the trained network (weights committed
+    with their training record) and the naive band, scored by agreement with the plain
+    search's winners within one plane over tested nodes, the fallback rate and the time of
+    the coarse search (device time, its CUDA events). Scenes: GPU-rendered held-out
+    1040x780 five-view-structure scenes and full-resolution five-view scenes, 192 planes."""
+    from chiaro_b200 import bandnet, scenes
+    from chiaro_b200.depth import DeviceStage
+    net, meta = band_network(ctx, device)
+    nets = {"learned": net} if net is not None else {}
+    out = {"weights": str(WEIGHTS.relative_to(ROOT)) if net is not None else None,
+           "training": (meta or {}).get("training"), "training_evaluation": (meta or {}).get("evaluation")}
+    for key, name, seeds in (("held_out_1040x780", "band", range(30000, 30000 + args.band_eval)),
+                             ("held_out_4160x3120", "five_view", range(31000, 31000 + args.band_eval_full))):
+        stages = (DeviceStage(sc.inputs(), 0, sc.alignments(), sc.options, context=ctx)
+                  for sc in (scenes.workload(name, seed=s, cache=False, render_device=device,
+                                             options=dict(planes=192)) for s in seeds))
+        out[key] = dict(bandnet.evaluate_search(stages, nets, 4, 24, 8, 0.5), scenes=len(seeds))
+    out["note"] = ("agreement over the plain search's tested nodes; speedup = plain coarse-search time over "
+                   "the banded search's (pre-pass, proposal, banded cost volume and SGM, fallback windows)")
+    return out
+
+
+def capture_stages(seed, ctx_for, device, planes=None, surfaces=(12, 3)):
+    """DeviceStages of one GPU-rendered 16-module capture's 10 groupings (ctx_for(g) gives
+    grouping g's context)."""
+    from chiaro_b200 import scenes
+    from chiaro_b200.depth import DeviceStage
+    groupings = scenes.make_capture(seed, render_device=device, planes=planes, surfaces=surfaces)
+    return [DeviceStage(g.inputs(), 0, g.alignments(), g.options, context=ctx_for(i))
+            for i, g in enumerate(groupings)], groupings
+
+
+def config2_capture(args, ctx, torch, device):
+    """Config 2: one 16-module capture's 10 reference/source groupings (4160x3120 to
+    1040x780, 64/128/192 planes; mid and tele modules behind mirrors) through the whole
+    stage: one call per grouping in turn, the same replayed from their CUDA graphs, and all
+    groupings at once, each on its own context and stream from its own host thread. Device
+    time between events on torch's stream that every context's stream waits on."""
+    import threading
+    from chiaro_b200.runtime import DepthContext
+    contexts = [DepthContext(device.index or 0) for _ in range(10)]
+    stages, groupings = capture_stages(args.seed, lambda i: contexts[i], device)
+    cells = sum(stage_bytes(g)["cells"] for g in groupings)
+    current = torch.cuda.current_stream(device)
+
+    def timed(fn, steps):
         for _ in range(max(args.warmup, 2)):
             fn()
-        total, steps = 0.0, max(1, min(args.steps, 5))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(current)
         for _ in range(steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
             fn()
-            with torch.cuda.stream(stream):
-                e1.record(stream)
-            e1.synchronize()
-            total += e0.elapsed_time(e1)
-        return round(total / steps, 4)
+        for st in stages:
+            current.wait_stream(st.stream)
+        e1.record(current)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
 
-    def banded(net):
-        offsets = net.propose(costs, guidance, full.columns, full.rows, full.labels, tile, width)
-        ctx.check(lib.chiaro_sgm_banded_device(ctx.handle, costs.data_ptr(), guidance.data_ptr(), full.columns,
-                                               full.rows, full.labels, offsets.data_ptr(), tile, width, margin,
-                                               winner.data_ptr(), fallback.data_ptr()))
+    def sequential():
+        for st in stages:
+            if not st():
+                raise RuntimeError("the stage returned None on a capture grouping")
 
-    timing = {"full_range_sgm": timed(lambda: ctx.check(lib.chiaro_sgm_aggregate_device(
-        ctx.handle, costs.data_ptr(), guidance.data_ptr(), full.columns, full.rows, full.labels, out.data_ptr())))}
-    for name, net in nets.items():
-        timing[f"propose_{name}"] = timed(lambda: net.propose(costs, guidance, full.columns, full.rows, full.labels,
-                                                              tile, width))
-        timing[f"propose_banded_fallback_{name}"] = timed(lambda: banded(net))
-    # the banded SGM itself, with no tile falling back: every offset at label 1, every cost flat
-    flat = torch.full_like(costs, 2.25)
-    ones = torch.ones(tx * ty, dtype=torch.int32, device=device)
-    timing["banded_sgm_no_fallback"] = timed(lambda: ctx.check(lib.chiaro_sgm_banded_device(
-        ctx.handle, flat.data_ptr(), guidance.data_ptr(), full.columns, full.rows, full.labels, ones.data_ptr(), tile,
-        width, margin, winner.data_ptr(), fallback.data_ptr())))
-    assert int(fallback.sum()) == 0
-    del flat, costs, out
+    def concurrent():
+        errors = []
+
+        def run(st):
+            try:
+                st()
+            except Exception as e:  # reported below
+                errors.append(e)
+        threads = [threading.Thread(target=run, args=(st,)) for st in stages]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+
+    steps = max(1, min(args.steps, 5))
+    seq_ms = timed(sequential, steps)
+    conc_ms = timed(concurrent, steps)
+    for st in stages:
+        st.graph = True
+    graph_ms = timed(sequential, steps)
+    for st in stages:
+        st.graph = False
+    per = []
+    for st, g in zip(stages, groupings):
+        st()
+        per.append({"raster": [g.width, g.height], "planes": g.options.planes, "sources": len(g.cameras) - 1,
+                    "mirrored": any(c.pose_kind == 1 for c in g.cameras), "stage_ms": st.ctx.timings()["total"]})
+    out = {"groupings": len(stages), "sgm_cells_per_capture": cells,
+           "sequential_ms": round(seq_ms, 3), "graph_replay_ms": round(graph_ms, 3),
+           "concurrent_streams_ms": round(conc_ms, 3),
+           "gcells_s": {"sequential": round(cells / seq_ms / 1e6, 3), "graph_replay": round(cells / graph_ms / 1e6, 3),
+                        "concurrent_streams": round(cells / conc_ms / 1e6, 3)},
+           "per_grouping": per,
+           "note": "whole stage per grouping (cost volume, SGM seeding the direct pass, filters, decisions); "
+                   "the SGM of each grouping is its own launch"}
+    del stages
+    for c in contexts:
+        c.close()
     torch.cuda.empty_cache()
-    return {"tile_nodes": tile, "band_labels": width, "fallback_margin_nodes": margin,
-            "train": {"scenes": args.band_train, "full_resolution_scenes": args.band_train_full,
-                      "workload": "five_view's structure at 1040x780 (reference + 4 sources), 192 planes",
-                      "render_s": round(render_s, 1), **training},
-            "held_out_1040x780": dict(held_scores, scenes=args.band_eval,
-                                      wide_tile_fraction=round(float(np.mean(
-                                          [bandnet.wide_tile_fraction(s, tile, width) for s in held])), 4)),
-            "workload_full_resolution": dict(full_scores, labels=full.labels,
-                                             wide_tile_fraction=round(bandnet.wide_tile_fraction(full, tile,
-                                                                                                 width), 4)),
-            "timing_ms_full_resolution": timing,
-            "note": "agreement: banded winners within one plane of the full-range SGM's over tested coarse nodes; "
-                    "wide_tile_fraction: tiles whose full-range winners span more than band - 3 labels"}
+    return out
+
+
+def config4_stream(args, ctx, torch, device):
+    """Config 4: a stream of seeded 16-module captures (plane counts drawn per grouping from
+    {64, 128, 192}, 4-20 slanted planes and 0-5 spheres per capture): the coarse search of
+    every grouping in plain form and in learned-band form (the trained network if its
+    weights are present, else the naive band), timed per capture (device time of the
+    searches; rendering and uploads outside), with captures/s, Gcells/s and the banded
+    form's agreement with the plain one."""
+    import numpy as np
+    from chiaro_b200.coarse import BandOptions, coarse_depth
+    net, _ = band_network(ctx, device)
+    band = BandOptions(net.params if net is not None else None, 4, 24, 8, 0.5)
+    rng = np.random.default_rng(args.seed + 4)
+    totals = dict(plain_ms=0.0, banded_ms=0.0, cells=0, tested=0, within_one=0, tiles=0, fallback=0)
+    for c in range(args.captures):
+        planes = [int(rng.choice([64, 128, 192])) for _ in range(10)]
+        surfaces = (int(rng.integers(4, 21)), int(rng.integers(0, 6)))
+        stages, groupings = capture_stages(50000 + c, lambda i: ctx, device, planes=planes, surfaces=surfaces)
+        if c == 0:  # warm-up on the first capture
+            for st in stages:
+                coarse_depth(st)
+                coarse_depth(st, band)
+        for st, g in zip(stages, groupings):
+            plain = coarse_depth(st)
+            banded = coarse_depth(st, band)
+            totals["plain_ms"] += plain.report["ms"]["total"]
+            totals["banded_ms"] += banded.report["ms"]["total"]
+            totals["cells"] += stage_bytes(g)["cells"]
+            tested = plain.tested.cpu().numpy().astype(bool)
+            diff = np.abs(banded.winner.cpu().numpy().astype(np.int64) - plain.winner.cpu().numpy())[tested]
+            totals["tested"] += int(tested.sum())
+            totals["within_one"] += int((diff <= 1).sum())
+            totals["tiles"] += banded.report["tiles"]
+            totals["fallback"] += banded.report["fallback_tiles"]
+        del stages, groupings
+    n = args.captures
+    return {"captures": n, "groupings_per_capture": 10, "sgm_cells": totals["cells"],
+            "band": "learned (committed weights)" if net is not None else "naive (no weights present)",
+            "plain": {"ms_per_capture": round(totals["plain_ms"] / n, 3),
+                      "captures_per_s": round(1e3 * n / totals["plain_ms"], 3),
+                      "gcells_s": round(totals["cells"] / totals["plain_ms"] / 1e6, 3)},
+            "banded": {"ms_per_capture": round(totals["banded_ms"] / n, 3),
+                       "captures_per_s": round(1e3 * n / totals["banded_ms"], 3),
+                       "gcells_s": round(totals["cells"] / totals["banded_ms"] / 1e6, 3),
+                       "within_one_plane": round(totals["within_one"] / max(totals["tested"], 1), 5),
+                       "fallback_rate": round(totals["fallback"] / max(totals["tiles"], 1), 5)},
+            "speedup_banded_vs_plain": round(totals["plain_ms"] / totals["banded_ms"], 3),
+            "note": "coarse search (cost volume, SGM, winners) of every grouping; device time from the "
+                    "library's CUDA events; the whole stage of a capture is config2"}
 
 
 def run_reference(args, rank, world):

@@ -58,7 +58,13 @@ __device__ __forceinline__ int cost_slot_label(const CostParams &p, int node, in
     return slot;
 }
 
+// Threads of a node CTA: T (a multiple of 32) is the kernel's template parameter; the
+// stage's default is COST_THREADS, and the autotuner times the COST_SHAPES once per
+// (targets, labels scored, radius) bucket. Every shape lists, scores and aggregates the
+// same items, each score computed alone and the views aggregated in their order, so the
+// results are the same bits whatever the shape.
 constexpr int COST_THREADS = 128;
+constexpr int COST_SHAPES[] = {64, 96, 128, 160, 192};
 constexpr int COST_MAX_CHUNKS = 32;  // item chunks listed per barrier pair
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16; }
@@ -105,20 +111,22 @@ __device__ inline NodeSmem carve_node_smem(unsigned char *base, int V, int taps,
     return s;
 }
 
-__global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams p) {
+// Registers bounded to 64 per thread at every shape (1024 / T CTAs per SM).
+template <int T>
+__global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patch;
-    __shared__ unsigned warp_undefined[COST_THREADS / 32];  // bit v: a tap of target v has no global warp
-    __shared__ int counts[COST_MAX_CHUNKS][2][COST_THREADS / 32];  // [chunk][fast, exact][warp]
+    __shared__ unsigned warp_undefined[T / 32];  // bit v: a tap of target v has no global warp
+    __shared__ int counts[COST_MAX_CHUNKS][2][T / 32];  // [chunk][fast, exact][warp]
     const unsigned full = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int warps = COST_THREADS / 32;
+    const int warps = T / 32;
     const int out_row = blockIdx.x;
     const int node = p.node_list ? __ldg(p.node_list + out_row) : out_row;
     const int V = p.n_targets, D = p.slots, full_labels = p.labels;
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
     const int total = V * D;
-    const int chunks = (total + COST_THREADS - 1) / COST_THREADS;
+    const int chunks = (total + T - 1) / T;
     NodeSmem s = carve_node_smem(smem_raw, V, taps, D);
     const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
     const DevView &rv = p.views[p.reference];
@@ -139,7 +147,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
     }
     bool sampled = true;
-    for (int t = tid; t < taps; t += COST_THREADS) {
+    for (int t = tid; t < taps; t += T) {
         int dx, dy;
         tap_offset(t, p.radius, dx, dy);
         float value = 0.0f;
@@ -157,7 +165,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         s.rr[t] = weighted * value;
     }
     unsigned undefined = 0u;
-    for (int i = tid; i < V * taps; i += COST_THREADS) {
+    for (int i = tid; i < V * taps; i += T) {
         const int v = i / taps, t = i - v * taps;
         int dx, dy;
         tap_offset(t, p.radius, dx, dy);
@@ -175,7 +183,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         s.gh[i] = make_double2((double)qx * 0.5, (double)qy * 0.5);
     }
     // displacement of every (target, slot) item, view-major: item = v * D + slot
-    for (int item = tid; item < total; item += COST_THREADS) {
+    for (int item = tid; item < total; item += T) {
         const int v = item / D, label = cost_slot_label(p, node, item - v * D);
         ViewGeom g;
         geom_from_rec(p.geometry[(size_t)node * V + v], origin, g);
@@ -213,7 +221,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
     __syncthreads();
 
     // ---- which items are scored, and on which path; then list them, fast
-    // first. Chunk c holds items c * COST_THREADS + tid; the counts of up to
+    // first. Chunk c holds items c * T + tid; the counts of up to
     // COST_MAX_CHUNKS chunks are exchanged per barrier pair.
     const bool patch_ok = patch.ok;
     unsigned taps_bad = 0u;
@@ -224,7 +232,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
         const int c1 = min(chunks, c0 + COST_MAX_CHUNKS);
         unsigned fast_bits = 0u, exact_bits = 0u;
         for (int c = c0; c < c1; ++c) {
-            const int item = c * COST_THREADS + tid;
+            const int item = c * T + tid;
             bool scored = false, fast = false;
             if (item < total) {
                 const int v = item / D;
@@ -261,7 +269,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
             const bool is_fast = (fast_bits >> (c - c0)) & 1u, is_exact = (exact_bits >> (c - c0)) & 1u;
             const unsigned fast_mask = __ballot_sync(full, is_fast);
             const unsigned exact_mask = __ballot_sync(full, is_exact);
-            const int item = c * COST_THREADS + tid;
+            const int item = c * T + tid;
             if (is_fast) s.list[fast_at + __popc(fast_mask & below)] = (unsigned short)item;
             if (is_exact) s.list[total - 1 - (exact_at + __popc(exact_mask & below))] = (unsigned short)item;
         }
@@ -270,7 +278,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
 
     // ---- the correlations of the listed items
     const int listed = n_fast + n_exact;
-    for (int j = tid; j < listed; j += COST_THREADS) {
+    for (int j = tid; j < listed; j += T) {
         const int item = s.list[j < n_fast ? j : total - 1 - (j - n_fast)];
         const int v = item / D;
         const DevView &tv = p.views[p.targets[v]];
@@ -285,7 +293,7 @@ __global__ void __launch_bounds__(COST_THREADS, 8) cost_volume_kernel(CostParams
 
     // ---- aggregate the views per label and price the label (depth.rs:1233-1246)
     int any_finite = 0;
-    for (int slot = tid; slot < D; slot += COST_THREADS) {
+    for (int slot = tid; slot < D; slot += T) {
         const int label = cost_slot_label(p, node, slot);
         float sc[MAX_VIEWS];
         for (int v = 0; v < V; ++v) sc[v] = s.score[v * D + slot];

@@ -70,6 +70,10 @@ struct chiaro_depth_ctx {
     int union_retries = -1;
     uint64_t memory_limit = 0;
     uint64_t memory_held = 0;
+    // launch shapes chosen by the autotuner: cost-volume threads per node CTA per bucket;
+    // autotune: 1 tune, 0 the default shape, or a forced shape (threads per node CTA)
+    int autotune = 1;
+    std::map<uint64_t, int> cost_tuning;
 };
 
 namespace {
@@ -204,13 +208,74 @@ void set_smem_limits() {
     CK(cudaGetDevice(&device));
     std::lock_guard<std::mutex> guard(lock);
     if (std::find(done_devices.begin(), done_devices.end(), device) != done_devices.end()) return;
-    CK(cudaFuncSetAttribute(cost_volume_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(cost_volume_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(cost_volume_kernel<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(cost_volume_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(cost_volume_kernel<160>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(cost_volume_kernel<192>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(direct_depth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(direct_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(target_decision_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(target_decision_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CK(cudaFuncSetAttribute(align_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done_devices.push_back(device);
+}
+
+// ---- cost-volume launch shapes (the autotuner) -----------------------------------------
+typedef void (*CostKernel)(CostParams);
+
+CostKernel cost_kernel_for(int threads) {
+    switch (threads) {
+        case 64: return cost_volume_kernel<64>;
+        case 96: return cost_volume_kernel<96>;
+        case 160: return cost_volume_kernel<160>;
+        case 192: return cost_volume_kernel<192>;
+        default: return cost_volume_kernel<128>;
+    }
+}
+
+// Launch build_cost_volume over n_rows node CTAs. With autotuning on, the first launch of a
+// (targets, labels scored, radius) bucket large enough to time (at least 4096 nodes, outside
+// any stream capture) runs every shape twice and keeps the fastest second run for the
+// context's later launches; every shape writes the same bits, and the last launch below
+// writes the outputs again.
+void launch_cost(chiaro_depth_ctx *ctx, const CostParams &p, size_t n_rows, size_t smem) {
+    cudaStream_t s = ctx->stream;
+    const uint64_t key = ((uint64_t)p.n_targets << 24) | ((uint64_t)p.slots << 8) | (uint64_t)p.radius;
+    int threads = ctx->autotune > 1 ? ctx->autotune : COST_THREADS;
+    auto it = ctx->cost_tuning.find(key);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s, &capture));
+    if (ctx->autotune > 1) {
+        // a forced shape
+    } else if (it != ctx->cost_tuning.end()) {
+        threads = it->second;
+    } else if (ctx->autotune == 1 && n_rows >= 4096 && capture == cudaStreamCaptureStatusNone) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        float best = INFINITY;
+        for (int t : COST_SHAPES) {
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2; ++rep) {
+                CK(cudaEventRecord(e0, s));
+                cost_kernel_for(t)<<<(unsigned)n_rows, t, smem, s>>>(p);
+                CK(cudaGetLastError());
+                CK(cudaEventRecord(e1, s));
+                CK(cudaEventSynchronize(e1));
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+            }
+            if (ms < best) {
+                best = ms;
+                threads = t;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        ctx->cost_tuning[key] = threads;
+    }
+    cost_kernel_for(threads)<<<(unsigned)n_rows, threads, smem, s>>>(p);
+    CK(cudaGetLastError());
 }
 
 // Per (node, target) geometry records of a step-spaced grid.
@@ -999,8 +1064,7 @@ void coarse_cost(chiaro_depth_ctx *ctx, const CoarseGrid &g, int reference, cons
     const size_t smem = node_smem_bytes(g.V, taps, slots);
     if ((size_t)g.V * slots > 65535 || smem > 200 * 1024)
         throw CudaError{cudaErrorInvalidValue, "cost volume: targets x labels exceed the node CTA's shared memory"};
-    cost_volume_kernel<<<(unsigned)n_rows, COST_THREADS, smem, ctx->stream>>>(p);
-    CK(cudaGetLastError());
+    launch_cost(ctx, p, n_rows, smem);
 }
 
 // The coarse search of the stage's reference grid (depth.rs:1187-1467 up to the winner):
@@ -1593,8 +1657,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         const size_t smem = node_smem_bytes(V, taps, D);
         if ((size_t)V * D > 65535 || smem > 200 * 1024)
             throw CudaError{cudaErrorInvalidValue, "cost volume: targets x labels exceed the node CTA's shared memory"};
-        cost_volume_kernel<<<(unsigned)N, COST_THREADS, smem, s>>>(p);
-        CK(cudaGetLastError());
+        launch_cost(ctx, p, N, smem);
     }
     record_event(ctx->events[1], s, capturing);
     // ---- SGM
@@ -2146,6 +2209,29 @@ int chiaro_depth_set_memory_limit(chiaro_depth_ctx *ctx, uint64_t bytes) {
 }
 
 uint64_t chiaro_depth_memory_held(const chiaro_depth_ctx *ctx) { return ctx ? ctx->memory_held : 0; }
+
+int chiaro_depth_set_autotune(chiaro_depth_ctx *ctx, int32_t mode) {
+    if (!ctx) return CHIARO_ERR_ARGUMENT;
+    bool shape = false;
+    for (int t : COST_SHAPES) shape |= t == mode;
+    if (mode != 0 && mode != 1 && !shape) return CHIARO_ERR_ARGUMENT;
+    ctx->autotune = mode;
+    if (mode != 1) ctx->cost_tuning.clear();
+    return CHIARO_OK;
+}
+
+int chiaro_depth_tuning(const chiaro_depth_ctx *ctx, uint64_t *keys, int32_t *threads, int capacity) {
+    if (!ctx) return 0;
+    int n = 0;
+    for (const auto &kv : ctx->cost_tuning) {
+        if (n < capacity) {
+            if (keys) keys[n] = kv.first;
+            if (threads) threads[n] = kv.second;
+        }
+        ++n;
+    }
+    return n;
+}
 
 int chiaro_depth_last_timings(const chiaro_depth_ctx *ctx, float *ms, int capacity) {
     if (!ctx || !ms) return 0;

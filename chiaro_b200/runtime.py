@@ -56,6 +56,8 @@ SIGNATURES = {
     "chiaro_depth_set_union_retry_limit": (C.c_int, [C.c_void_p, C.c_int32]),
     "chiaro_depth_set_memory_limit": (C.c_int, [C.c_void_p, C.c_uint64]),
     "chiaro_depth_memory_held": (C.c_uint64, [C.c_void_p]),
+    "chiaro_depth_set_autotune": (C.c_int, [C.c_void_p, C.c_int32]),
+    "chiaro_depth_tuning": (C.c_int, [C.c_void_p, P(C.c_uint64), P(C.c_int32), C.c_int]),
     "chiaro_align_options_default": (None, [P(abi.AlignOptionsC)]),
     "chiaro_align_module": (C.c_int, [C.c_void_p, P(abi.AlignInputC), P(abi.AlignInputC), C.c_int32,
                                       P(abi.AlignOptionsC), P(abi.WarpC), P(abi.WarpC), P(C.c_float),
@@ -219,6 +221,19 @@ class DepthContext:
 
     def memory_held(self) -> int:
         return int(self.lib.chiaro_depth_memory_held(self.handle))
+
+    def set_autotune(self, mode) -> None:
+        """Launch shapes of the cost volume: True/1 autotune (the default), False/0 the default
+        shape, or a CTA size (64, 96, 128, 160, 192) for every launch."""
+        self.check(self.lib.chiaro_depth_set_autotune(self.handle, int(mode)))
+
+    def tuning(self) -> dict:
+        """The autotuner's choices: {(targets, labels scored, radius): threads per node CTA}."""
+        n = int(self.lib.chiaro_depth_tuning(self.handle, None, None, 0))
+        keys = (C.c_uint64 * max(n, 1))()
+        threads = (C.c_int32 * max(n, 1))()
+        n = int(self.lib.chiaro_depth_tuning(self.handle, keys, threads, n))
+        return {(int(k) >> 24, (int(k) >> 8) & 0xFFFF, int(k) & 0xFF): int(t) for k, t in zip(keys[:n], threads[:n])}
 
     def make_debug(self, arrays: dict) -> DepthDebugC:
         dbg = DepthDebugC()

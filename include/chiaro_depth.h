@@ -289,6 +289,18 @@ int chiaro_depth_set_union_retry_limit(chiaro_depth_ctx *ctx, int32_t retries);
 int chiaro_depth_set_memory_limit(chiaro_depth_ctx *ctx, uint64_t bytes);
 uint64_t chiaro_depth_memory_held(const chiaro_depth_ctx *ctx);
 
+/* No counterpart in the reference: launch-shape autotuning. With mode 1 (the default),
+ * the first cost-volume launch of each (targets, labels scored, patch radius) bucket with
+ * at least 4096 nodes, outside any stream capture, times every candidate CTA size (64, 96,
+ * 128, 160 and 192 threads per node) and keeps the fastest for the context's later launches.
+ * Every size gives the same bits. Mode 0 runs the default of 128 threads; mode 64, 96, 128,
+ * 160 or 192 runs that size everywhere; both forget the choices made. Other modes return
+ * CHIARO_ERR_ARGUMENT. chiaro_depth_tuning writes up to `capacity` choices, each a bucket
+ * key ((targets << 24) | (labels scored << 8) | radius) and its threads, and returns how
+ * many the context holds. */
+int chiaro_depth_set_autotune(chiaro_depth_ctx *ctx, int32_t mode);
+int chiaro_depth_tuning(const chiaro_depth_ctx *ctx, uint64_t *keys, int32_t *threads, int capacity);
+
 /* Device time in milliseconds of each stage of the last call on this context:
  * [0] cost volume, [1] SGM, [2] select, [3] direct pass, [4] filters,
  * [5] per-target decisions, [6] whole stage. Returns the count written. */
