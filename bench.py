@@ -67,6 +67,10 @@ def parse_args():
     p.add_argument("--captures", type=int, default=32, help="captures of the config-4 stream")
     p.add_argument("--no-learned-band", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the per-config sub-objects (two_view, ...)")
+    p.add_argument("--profile-case", choices=["stage", "sgm", "bandnet"], default=None,
+                   help="run only one case's kernels, for an ncu capture (small device footprint): the five-view "
+                        "stage (3 warm-up calls and one more), its SGMs (f32 and u16) on a five-view-shaped volume, "
+                        "or the band network (a full-resolution proposal and a training step)")
     return p.parse_args()
 
 
@@ -996,9 +1000,60 @@ def run_reference(args, rank, world):
     }
 
 
+def profile_case(args):
+    """One case's kernels alone, for an ncu capture of committed code (see --profile-case)."""
+    import numpy as np
+    import torch
+    from chiaro_b200 import build, scenes
+    from chiaro_b200.runtime import DepthContext
+    build.build()
+    device = torch.device("cuda", 0)
+    ctx = DepthContext(0)
+    if args.profile_case == "stage":
+        from chiaro_b200.depth import DeviceStage
+        scene = scenes.workload("five_view", seed=args.seed)  # rendered on the host: no torch kernels to skip
+        stage = DeviceStage(scene.inputs(), 0, scene.alignments(), scene.options, context=ctx)
+        for _ in range(4):
+            assert stage()
+    elif args.profile_case == "sgm":
+        c, r, d = 521, 391, 129
+        g = torch.Generator(device=device)
+        g.manual_seed(args.seed)
+        costs = torch.rand(c * r * d, generator=g, device=device) * 2.25
+        guidance = torch.rand(c * r, generator=g, device=device) * 7.0
+        out = torch.empty_like(costs)
+        best = torch.empty(c * r, dtype=torch.int16, device=device)
+        for _ in range(2):
+            ctx.check(ctx.lib.chiaro_sgm_aggregate_device(ctx.handle, costs.data_ptr(), guidance.data_ptr(), c, r, d,
+                                                          out.data_ptr()))
+            ctx.check(ctx.lib.chiaro_sgm_aggregate_u16_device(ctx.handle, costs.data_ptr(), guidance.data_ptr(), c,
+                                                              r, d, None, best.data_ptr()))
+    else:
+        from chiaro_b200 import bandnet
+        from chiaro_b200.coarse import PREPASS_SLOTS
+        net, _ = band_network(ctx, device)
+        net = net or bandnet.BandNet(ctx, seed=args.seed)
+        columns, rows, labels = 521, 391, 193
+        rng = np.random.default_rng(args.seed)
+        costs = torch.from_numpy(rng.uniform(0, 2.25, (columns * rows, PREPASS_SLOTS)).astype(np.float32)).to(device)
+        guidance = torch.from_numpy(rng.uniform(0, 7, columns * rows).astype(np.float32)).to(device)
+        for _ in range(2):
+            net.propose(costs, guidance, columns, rows, labels, 4, 24, stride=PREPASS_SLOTS)
+        sample = bandnet.Sample(costs.reshape(-1), guidance, torch.from_numpy(
+            rng.integers(1, labels, columns * rows).astype(np.int32)).to(device),
+            torch.ones(columns * rows, dtype=torch.uint8, device=device), columns, rows, labels, PREPASS_SLOTS)
+        net.train([sample], 2, 1e-3)
+    torch.cuda.synchronize()
+    ctx.close()
+    print(json.dumps({"profile_case": args.profile_case, "ok": True}))
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_env()
+    if args.profile_case:
+        profile_case(args)
+        return
     if args.impl == "reference":
         line = run_reference(args, rank, world)
     else:

@@ -90,6 +90,188 @@ __global__ void net_features_kernel(const float *__restrict__ costs, int stride,
     features[(size_t)node * NET_CH + lane] = __float2bfloat16_rn(value);
 }
 
+// ---- the convolution on the 5th-generation tensor cores (tcgen05) ------------------------
+// An implicit GEMM per tile of 128 consecutive pixels of one image row: M = 128 pixels,
+// N = 32 output channels, K = 9 taps x 32 input channels, as 18 tcgen05.mma of kind::f16
+// (bf16 operands, fp32 accumulator in tensor memory, 128 lanes x 32 columns). Both operands
+// sit in shared memory in the canonical K-major layout without swizzle: 16-byte rows of 8
+// channels, 8-row groups 128 bytes apart (SBO), the two 8-channel halves of a 16-deep K step
+// LBO apart. The staged input holds, per window row and 8-channel block, 130 pixels (the
+// tile and one on each side) in consecutive 16-byte rows, so a tap's pixel shift moves the
+// A descriptor's start by 16 bytes and no shifted copy is made. The layer's weights are
+// staged once per persistent CTA as [tap][channel block][co][8]. One thread issues the MMAs
+// and commits them to an mbarrier; the CTA waits on it (a bounded wait: a run-out sets the
+// status word and the CTA frees its tensor memory and returns), then each warp reads its
+// 32 accumulator lanes (tcgen05.ld 32x32b), adds the bias, applies ReLU or the mask and
+// stores bf16 (and channel 0 in fp32 for the last layer).
+constexpr int NET_TC_M = 128;   // pixels per tile (accumulator lanes)
+constexpr int NET_TC_PP = 136;  // staged pixels per window row and channel block (130 used)
+constexpr size_t NET_TC_W_BYTES = (size_t)NET_TAPS * 4 * NET_CH * 16;
+constexpr size_t NET_TC_IN_BYTES = (size_t)3 * 4 * NET_TC_PP * 16;
+constexpr size_t NET_TC_SMEM = NET_TC_W_BYTES + NET_TC_IN_BYTES;
+// instruction descriptor: fp32 accumulator (bits 4-5), bf16 A and B (bits 7-9, 10-12),
+// both K-major, N >> 3 (bits 17-22), M >> 4 (bits 24-28)
+constexpr uint32_t NET_TC_IDESC =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NET_CH >> 3) << 17) | ((uint32_t)(NET_TC_M >> 4) << 24);
+constexpr long NET_TC_SPIN = 1L << 22;  // polls of the MMA barrier (each a bounded try_wait) before giving up
+constexpr int NET_TC_GAVE_UP = 1;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, no swizzle (layout type 0), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t address, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((address >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+        :
+        : "r"(tmem), "l"(a), "l"(b), "r"(NET_TC_IDESC), "r"(accumulate), "r"(0u));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the MMA barrier's phase: true when it completed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase) {
+    for (long spin = 0; spin < NET_TC_SPIN; ++spin)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+__global__ void __launch_bounds__(NET_TC_M) net_conv_tc_kernel(
+    const __nv_bfloat16 *__restrict__ in, int images, int height, int width, const __nv_bfloat16 *__restrict__ w,
+    const float *__restrict__ bias, int relu, const __nv_bfloat16 *__restrict__ mask, __nv_bfloat16 *__restrict__ out,
+    float *__restrict__ out_f32, int *status) {
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    __shared__ __align__(8) uint64_t mma_bar;
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    unsigned char *wsm = tc_smem, *insm = tc_smem + NET_TC_W_BYTES;
+    const uint32_t w_addr = smem_u32(wsm), in_addr = smem_u32(insm), bar = smem_u32(&mma_bar);
+    // the layer's weights w[tap][co][ci] as [tap][channel block][co][8 channels]
+    for (int c = tid; c < NET_TAPS * NET_CH * 4; c += NET_TC_M) {
+        const int row = c >> 2, j = c & 3, tap = row / NET_CH, co = row - tap * NET_CH;
+        *reinterpret_cast<uint4 *>(wsm + (((size_t)tap * 4 + j) * NET_CH + co) * 16) =
+            *reinterpret_cast<const uint4 *>(w + (size_t)row * NET_CH + j * 8);
+    }
+    if (warp == 0) {  // 32 columns of tensor memory: the 128 x 32 fp32 accumulator
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(32u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+    const int segments = (width + NET_TC_M - 1) / NET_TC_M;
+    const long tiles = (long)images * height * segments;
+    uint32_t phase = 0;
+    bool failed = false;
+    for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int n = (int)(tile / ((long)height * segments));
+        const int rest = (int)(tile - (long)n * height * segments);
+        const int y = rest / segments, x0 = (rest - y * segments) * NET_TC_M;
+        const __nv_bfloat16 *image = in + (size_t)n * height * width * NET_CH;
+        // the window: rows y - 1 .. y + 1, pixels x0 - 1 .. x0 + 128, zero outside the image
+        for (int c = tid; c < 3 * 130 * 4; c += NET_TC_M) {
+            const int j = c & 3, px = (c >> 2) % 130, r = (c >> 2) / 130;
+            const int xx = x0 - 1 + px, yy = y - 1 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (yy >= 0 && yy < height && xx >= 0 && xx < width)
+                v = *reinterpret_cast<const uint4 *>(image + ((size_t)yy * width + xx) * NET_CH + j * 8);
+            *reinterpret_cast<uint4 *>(insm + (((size_t)r * 4 + j) * NET_TC_PP + px) * 16) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+            for (int tap = 0; tap < NET_TAPS; ++tap) {
+                const int r = tap / 3, dx = tap % 3;
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+                    const uint64_t a = umma_desc(
+                        in_addr + (uint32_t)((((r * 4 + 2 * half) * NET_TC_PP) + dx) * 16), NET_TC_PP * 16, 128);
+                    const uint64_t b = umma_desc(w_addr + (uint32_t)(((tap * 4 + 2 * half) * NET_CH) * 16), NET_CH * 16,
+                                                 128);
+                    umma_bf16(tmem, a, b, (tap | half) != 0);
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        // the MMAs are complete (their reads of the window too) once the barrier's phase flips
+        failed = __syncthreads_or(!mbar_wait_bounded(bar, phase));
+        if (failed) break;
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        uint32_t acc[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(acc[0]), "=r"(acc[1]), "=r"(acc[2]), "=r"(acc[3]), "=r"(acc[4]), "=r"(acc[5]), "=r"(acc[6]),
+              "=r"(acc[7]), "=r"(acc[8]), "=r"(acc[9]), "=r"(acc[10]), "=r"(acc[11]), "=r"(acc[12]), "=r"(acc[13]),
+              "=r"(acc[14]), "=r"(acc[15]), "=r"(acc[16]), "=r"(acc[17]), "=r"(acc[18]), "=r"(acc[19]),
+              "=r"(acc[20]), "=r"(acc[21]), "=r"(acc[22]), "=r"(acc[23]), "=r"(acc[24]), "=r"(acc[25]),
+              "=r"(acc[26]), "=r"(acc[27]), "=r"(acc[28]), "=r"(acc[29]), "=r"(acc[30]), "=r"(acc[31])
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int x = x0 + tid;  // this thread's accumulator lane is pixel x0 + tid
+        if (x < width) {
+            const size_t p = ((size_t)n * height + y) * width + x;
+            unsigned packed[16];
+#pragma unroll
+            for (int co = 0; co < NET_CH; co += 2) {
+                float v0 = __uint_as_float(acc[co]) + (bias ? bias[co] : 0.0f);
+                float v1 = __uint_as_float(acc[co + 1]) + (bias ? bias[co + 1] : 0.0f);
+                if (relu) {
+                    v0 = fmaxf(v0, 0.0f);
+                    v1 = fmaxf(v1, 0.0f);
+                }
+                if (mask) {
+                    const __nv_bfloat16 *m = mask + p * NET_CH + co;
+                    if (!(__bfloat162float(m[0]) > 0.0f)) v0 = 0.0f;
+                    if (!(__bfloat162float(m[1]) > 0.0f)) v1 = 0.0f;
+                }
+                if (co == 0 && out_f32) out_f32[p] = v0;
+                packed[co / 2] = pack_bf16(v0, v1);
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(out + p * NET_CH);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                dst[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();  // every warp has read the accumulator before the next tile's MMAs
+    }
+    if (failed) {
+        if (tid == 0) atomicOr(status, NET_TC_GAVE_UP);
+        mbar_wait_bounded(bar, phase);  // give MMAs still in flight a last bounded wait
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u));
+}
+
 // Shared-memory rows of the convolution: 32 bf16 channels padded to 40 (80 bytes), so
 // the eight 16-byte rows an ldmatrix reads fall in distinct banks.
 constexpr int NET_SROW = 40;

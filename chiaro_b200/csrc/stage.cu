@@ -923,6 +923,7 @@ struct NetState {
     __nv_bfloat16 *act[NET_LAYERS + 1];  // act[0] = features, act[l + 1] = output of layer l
     __nv_bfloat16 *grad_a, *grad_b;    // pre-activation gradients, ping-pong
     float *y;                          // channel 0 of the last layer, fp32
+    int *status;                       // NET_TC_GAVE_UP when a convolution's bounded wait ran out
     long pixels;
     int images, height, width;
 };
@@ -940,6 +941,8 @@ NetState net_state(chiaro_depth_ctx *ctx, int images, int height, int width) {
     s.grad_a = dbuf<__nv_bfloat16>(ctx, "net.grad_a", act);
     s.grad_b = dbuf<__nv_bfloat16>(ctx, "net.grad_b", act);
     s.y = dbuf<float>(ctx, "net.y", (size_t)s.pixels);
+    s.status = dbuf<int>(ctx, "net.status", 1);
+    CK(cudaMemsetAsync(s.status, 0, sizeof(int), ctx->stream));
     return s;
 }
 
@@ -952,24 +955,41 @@ void net_features(chiaro_depth_ctx *ctx, const NetState &s, const float *costs, 
     CK(cudaGetLastError());
 }
 
-// Persistent grid of the convolution: as many CTAs as are resident at once (shared memory
-// allows five per SM), or fewer when there are fewer tiles.
-unsigned net_conv_blocks(chiaro_depth_ctx *ctx, long tiles) {
-    return (unsigned)std::min<size_t>(div_ceil((size_t)tiles, NET_CONV_WARPS), (size_t)ctx->sm_count * 5);
+// Persistent grid of the tensor-core convolution: four CTAs per SM (44.5 KB of shared memory
+// and 32 tensor-memory columns each), or one per 128-pixel tile when there are fewer tiles.
+unsigned net_conv_tc_blocks(chiaro_depth_ctx *ctx, const NetState &s) {
+    const long tiles = (long)s.images * s.height * ((s.width + NET_TC_M - 1) / NET_TC_M);
+    return (unsigned)std::max<long>(1, std::min<long>(tiles, (long)ctx->sm_count * 4));
+}
+
+// A convolution of the band network: tcgen05 tiles (bandnet.cuh).
+void net_conv(chiaro_depth_ctx *ctx, const NetState &s, const __nv_bfloat16 *in, const __nv_bfloat16 *w,
+              const float *bias, int relu, const __nv_bfloat16 *mask, __nv_bfloat16 *out, float *out_f32) {
+    net_conv_tc_kernel<<<net_conv_tc_blocks(ctx, s), NET_TC_M, NET_TC_SMEM, ctx->stream>>>(
+        in, s.images, s.height, s.width, w, bias, relu, mask, out, out_f32, s.status);
+    CK(cudaGetLastError());
+}
+
+// The status word of the network's convolutions after the call's work (synchronises).
+int net_status(chiaro_depth_ctx *ctx, const NetState &s) {
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, s.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h & NET_TC_GAVE_UP) {
+        ctx->error = "band network: a tensor-core convolution's wait for its MMAs ran out";
+        return CHIARO_ERR_TIMEOUT;
+    }
+    return CHIARO_OK;
 }
 
 void net_forward(chiaro_depth_ctx *ctx, const NetState &s, const float *params) {
     cudaStream_t st = ctx->stream;
     net_pack_kernel<<<(unsigned)div_ceil((size_t)NET_LAYERS * NET_W, 256), 256, 0, st>>>(params, s.w, s.wt);
     CK(cudaGetLastError());
-    const long tiles = (long)s.images * s.height * ((s.width + 15) / 16);
-    const unsigned blocks = net_conv_blocks(ctx, tiles);
     for (int l = 0; l < NET_LAYERS; ++l) {
         const bool last = l + 1 == NET_LAYERS;
-        net_conv_kernel<<<blocks, 32 * NET_CONV_WARPS, NET_CONV_SMEM, st>>>(s.act[l], s.images, s.height, s.width, s.w + (size_t)l * NET_W,
-                                                params + (size_t)l * (NET_W + NET_CH) + NET_W, last ? 0 : 1,
-                                                nullptr, s.act[l + 1], last ? s.y : nullptr);
-        CK(cudaGetLastError());
+        net_conv(ctx, s, s.act[l], s.w + (size_t)l * NET_W, params + (size_t)l * (NET_W + NET_CH) + NET_W,
+                 last ? 0 : 1, nullptr, s.act[l + 1], last ? s.y : nullptr);
     }
 }
 
@@ -983,8 +1003,6 @@ void net_backward(chiaro_depth_ctx *ctx, const NetState &s, const float *params,
     const unsigned eblocks = (unsigned)std::min<size_t>(div_ceil((size_t)s.pixels, 256), (size_t)ctx->sm_count * 8);
     net_loss_kernel<<<eblocks, 256, 0, st>>>(s.y, targets, mask, s.pixels, inverse_count, 0.02f, s.grad_a, loss_sum);
     CK(cudaGetLastError());
-    const long tiles = (long)s.images * s.height * ((s.width + 15) / 16);
-    const unsigned cblocks = net_conv_blocks(ctx, tiles);
     const long chunks = (s.pixels + 16L * NET_WGRAD_STEPS - 1) / (16L * NET_WGRAD_STEPS);
     const unsigned wblocks = (unsigned)div_ceil((size_t)chunks * NET_TAPS, 4);
     __nv_bfloat16 *dpre = s.grad_a, *dnext = s.grad_b;
@@ -994,9 +1012,7 @@ void net_backward(chiaro_depth_ctx *ctx, const NetState &s, const float *params,
         net_bias_grad_kernel<<<(unsigned)ctx->sm_count * 4, 256, 0, st>>>(dpre, s.pixels, g + NET_W);
         CK(cudaGetLastError());
         if (l > 0) {  // gradient at the previous layer's output, masked by its ReLU
-            net_conv_kernel<<<cblocks, 32 * NET_CONV_WARPS, NET_CONV_SMEM, st>>>(dpre, s.images, s.height, s.width, s.wt + (size_t)l * NET_W,
-                                                     nullptr, 0, s.act[l], dnext, nullptr);
-            CK(cudaGetLastError());
+            net_conv(ctx, s, dpre, s.wt + (size_t)l * NET_W, nullptr, 0, s.act[l], dnext, nullptr);
             std::swap(dpre, dnext);
         }
     }
@@ -1173,12 +1189,14 @@ int run_coarse(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, int referenc
         }
         // the band proposal: the network on the pre-pass's costs, or the naive band
         int *offsets = dbuf<int>(ctx, "coarse.band_offsets", tiles);
+        int *net_status_word = nullptr;
         if (spec->params) {
             NetState ns = net_state(ctx, 1, g.rows, g.columns);
             net_features(ctx, ns, pre_costs, guidance, D, PREPASS_SLOTS);
             net_forward(ctx, ns, spec->params);
             net_tile_offsets_kernel<<<(unsigned)div_ceil(tiles, 128), 128, 0, s>>>(ns.y, g.columns, g.rows, D, tile,
                                                                                    band, offsets);
+            net_status_word = ns.status;
         } else {
             naive_band_offsets_kernel<<<(unsigned)div_ceil(tiles, 128), 128, 0, s>>>(pre_costs, g.columns, g.rows, D,
                                                                                      tile, band, offsets);
@@ -1218,10 +1236,16 @@ int run_coarse(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, int referenc
         }
         CK(cudaEventRecord(ctx->events[5], s));
         std::vector<uint8_t> flags(tiles), edges(tiles), crossed(tiles);
+        int net_word = 0;
+        if (net_status_word) CK(cudaMemcpyAsync(&net_word, net_status_word, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(flags.data(), fallback, tiles, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(edges.data(), edge, tiles, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(crossed.data(), consistency, tiles, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        if (net_word & NET_TC_GAVE_UP) {
+            ctx->error = "band network: a tensor-core convolution's wait for its MMAs ran out";
+            return CHIARO_ERR_TIMEOUT;
+        }
         size_t cost_floats = 0, node_count = 0;
         int most = 0;
         std::vector<BandWindow> windows = fallback_windows(flags, tiles_x, tiles_y, tile, g.columns, g.rows,
@@ -2671,7 +2695,7 @@ int chiaro_bandnet_propose_device(chiaro_depth_ctx *ctx, const float *params, co
         CK(cudaGetLastError());
         if (centres)
             CK(cudaMemcpyAsync(centres, s.y, sizeof(float) * columns * rows, cudaMemcpyDeviceToDevice, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        if (int st = net_status(ctx, s)) return st;
     } catch (const CudaError &e) {
         return fail(ctx, e);
     }
@@ -2695,7 +2719,7 @@ int chiaro_bandnet_gradient_device(chiaro_depth_ctx *ctx, const float *params, c
         CK(cudaMemsetAsync(d_loss, 0, sizeof(float), ctx->stream));
         net_backward(ctx, s, params, targets, mask, inverse, grads, d_loss);
         CK(cudaMemcpyAsync(loss, d_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        if (int st = net_status(ctx, s)) return st;
     } catch (const CudaError &e) {
         return fail(ctx, e);
     }
@@ -2730,7 +2754,7 @@ int chiaro_bandnet_train_device(chiaro_depth_ctx *ctx, float *params, float *ada
             CK(cudaGetLastError());
         }
         if (losses) CK(cudaMemcpyAsync(losses, d_losses, sizeof(float) * steps, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        if (int st = net_status(ctx, s)) return st;
     } catch (const CudaError &e) {
         return fail(ctx, e);
     }

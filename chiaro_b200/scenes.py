@@ -399,10 +399,13 @@ def _torch_cast(surfaces: List[Surface], tiles, origin, direction):
 
 
 def render_module_gpu(camera: ResolvedCamera, surfaces: List[Surface], tiles, seed: int, device,
-                      chunk_rows: int = 512):
-    """Ray cast one module on the GPU: its u16 raster [h, w] as an int32 device tensor."""
+                      chunk_pixels: int = 1 << 24):
+    """Ray cast one module on the GPU: its u16 raster [h, w] as an int32 device tensor. Rows go
+    in chunks of about chunk_pixels pixels (a whole full-resolution module in one), so the
+    torch ops run on large arrays rather than paying their launch cost per small chunk."""
     import torch
     h, w = camera.height, camera.width
+    chunk_rows = max(1, chunk_pixels // w)
     raw = torch.empty((h, w), dtype=torch.int32, device=device)
     gen = torch.Generator(device=device)
     gen.manual_seed(int(seed) & 0x7FFFFFFFFFFFFFFF)
