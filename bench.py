@@ -67,10 +67,12 @@ def parse_args():
     p.add_argument("--captures", type=int, default=32, help="captures of the config-4 stream")
     p.add_argument("--no-learned-band", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the per-config sub-objects (two_view, ...)")
-    p.add_argument("--profile-case", choices=["stage", "sgm", "bandnet"], default=None,
+    p.add_argument("--profile-case", choices=["stage", "sgm", "bandnet", "coarse"], default=None,
                    help="run only one case's kernels, for an ncu capture (small device footprint): the five-view "
                         "stage (3 warm-up calls and one more), its SGMs (f32 and u16) on a five-view-shaped volume, "
-                        "or the band network (a full-resolution proposal and a training step)")
+                        "or the band network (a full-resolution proposal and a training step), or the coarse "
+                        "search on five_view with the default CTA shape (plain, then the naive band: the cost "
+                        "volume at 129, 17 and 25 labels per node)")
     return p.parse_args()
 
 
@@ -371,6 +373,10 @@ def run_ours(args, rank, world, local):
                          "api": "chiaro_b200.depth.refine_multiview_depth (host buffers: the scene's own pageable "
                                 "numpy planes, as a caller passing ordinary host vectors)"},
         **({"configs": configs} if configs else {}),
+        "autotune": {"cost_volume_threads_per_node": {f"targets {t}, labels {l}, radius {r}": v
+                                                      for (t, l, r), v in ctx.tuning().items()},
+                     "note": "CTA size of the cost volume chosen by timing 64-192 threads per node once per bucket "
+                             "(every size gives the same bits)"},
         "gpu_launches": launches * args.steps,
         "clocks": clk,
     }
@@ -1015,6 +1021,15 @@ def profile_case(args):
         stage = DeviceStage(scene.inputs(), 0, scene.alignments(), scene.options, context=ctx)
         for _ in range(4):
             assert stage()
+    elif args.profile_case == "coarse":
+        from chiaro_b200.coarse import BandOptions, coarse_depth
+        from chiaro_b200.depth import DeviceStage
+        ctx.set_autotune(128)  # one shape: the launches are the same on every run
+        scene = scenes.workload("five_view", seed=args.seed)
+        stage = DeviceStage(scene.inputs(), 0, scene.alignments(), scene.options, context=ctx)
+        for _ in range(2):
+            coarse_depth(stage)
+            coarse_depth(stage, BandOptions(None, 4, 24, 8, 0.5))
     elif args.profile_case == "sgm":
         c, r, d = 521, 391, 129
         g = torch.Generator(device=device)

@@ -8,17 +8,13 @@
 // ReLU after the first five; channel 0 of the last is the node's label centre,
 // normalised to [0, 1] over the finite labels.
 //
-// The convolutions are implicit GEMMs on the tensor cores with mma.sync
-// m16n8k16 (bf16 in, fp32 accumulate): a warp owns 16 consecutive pixels of a
-// row and all 32 output channels (four n8 tiles), and walks K = 9 taps x 32
-// input channels in 18 steps, its A fragments read by ldmatrix from the window of
-// input rows it staged in shared memory (zero outside the image) and its B
-// fragments from the layer's weights staged there once per CTA. The data gradient
-// is the same kernel with the weights transposed and the taps mirrored, its
-// epilogue masking by the previous layer's ReLU. The weight gradient is a GEMM
-// over pixels (M = co, N = ci, K = pixels) per tap, accumulated in fp32 with
-// atomics. These GEMMs are small (M ~ 10^4-10^5 pixels, N = 32, K = 288): a
-// layer takes microseconds, bound by latency rather than by tensor throughput.
+// The convolutions are implicit GEMMs on the 5th-generation tensor cores
+// (net_conv_tc_kernel: tcgen05.mma, accumulator in tensor memory; below). The data
+// gradient is the same kernel with the weights transposed and the taps mirrored,
+// its epilogue masking by the previous layer's ReLU. The weight gradient is a GEMM
+// over pixels (M = 32 output channels, N = 32 input channels, K = pixels) per tap,
+// accumulated in fp32 with atomics, on mma.sync m16n8k16: its 32 rows are below the
+// 64-row minimum of a tcgen05 tile.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -272,109 +268,9 @@ __global__ void __launch_bounds__(NET_TC_M) net_conv_tc_kernel(
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u));
 }
 
-// Shared-memory rows of the convolution: 32 bf16 channels padded to 40 (80 bytes), so
+// Shared-memory rows of the weight gradient: 32 bf16 channels padded to 40 (80 bytes), so
 // the eight 16-byte rows an ldmatrix reads fall in distinct banks.
 constexpr int NET_SROW = 40;
-constexpr int NET_WIN = 3 * 18;  // a warp's input window: rows y - 1 .. y + 1, pixels x0 - 1 .. x0 + 16
-constexpr int NET_CONV_WARPS = 4;
-constexpr size_t NET_CONV_SMEM =
-    (size_t)(NET_TAPS * NET_CH + NET_CONV_WARPS * NET_WIN) * NET_SROW * sizeof(__nv_bfloat16);
-
-__device__ __forceinline__ void ldmatrix_x4(unsigned (&r)[4], const __nv_bfloat16 *p) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-
-// out[p][co] = sum_{tap, ci} in[p + tap][ci] * w[tap][co][ci] + bias[co]; then ReLU
-// (relu), or the mask of a previous activation (mask: zero where mask <= 0). out_f32,
-// when given, receives channel 0 in fp32. Persistent CTAs of four warps: the layer's
-// weights are staged in shared memory once per CTA; each warp stages its tile's 3 x 18
-// pixel window (zero outside the image) with 16-byte loads and feeds the MMAs through
-// ldmatrix. The k order (tap, then channel halves) is fixed, so the sums do not depend
-// on the staging.
-__global__ void __launch_bounds__(32 * NET_CONV_WARPS) net_conv_kernel(
-    const __nv_bfloat16 *__restrict__ in, int images, int height, int width, const __nv_bfloat16 *__restrict__ w,
-    const float *__restrict__ bias, int relu, const __nv_bfloat16 *__restrict__ mask, __nv_bfloat16 *__restrict__ out,
-    float *__restrict__ out_f32) {
-    extern __shared__ __align__(16) __nv_bfloat16 net_smem[];
-    __nv_bfloat16 *wsm = net_smem;                                     // [tap][co][NET_SROW]
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16 *win = net_smem + (NET_TAPS * NET_CH + warp * NET_WIN) * NET_SROW;  // [3][18][NET_SROW]
-    const int group = lane >> 2, tig = lane & 3;
-    // the weights, 16 bytes (8 channels) at a time
-    for (int c = threadIdx.x; c < NET_TAPS * NET_CH * 4; c += blockDim.x) {
-        const int row = c >> 2, part = c & 3;
-        *reinterpret_cast<uint4 *>(wsm + row * NET_SROW + part * 8) =
-            *reinterpret_cast<const uint4 *>(w + (size_t)row * NET_CH + part * 8);
-    }
-    __syncthreads();
-    const int segments = (width + 15) / 16;
-    const long tiles = (long)images * height * segments;
-    // ldmatrix row addresses of this lane: matrix j = lane / 8, row lane % 8
-    const int mj = lane >> 3, mr = lane & 7;
-    for (long base = (long)blockIdx.x * NET_CONV_WARPS; base < tiles; base += (long)gridDim.x * NET_CONV_WARPS) {
-        const long tile = base + warp;
-        if (tile >= tiles) break;  // whole warp; no block barrier follows
-        const int n = (int)(tile / ((long)height * segments));
-        const int rest = (int)(tile - (long)n * height * segments);
-        const int y = rest / segments, x0 = (rest - y * segments) * 16;
-        const __nv_bfloat16 *image = in + (size_t)n * height * width * NET_CH;
-        __syncwarp();  // the previous tile's reads of the window are done
-        for (int c = lane; c < NET_WIN * 4; c += 32) {
-            const int px = c >> 2, part = c & 3;
-            const int r = px / 18, xx = x0 - 1 + px % 18, yy = y - 1 + r;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (yy >= 0 && yy < height && xx >= 0 && xx < width)
-                v = *reinterpret_cast<const uint4 *>(image + ((size_t)yy * width + xx) * NET_CH + part * 8);
-            *reinterpret_cast<uint4 *>(win + px * NET_SROW + part * 8) = v;
-        }
-        __syncwarp();
-        float acc[4][4] = {};
-#pragma unroll
-        for (int tap = 0; tap < NET_TAPS; ++tap) {
-            const int r = tap / 3, dx = tap % 3;  // window row and pixel shift
-#pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                unsigned a[4];
-                ldmatrix_x4(a, win + (r * 18 + dx + (mj & 1) * 8 + mr) * NET_SROW + half * 16 + (mj >> 1) * 8);
-#pragma unroll
-                for (int np = 0; np < 2; ++np) {
-                    unsigned b[4];  // b0, b1 of n-tile 2 np, then of n-tile 2 np + 1
-                    ldmatrix_x4(b, wsm + (tap * NET_CH + (2 * np + (mj >> 1)) * 8 + mr) * NET_SROW + half * 16 +
-                                       (mj & 1) * 8);
-                    mma_bf16_16816(acc[2 * np], a[0], a[1], a[2], a[3], b[0], b[1]);
-                    mma_bf16_16816(acc[2 * np + 1], a[0], a[1], a[2], a[3], b[2], b[3]);
-                }
-            }
-        }
-        // epilogue: rows group (pixel x0 + group) and group + 8, columns co = nt * 8 + 2 tig + (0, 1)
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-            const int x = x0 + group + 8 * hh;
-            if (x >= width) continue;
-            const size_t p = ((size_t)n * height + y) * width + x;
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const int co = nt * 8 + tig * 2;
-                float v0 = acc[nt][2 * hh] + (bias ? bias[co] : 0.0f);
-                float v1 = acc[nt][2 * hh + 1] + (bias ? bias[co + 1] : 0.0f);
-                if (relu) {
-                    v0 = fmaxf(v0, 0.0f);
-                    v1 = fmaxf(v1, 0.0f);
-                }
-                if (mask) {
-                    const __nv_bfloat16 *m = mask + p * NET_CH + co;
-                    if (!(__bfloat162float(m[0]) > 0.0f)) v0 = 0.0f;
-                    if (!(__bfloat162float(m[1]) > 0.0f)) v1 = 0.0f;
-                }
-                *reinterpret_cast<unsigned *>(out + p * NET_CH + co) = pack_bf16(v0, v1);
-                if (out_f32 && co == 0) out_f32[p] = v0;
-            }
-        }
-    }
-}
 
 // dW[tap][co][ci] += sum_p dpre[p][co] * in[p + tap][ci] over a chunk of pixels (K):
 // M = co (two m16 tiles), N = ci (four n8 tiles). A warp owns (tap, chunk of 16 x

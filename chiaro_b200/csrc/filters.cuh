@@ -41,13 +41,16 @@ __global__ void reject_isolated_kernel(const uint8_t *__restrict__ src_has, cons
 }
 
 // ---- connected components ------------------------------------------------------
-// parent[] is read through L2 (__ldcg), where the atomicCAS of uf_union resolves: a
-// thread never retries a union on a stale L1 copy of a root it has just lost.
+// uf_find follows parent links to the root with path halving (benign races: any
+// ancestor is a valid parent). With through_l2, parent[] is read through L2 (__ldcg),
+// where the atomicCAS of uf_union resolves, so a thread never retries a join on a
+// stale L1 copy of a root it has just lost; a first attempt reads normally.
+template <bool through_l2>
 __device__ inline int uf_find(int *parent, int x) {
-    int p = __ldcg(parent + x);
+    int p = through_l2 ? __ldcg(parent + x) : parent[x];
     while (p != x) {
-        int gp = __ldcg(parent + p);
-        if (gp != p) parent[x] = gp;  // path halving (benign races: any ancestor is a valid parent)
+        int gp = through_l2 ? __ldcg(parent + p) : parent[p];
+        if (gp != p) parent[x] = gp;
         x = p;
         p = gp;
     }
@@ -58,14 +61,15 @@ __device__ inline int uf_find(int *parent, int x) {
 // into CHIARO_ERR_TIMEOUT instead of returning components with an edge left out.
 constexpr int UNION_GAVE_UP = 1;
 
-// Lock-free union. Each failed compare-and-swap means another thread attached root b,
-// and at most n - 1 attachments happen in all, so with retries >= n the loop always
+// Lock-free union. A failed compare-and-swap means another thread attached root b (at
+// most n - 1 attachments happen in all) or, on the first attempt only, that its reads
+// were stale (retries read through L2). With retries >= n + 1 the loop therefore always
 // ends by joining or finding a == b; a smaller bound (a caller's choice) can run out,
 // which is reported, never silent.
 __device__ inline void uf_union(int *parent, int a, int b, int retries, int *status) {
     for (int attempt = 0; attempt < retries; ++attempt) {
-        a = uf_find(parent, a);
-        b = uf_find(parent, b);
+        a = attempt ? uf_find<true>(parent, a) : uf_find<false>(parent, a);
+        b = attempt ? uf_find<true>(parent, b) : uf_find<false>(parent, b);
         if (a == b) return;
         if (a > b) {
             int t = a;
@@ -115,7 +119,7 @@ __global__ void components_size_kernel(const uint8_t *__restrict__ has, int *par
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !has[i]) return;
     const unsigned active = __activemask();
-    int root = uf_find(parent, i);
+    int root = uf_find<false>(parent, i);
     const unsigned peers = __match_any_sync(active, root);
     if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(size + root, __popc(peers));
 }
@@ -128,7 +132,7 @@ __global__ void components_mark_kernel(const uint8_t *__restrict__ src_has, int 
         dst_has[i] = 0;
         return;
     }
-    dst_has[i] = size[uf_find(parent, i)] < minimum_nodes ? 0 : 1;
+    dst_has[i] = size[uf_find<false>(parent, i)] < minimum_nodes ? 0 : 1;
 }
 
 // ---- local plane fit -------------------------------------------------------------
