@@ -182,6 +182,70 @@ CH_HD double exp_f64(double x) {
 // floor(x) as an int and x - floor(x) for 0 <= x < 2^22 without a
 // float-to-int conversion: r = floor(x) is an integer below 2^22, so r + 2^23
 // is exact and holds r in its low mantissa bits; x - r is exact.
+// floor(n / d) for 0 <= n, 1 <= d and n d < 2^32, with one multiply instead of an
+// integer division: division by an invariant integer (Granlund and Montgomery, 1994)
+// with m = ceil(2^32 / d). Writing m d = 2^32 + e with 0 <= e < d, n m / 2^32 =
+// n / d + n e / (d 2^32), and n e < n d < 2^32 keeps the second term below 1 / d, so the
+// high word of n m is the exact quotient. d = 1 keeps n (its m would be 2^32). Every use
+// in the kernels has n, d < 2^16 (items below MAX_VIEWS * MAX_LABELS, taps below 65^2).
+struct SmallDiv {
+    uint32_t m, d;
+    CH_HD explicit SmallDiv(int divisor)
+        : m(divisor > 1 ? 0xFFFFFFFFu / (uint32_t)divisor + 1u : 0u), d((uint32_t)divisor) {}
+    CH_HD int quotient(int n) const {
+        return d > 1 ? (int)(((uint64_t)(uint32_t)n * m) >> 32) : n;
+    }
+};
+
+// aggregate (depth.rs:1761-1770) of n <= N per-view scores s[i * stride] (NaN = None) in
+// registers. The reference compacts the Some scores, sorts them descending by
+// f32::total_cmp with a stable sort, needs at least minimum_support of them, and averages
+// the first min(best_view_count, m) after adding them in that order from -0.0. Here a
+// sorting network (Batcher's odd-even merge, N = 4 or 8) orders (key, score) pairs
+// descending, a None taking a key below every score. Equal keys are bit-identical scores,
+// so the sorted sequence, and with it the sum, is the reference's whatever the order the
+// network leaves among equals.
+template <int N>
+CH_HD bool aggregate_small(const float *s, int stride, int n, int minimum_support, int best_view_count,
+                           float &out) {
+    static_assert(N == 4 || N == 8, "networks for 4 and 8 views");
+    int32_t key[N];
+    float val[N];
+    int m = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const float x = i < n ? s[i * stride] : NAN;
+        const bool some = !(x != x);
+        m += some ? 1 : 0;
+        key[i] = some ? total_key(x) : INT32_MIN;
+        val[i] = x;
+    }
+    if (m < minimum_support) return false;
+    constexpr int pairs = N == 4 ? 5 : 19;
+    constexpr int net[19][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {1, 2}, {5, 6},
+                                {0, 4}, {1, 5}, {2, 6}, {3, 7}, {2, 4}, {3, 5}, {1, 2}, {3, 4}, {5, 6}};
+    constexpr int net4[5][2] = {{0, 1}, {2, 3}, {0, 2}, {1, 3}, {1, 2}};
+#pragma unroll
+    for (int c = 0; c < pairs; ++c) {
+        const int a = N == 4 ? net4[c][0] : net[c][0], b = N == 4 ? net4[c][1] : net[c][1];
+        const bool swap = key[a] < key[b];
+        const int32_t ka = key[a];
+        const float va = val[a];
+        key[a] = swap ? key[b] : ka;
+        val[a] = swap ? val[b] : va;
+        key[b] = swap ? ka : key[b];
+        val[b] = swap ? va : val[b];
+    }
+    const int k = best_view_count < m ? best_view_count : m;
+    if (k < minimum_support) return false;
+    float sum = -0.0f;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (i < k) sum += val[i];
+    out = sum / (float)k;
+    return true;
+}
+
 CH_HD float floor_frac_small(float x, int &ix) {
     const float r = floorf(x);
     ix = (int)(f2u(r + 8388608.0f) - 0x4B000000u);  // 2^23

@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
     const int total = V * D;
     const int chunks = (total + T - 1) / T;
+    const SmallDiv by_slots(D), by_taps(taps), side(2 * p.radius + 1);  // item / D, i / taps, tap rows
     NodeSmem s = carve_node_smem(smem_raw, V, taps, D);
     const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
     const DevView &rv = p.views[p.reference];
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     bool sampled = true;
     for (int t = tid; t < taps; t += T) {
         int dx, dy;
-        tap_offset(t, p.radius, dx, dy);
+        tap_offset(t, p.radius, side, dx, dy);
         float value = 0.0f;
         if (lat.planes) {
             const float2 r = __ldg(lat.planes + at0 + (ptrdiff_t)dy * lat.columns + dx);
@@ -166,9 +167,9 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     }
     unsigned undefined = 0u;
     for (int i = tid; i < V * taps; i += T) {
-        const int v = i / taps, t = i - v * taps;
+        const int v = by_taps.quotient(i), t = i - v * taps;
         int dx, dy;
-        tap_offset(t, p.radius, dx, dy);
+        tap_offset(t, p.radius, side, dx, dy);
         float qx = 0.0f, qy = 0.0f;
         if (lat.planes) {
             const float2 q = __ldg(lat.planes + (size_t)(v + 1) * lat.plane_size() + at0 +
@@ -182,19 +183,18 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
         }
         s.gh[i] = make_double2((double)qx * 0.5, (double)qy * 0.5);
     }
+    undefined = __reduce_or_sync(full, undefined);
+    if (lane == 0) warp_undefined[warp] = undefined;
+    const bool all_sampled = __syncthreads_and(sampled);
     // displacement of every (target, slot) item, view-major: item = v * D + slot
     for (int item = tid; item < total; item += T) {
-        const int v = item / D, label = cost_slot_label(p, node, item - v * D);
-        ViewGeom g;
-        geom_from_rec(p.geometry[(size_t)node * V + v], origin, g);
+        const int v = by_slots.quotient(item), label = cost_slot_label(p, node, item - v * D);
+        const ViewGeom &g = s.geom[v];
         double ddx = 0.0, ddy = 0.0;
         bool ok = g.gc_ok;
         if (ok && label > 0) ok = depth_delta(p.views[p.targets[v]].cam, g, p.label_depth[label], ddx, ddy);
         s.disp[item] = make_double2(ok ? ddx : NAN, ddy);
     }
-    undefined = __reduce_or_sync(full, undefined);
-    if (lane == 0) warp_undefined[warp] = undefined;
-    const bool all_sampled = __syncthreads_and(sampled);
     // tap boxes (eight lanes per target) and the three sequential reference
     // sums (lanes 0-2 of the warp after the box warps)
     for (int vb = warp * 4; vb < V; vb += 4 * warps) {
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
             const int item = c * T + tid;
             bool scored = false, fast = false;
             if (item < total) {
-                const int v = item / D;
+                const int v = by_slots.quotient(item);
                 const double2 dd = s.disp[item];
                 scored = !(dd.x != dd.x) && patch_ok && !((taps_bad >> v) & 1u);
                 if (scored) {
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     const int listed = n_fast + n_exact;
     for (int j = tid; j < listed; j += T) {
         const int item = s.list[j < n_fast ? j : total - 1 - (j - n_fast)];
-        const int v = item / D;
+        const int v = by_slots.quotient(item);
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = s.disp[item];
         float score;
@@ -295,10 +295,18 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     int any_finite = 0;
     for (int slot = tid; slot < D; slot += T) {
         const int label = cost_slot_label(p, node, slot);
-        float sc[MAX_VIEWS];
-        for (int v = 0; v < V; ++v) sc[v] = s.score[v * D + slot];
-        float agg;
-        float score = aggregate_scores(sc, V, p.minimum_support, p.best_view_count, agg) ? agg : NAN;
+        float agg = 0.0f;
+        bool some;
+        if (V <= 4) {  // the views' scores in registers (V is the same for the whole launch)
+            some = aggregate_small<4>(s.score + slot, D, V, p.minimum_support, p.best_view_count, agg);
+        } else if (V <= 8) {
+            some = aggregate_small<8>(s.score + slot, D, V, p.minimum_support, p.best_view_count, agg);
+        } else {
+            float sc[MAX_VIEWS];
+            for (int v = 0; v < V; ++v) sc[v] = s.score[v * D + slot];
+            some = aggregate_scores(sc, V, p.minimum_support, p.best_view_count, agg);
+        }
+        float score = some ? agg : NAN;
         float cost;
         if (isfinite(score)) {
             any_finite = 1;

@@ -43,6 +43,13 @@ __device__ __forceinline__ void tap_offset(int t, int radius, int &dx, int &dy) 
     dx = t % side - radius;
 }
 
+// The same with the row split by SmallDiv(2 radius + 1) (one multiply per tap).
+__device__ __forceinline__ void tap_offset(int t, int radius, const SmallDiv &side, int &dx, int &dy) {
+    const int row = side.quotient(t);
+    dy = row - radius;
+    dx = t - row * (int)side.d - radius;
+}
+
 // Tap positions are kept either as g/2 in f64 (double2: one 16-byte load per
 // tap on the fast path) or as g in f32 (float2: half the shared memory, halved
 // to f64 at use). g is f32 and halving is exact in f64, so both give the same

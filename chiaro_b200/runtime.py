@@ -121,6 +121,8 @@ HOSTCHECK_SIGNATURES = {
     "chiaro_hc_expf_mismatches": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_int, P(C.c_uint32)]),
     "chiaro_hc_exp_mismatches": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_double, P(C.c_uint32)]),
     "chiaro_hc_floor_mismatches": (C.c_uint64, [C.c_uint32, C.c_uint32]),
+    "chiaro_hc_smalldiv_mismatches": (C.c_uint64, []),
+    "chiaro_hc_aggregate_mismatches": (C.c_uint64, [C.c_uint64, C.c_uint64]),
     "chiaro_hc_plane_sample": (C.c_float, [P(C.c_float), C.c_int, C.c_int, C.c_float, C.c_float, P(C.c_int)]),
     "chiaro_hc_warp_map": (C.c_int, [P(C.c_float), C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                      P(C.c_float)]),

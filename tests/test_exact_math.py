@@ -84,6 +84,17 @@ def test_magic_floor_is_exact_below_2_pow_22(hc):
             assert hc.chiaro_hc_floor_mismatches(e, min(hi, e + 262144)) == 0
 
 
+def test_small_division_is_exact(hc):
+    # the kernels' item, tap and label indices (below 2^16) are split by SmallDiv's
+    # multiply instead of an integer division
+    assert hc.chiaro_hc_smalldiv_mismatches() == 0
+
+
+def test_register_aggregate_matches_the_sorted_form(hc):
+    # the cost kernel aggregates up to 8 views with a sorting network in registers
+    assert hc.chiaro_hc_aggregate_mismatches(200000, 7) == 0
+
+
 def test_plane_sample_matches_oracle(hc, oracle_lib):
     rng = np.random.default_rng(3)
     data = rng.uniform(0, 7, (37, 53)).astype(np.float32)
