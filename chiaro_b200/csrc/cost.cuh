@@ -65,7 +65,6 @@ __device__ __forceinline__ int cost_slot_label(const CostParams &p, int node, in
 // results are the same bits whatever the shape.
 constexpr int COST_THREADS = 128;
 constexpr int COST_SHAPES[] = {64, 96, 128, 160, 192};
-constexpr int COST_MAX_CHUNKS = 32;  // item chunks listed per barrier pair
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16; }
 
@@ -117,7 +116,7 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ RefPatch patch;
     __shared__ unsigned warp_undefined[T / 32];  // bit v: a tap of target v has no global warp
-    __shared__ int counts[COST_MAX_CHUNKS][2][T / 32];  // [chunk][fast, exact][warp]
+    __shared__ int list_ends[2];                 // fast items listed, exact items listed
     const unsigned full = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int warps = T / 32;
@@ -136,6 +135,7 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     // ---- staging: geometry, reference patch, tap positions (from the tap lattice when
     // the grid has one)
     if (tid < V) geom_from_rec(p.geometry[(size_t)node * V + tid], origin, s.geom[tid]);
+    if (tid < 2) list_ends[tid] = 0;  // read after the staging's barriers
     const TapLattice &lat = p.lattice;
     const size_t at0 = lat.planes ? lat.index(cx, cy) : 0;
     float centre = 0.0f;
@@ -220,74 +220,60 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     }
     __syncthreads();
 
-    // ---- which items are scored, and on which path; then list them, fast
-    // first. Chunk c holds items c * T + tid; the counts of up to
-    // COST_MAX_CHUNKS chunks are exchanged per barrier pair.
+    // ---- which items are scored, and on which path; then list them: fast ones from the
+    // front, exact ones from the back. A warp reserves its chunk's places at either end with
+    // one shared atomic add each; the order of the list only decides which thread scores
+    // which item (each score is computed alone into its own slot), so it does not change
+    // a result.
     const bool patch_ok = patch.ok;
     unsigned taps_bad = 0u;
     for (int w = 0; w < warps; ++w) taps_bad |= warp_undefined[w];
     const unsigned below = (1u << lane) - 1u;
-    int n_fast = 0, n_exact = 0;
-    for (int c0 = 0; c0 < chunks; c0 += COST_MAX_CHUNKS) {
-        const int c1 = min(chunks, c0 + COST_MAX_CHUNKS);
-        unsigned fast_bits = 0u, exact_bits = 0u;
-        for (int c = c0; c < c1; ++c) {
-            const int item = c * T + tid;
-            bool scored = false, fast = false;
-            if (item < total) {
-                const int v = by_slots.quotient(item);
-                const double2 dd = s.disp[item];
-                scored = !(dd.x != dd.x) && patch_ok && !((taps_bad >> v) & 1u);
-                if (scored) {
-                    const PlaneRef &plane = p.views[p.targets[v]].luma;
-                    fast = taps_inside(s.box[v], dd.x * 0.5, dd.y * 0.5, plane.width, plane.height);
-                } else {
-                    s.score[item] = NAN;
-                }
+    for (int c = 0; c < chunks; ++c) {
+        const int item = c * T + tid;
+        bool scored = false, fast = false;
+        if (item < total) {
+            const int v = by_slots.quotient(item);
+            const double2 dd = s.disp[item];
+            scored = !(dd.x != dd.x) && patch_ok && !((taps_bad >> v) & 1u);
+            if (scored) {
+                const PlaneRef &plane = p.views[p.targets[v]].luma;
+                fast = taps_inside(s.box[v], dd.x * 0.5, dd.y * 0.5, plane.width, plane.height);
+            } else {
+                s.score[item] = NAN;
             }
-            const unsigned fast_mask = __ballot_sync(full, scored && fast);
-            const unsigned exact_mask = __ballot_sync(full, scored && !fast);
-            if (lane == 0) {
-                counts[c - c0][0][warp] = __popc(fast_mask);
-                counts[c - c0][1][warp] = __popc(exact_mask);
-            }
-            if (scored && fast) fast_bits |= 1u << (c - c0);
-            if (scored && !fast) exact_bits |= 1u << (c - c0);
         }
-        __syncthreads();
-        for (int c = c0; c < c1; ++c) {
-            int fast_at = n_fast, exact_at = n_exact;
-            for (int w = 0; w < warps; ++w) {
-                const int f = counts[c - c0][0][w], e = counts[c - c0][1][w];
-                if (w < warp) {
-                    fast_at += f;
-                    exact_at += e;
-                }
-                n_fast += f;
-                n_exact += e;
-            }
-            const bool is_fast = (fast_bits >> (c - c0)) & 1u, is_exact = (exact_bits >> (c - c0)) & 1u;
-            const unsigned fast_mask = __ballot_sync(full, is_fast);
-            const unsigned exact_mask = __ballot_sync(full, is_exact);
-            const int item = c * T + tid;
-            if (is_fast) s.list[fast_at + __popc(fast_mask & below)] = (unsigned short)item;
-            if (is_exact) s.list[total - 1 - (exact_at + __popc(exact_mask & below))] = (unsigned short)item;
+        const unsigned fast_mask = __ballot_sync(full, scored && fast);
+        const unsigned exact_mask = __ballot_sync(full, scored && !fast);
+        int fast_at = 0, exact_at = 0;
+        if (lane == 0) {
+            if (fast_mask) fast_at = atomicAdd(&list_ends[0], __popc(fast_mask));
+            if (exact_mask) exact_at = atomicAdd(&list_ends[1], __popc(exact_mask));
         }
-        __syncthreads();
+        fast_at = __shfl_sync(full, fast_at, 0);
+        exact_at = __shfl_sync(full, exact_at, 0);
+        if (scored && fast) s.list[fast_at + __popc(fast_mask & below)] = (unsigned short)item;
+        if (scored && !fast) s.list[total - 1 - (exact_at + __popc(exact_mask & below))] = (unsigned short)item;
     }
+    __syncthreads();
+    const int n_fast = list_ends[0], n_exact = list_ends[1];
 
-    // ---- the correlations of the listed items
+    // ---- the correlations of the listed items; an item's path is known from its place
     const int listed = n_fast + n_exact;
     for (int j = tid; j < listed; j += T) {
-        const int item = s.list[j < n_fast ? j : total - 1 - (j - n_fast)];
+        const bool fast = j < n_fast;
+        const int item = s.list[fast ? j : total - 1 - (j - n_fast)];
         const int v = by_slots.quotient(item);
         const DevView &tv = p.views[p.targets[v]];
         const double2 dd = s.disp[item];
         float score;
-        if (!zncc_any(TargetRef{tv.luma, tv.quads}, s.gh + v * taps, s.box[v], s.wt, patch, taps, dd.x, dd.y,
-                      score))
-            score = NAN;
-        s.score[item] = score;
+        bool ok;
+        if (fast)
+            score = zncc_inside(tv.quads, quad_pair_stride(tv.luma.width), s.gh + v * taps, s.wt, patch, taps,
+                                dd.x * 0.5, dd.y * 0.5, ok);
+        else
+            ok = zncc_score(tv.luma, s.gh + v * taps, s.wt, patch, taps, dd.x, dd.y, score);
+        s.score[item] = ok ? score : NAN;
     }
     __syncthreads();
 
