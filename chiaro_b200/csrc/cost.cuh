@@ -205,8 +205,8 @@ __global__ void __launch_bounds__(T, 1024 / T) cost_volume_kernel(CostParams p) 
     if (warp == ((V + 3) / 4) % warps) {
         float sum = 0.0f;
         if (lane < 3)
-            sum = lane == 2 ? sequential_sum(s.rr, 1, taps)
-                            : sequential_sum(reinterpret_cast<const float *>(s.wt) + lane, 2, taps);
+            sum = lane == 2 ? sequential_sum_unrolled(s.rr, 1, taps)
+                            : sequential_sum_unrolled(reinterpret_cast<const float *>(s.wt) + lane, 2, taps);
         const float count = __shfl_sync(full, sum, 0), sum_r = __shfl_sync(full, sum, 1);
         const float sum_rr = __shfl_sync(full, sum, 2);
         if (lane == 0) {
