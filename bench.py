@@ -170,17 +170,21 @@ def correlation_instructions():
     f = ROOT / "profiles" / "correlation_issue_five_view.md"
     if not f.exists():
         return {}
-    return {m.group(1): int(m.group(2)) for m in re.finditer(r"warp_instructions (\w+) = (\d+)", f.read_text())}
+    return {m.group(1): int(m.group(2)) for m in re.finditer(r"warp_instructions ([\w<>]+) = (\d+)", f.read_text())}
 
 
-def issue_roofline(stage_ms, sm_mhz):
+def issue_roofline(stage_ms, sm_mhz, cost_threads=None):
     """Instruction-issue fractions of the correlation stages: warp instructions per launch
-    (ncu) over the stage's event time at 148 SMs x 4 schedulers x one instruction per cycle."""
+    (ncu) over the stage's event time at 148 SMs x 4 schedulers x one instruction per cycle.
+    cost_threads: the CTA size the autotuner chose for the cost volume (its count differs
+    by shape)."""
     counts = correlation_instructions()
     if not counts:
         return None
     peak = 148 * 4 * sm_mhz * 1e6
-    stages = {"cost_volume": ["cost_volume_kernel"], "direct": ["direct_depth_kernel", "direct_wide_kernel"],
+    cost = f"cost_volume_kernel<{cost_threads}>" if f"cost_volume_kernel<{cost_threads}>" in counts \
+        else "cost_volume_kernel"
+    stages = {"cost_volume": [cost], "direct": ["direct_depth_kernel", "direct_wide_kernel"],
               "decisions": ["target_decision_kernel"]}
     out = {"unit": "warp instructions / s", "peak": peak, "peak_source": f"148 SMs x 4 schedulers at {sm_mhz:.0f} MHz",
            "instructions_source": "profiles/correlation_issue_five_view.md (ncu smsp__inst_executed.sum, one launch)"}
@@ -188,7 +192,8 @@ def issue_roofline(stage_ms, sm_mhz):
         inst = sum(counts.get(k, 0) for k in kernels)
         if inst and stage_ms.get(stage):
             achieved = inst / (stage_ms[stage] / 1e3)
-            out[stage] = {"warp_instructions": inst, "achieved": round(achieved / 1e9, 1), "frac": round(achieved / peak, 4)}
+            out[stage] = {"kernels": kernels, "warp_instructions": inst, "achieved": round(achieved / 1e9, 1),
+                          "frac": round(achieved / peak, 4)}
     return out
 
 
@@ -359,7 +364,9 @@ def run_ours(args, rank, world, local):
         "batched_sgm": dict(batched, note="SGM of many instances of uneven sizes and label counts: "
                             "per-instance calls (plain) against one persistent batch replayed from a CUDA graph"),
         **({"learned_band": band} if band else {}),
-        "issue_roofline": issue_roofline(stage_ms, sm_mhz) if args.workload == "five_view" else None,
+        "issue_roofline": issue_roofline(stage_ms, sm_mhz, ctx.tuning().get((len(scene.cameras) - 1, scene.options.planes + 1,
+                                                                          scene.options.patch_radius)))
+        if args.workload == "five_view" else None,
         "compute_roofline": {"kernel": "cost_volume_kernel (build_cost_volume, the largest correlation kernel)",
                              "bound": "fp32", "achieved": round(cost_tflops, 2), "peak": round(fp32_peak, 1),
                              "unit": "TFLOP/s", "frac": round(cost_tflops / fp32_peak, 4),
