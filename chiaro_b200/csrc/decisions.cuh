@@ -30,6 +30,7 @@ struct DecisionParams {
     Field field;
     const GeomRec *geometry;  // [node][target] of the fine grid
     TapLattice lattice;       // of the fine grid, or planes == nullptr
+    const RefPatch *patches;  // [node] reference patch at `radius`, or nullptr
     double inverse_step, near_depth, far_depth;
     int radius;
     const float *spatial;
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(32 * DECISION_WARPS) target_decision_kernel(De
     unsigned undefined_taps = 0u;
     if (active)
         undefined_taps = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, p.radius, p.spatial, d.rr,
-                                          d.wt, d.gh, d.box, patch, p.lattice);
+                                          d.wt, d.gh, d.box, patch, p.lattice, p.patches ? p.patches + node : nullptr);
     const bool patch_ok = active && patch.ok;
     const D3 origin = camera_origin(rv.cam);
     const double shared_inverse = active ? 1.0 / p.field.depth[node] : 0.0;

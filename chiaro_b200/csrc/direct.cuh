@@ -91,6 +91,7 @@ struct DirectParams {
     const double *unseeded;                            // 32 candidates, far to near
     const GeomRec *geometry;                           // [node][target] of the fine grid
     TapLattice lattice;                                // of the fine grid, or planes == nullptr
+    const RefPatch *patches;                           // [node] reference patch at `radius`, or nullptr
     int radius, wide_radius;
     const float *spatial, *spatial_wide;
     float minimum_score, minimum_margin, minimum_improvement;
@@ -197,11 +198,12 @@ __device__ inline int warp_direct_candidates(const DirectParams &p, double cx, d
 // node at `radius` (warp_stage_patch); geometry from the records.
 template <typename TapT>
 __device__ inline void warp_stage_node(const DirectParams &p, const DirectSlot<TapT> &d, RefPatch &patch, double cx,
-                                       double cy, int radius, const float *spatial, const GeomRec *recs) {
+                                       double cy, int radius, const float *spatial, const GeomRec *recs,
+                                       const RefPatch *pre) {
     const int lane = threadIdx.x & 31;
     const int V = p.n_targets;
     const unsigned undefined = warp_stage_patch(p.views, p.reference, p.targets, V, cx, cy, radius, spatial, d.rr,
-                                                d.wt, d.gh, d.box, patch, p.lattice);
+                                                d.wt, d.gh, d.box, patch, p.lattice, pre);
     if (lane < V) {
         geom_from_rec(recs[lane], camera_origin(p.views[p.reference].cam), d.geom[lane]);
         d.geom[lane].taps_ok = ((undefined >> lane) & 1u) ? 0 : 1;
@@ -321,7 +323,8 @@ __global__ void __launch_bounds__(256) direct_depth_kernel(DirectParams p) {
     int seeded = 0, n = 0, n_fast = 0, n_exact = 0;
     if (active) {
         n = warp_direct_candidates(p, cx, cy, d.cand, seeded);
-        warp_stage_node(p, d, patch, cx, cy, p.radius, p.spatial, p.geometry + (size_t)node * V);
+        warp_stage_node(p, d, patch, cx, cy, p.radius, p.spatial, p.geometry + (size_t)node * V,
+                        p.patches ? p.patches + node : nullptr);
         warp_direct_list(p, d, patch, d.cand, n, n_fast, n_exact);
     }
     if (lane == 0) {
@@ -396,7 +399,7 @@ __global__ void __launch_bounds__(256) direct_wide_kernel(DirectParams p) {
         const double cx = (double)((node % p.columns) * p.step), cy = (double)((node / p.columns) * p.step);
         int seeded;
         warp_direct_candidates(p, cx, cy, d.cand, seeded);
-        warp_stage_node(p, d, patch, cx, cy, p.wide_radius, p.spatial_wide, p.geometry + (size_t)node * V);
+        warp_stage_node(p, d, patch, cx, cy, p.wide_radius, p.spatial_wide, p.geometry + (size_t)node * V, nullptr);
         const int n = last - first + 1;
         warp_direct_scores(p, d, patch, d.cand + first, n, p.wide_radius);
         double depth = 0.0;

@@ -1582,7 +1582,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     }
     // quad planes 1 per target, tap lattice 1, geometry 2, cost 1, SGM 2, select 1, completion, direct 2, filters 6, stats 2,
     // decisions 1 + 3 per target, map 1
-    ctx->launches = V + (V > 0 ? 2 : 0) + (lattice.planes ? 1 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 2 + 6 +
+    ctx->launches = V + (V > 0 ? 2 : 0) + (lattice.planes ? 1 : 0) + 1 + 2 + 1 + (int)o.completion_iterations + 3 + 6 +
                     2 + (V > 0 ? 1 + 3 * V : 0) + 1;
     // the whole-stage graph (device-buffer calls only)
     ctx->stage_graph_state = 0;
@@ -1735,10 +1735,28 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     Field direct = field_bufs(ctx, "direct", M);
     float *fguidance = dbuf<float>(ctx, "fine_guidance", M);
     uint8_t *ftested = dbuf<uint8_t>(ctx, "fine_tested", M);
+    // each fine node's reference patch at the direct radius, read by the direct pass and,
+    // at the same radius, by the decisions
+    RefPatch *fine_patches = dbuf<RefPatch>(ctx, "fine_patches", M);
+    {
+        PatchParams pp{};
+        pp.views = d_views;
+        pp.reference = reference;
+        pp.columns = (int)g.columns;
+        pp.rows = (int)g.rows;
+        pp.step = (int)g.step;
+        pp.radius = direct_radius;
+        pp.spatial = d_sp_direct;
+        if (fine_lattice) pp.lattice = lattice;
+        pp.out = fine_patches;
+        patch_sums_kernel<<<blocks_for(M, 256), 256, 0, s>>>(pp);
+        CK(cudaGetLastError());
+    }
     {
         DirectParams p{};
         p.geometry = fine_geometry;
         if (fine_lattice) p.lattice = lattice;
+        p.patches = fine_patches;
         p.views = d_views;
         p.reference = reference;
         p.n_targets = V;
@@ -1871,6 +1889,7 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         p.far_depth = o.far_depth;
         p.radius = radius;
         p.spatial = d_sp;
+        p.patches = radius == direct_radius ? fine_patches : nullptr;  // the same patch and weights
         p.minimum_score = o.minimum_score;
         int taps = (2 * radius + 1) * (2 * radius + 1);
         const size_t slot = decision_slot_bytes(V, taps);

@@ -167,12 +167,13 @@ __global__ void __launch_bounds__(256) tap_lattice_kernel(LatticeParams p) {
 // centre sample) and, for each target, g/2 of every tap and their box. Returns
 // on every lane the mask of targets with a tap where the global warp is None
 // (bit v); `patch` is written by lanes 0-2 and valid after the trailing
-// __syncwarp().
+// __syncwarp(). `pre`: the node's patch from patch_sums_kernel at this radius, or
+// nullptr; lane 0 copies it instead of the three lanes summing the taps.
 template <typename TapT>
 __device__ inline unsigned warp_stage_patch(const DevView *views, int reference, const int *targets, int V,
                                             double cx, double cy, int radius, const float *spatial, float *rr,
                                             float2 *wt, TapT *gh, TapBox *box, RefPatch &patch,
-                                            const TapLattice &lattice) {
+                                            const TapLattice &lattice, const RefPatch *pre) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int taps = (2 * radius + 1) * (2 * radius + 1);
@@ -225,18 +226,84 @@ __device__ inline unsigned warp_stage_patch(const DevView *views, int reference,
         TapBox b = group8_tap_box(gh + (v < V ? v : V - 1) * taps, taps);
         if ((lane & 7) == 0 && v < V) box[v] = b;
     }
-    if (lane < 3)
-        store_reference_sum(patch, lane,
-                            lane == 2 ? sequential_sum(rr, 1, taps)
-                                      : sequential_sum(reinterpret_cast<const float *>(wt) + lane, 2, taps));
-    __syncwarp();
-    if (lane == 0) {
-        patch.centre = centre;
-        patch.ok = centre_ok && sampled;
-        patch.ref_energy = patch.sum_rr - patch.sum_r * patch.sum_r / patch.count;
+    if (pre) {
+        if (lane == 0) patch = *pre;
+    } else {
+        if (lane < 3)
+            store_reference_sum(patch, lane,
+                                lane == 2 ? sequential_sum(rr, 1, taps)
+                                          : sequential_sum(reinterpret_cast<const float *>(wt) + lane, 2, taps));
+        __syncwarp();
+        if (lane == 0) {
+            patch.centre = centre;
+            patch.ok = centre_ok && sampled;
+            patch.ref_energy = patch.sum_rr - patch.sum_r * patch.sum_r / patch.count;
+        }
     }
     __syncwarp();
     return undefined;
+}
+
+// The reference patch of every node of a step-spaced grid at `radius`, a thread per node:
+// what warp_stage_patch computes for it (the taps' weights w = spatial * exp(-1.2 |r -
+// centre|), the sums of w, w r and (w r) r in tap order, the energy, the centre sample and
+// whether the centre and every tap were sampled), with the same expressions in the same
+// order, so the same bits. The direct pass and the decisions read it instead of summing 81
+// or more taps in three lanes of a warp.
+struct PatchParams {
+    const DevView *views;
+    int reference;
+    int columns, rows, step, radius;
+    const float *spatial;
+    TapLattice lattice;  // of this grid, or planes == nullptr
+    RefPatch *out;
+};
+
+__global__ void __launch_bounds__(256) patch_sums_kernel(PatchParams p) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)p.columns * p.rows) return;
+    const double cx = (double)((int)(i % p.columns) * p.step), cy = (double)((int)(i / p.columns) * p.step);
+    const DevView &rv = p.views[p.reference];
+    const TapLattice &lattice = p.lattice;
+    const int taps = (2 * p.radius + 1) * (2 * p.radius + 1);
+    float centre = 0.0f;
+    bool centre_ok;
+    const size_t at0 = lattice.planes ? lattice.index(cx, cy) : 0;
+    if (lattice.planes) {
+        const float2 c = __ldg(lattice.planes + at0);
+        centre = c.x;
+        centre_ok = c.y != 0.0f;
+    } else {
+        centre_ok = plane_sample(rv.luma, (float)((cx - 0.5) * 0.5), (float)((cy - 0.5) * 0.5), centre);
+    }
+    bool sampled = true;
+    float count = 0.0f, sum_r = 0.0f, sum_rr = 0.0f;
+    for (int t = 0; t < taps; ++t) {
+        int dx, dy;
+        tap_offset(t, p.radius, dx, dy);
+        float value = 0.0f;
+        if (lattice.planes) {
+            const float2 r = __ldg(lattice.planes + at0 + (ptrdiff_t)dy * lattice.columns + dx);
+            value = r.x;
+            sampled &= r.y != 0.0f;
+        } else {
+            double px = cx + (double)dx * 2.0, py = cy + (double)dy * 2.0;
+            sampled &= plane_sample(rv.luma, (float)((px - 0.5) * 0.5), (float)((py - 0.5) * 0.5), value);
+        }
+        float weight = __ldg(p.spatial + t) * exp_f32(-1.2f * fabsf(value - centre));
+        float weighted = weight * value;
+        count += weight;
+        sum_r += weighted;
+        sum_rr += weighted * value;
+    }
+    RefPatch r;
+    r.count = count;
+    r.sum_r = sum_r;
+    r.sum_rr = sum_rr;
+    r.ref_energy = sum_rr - sum_r * sum_r / count;
+    r.centre = centre;
+    r.ok = centre_ok && sampled;
+    p.out[i] = r;
 }
 
 // Label-independent geometry of map_at_depth for one (node, target); one thread.
