@@ -17,7 +17,7 @@ import zlib
 from dataclasses import dataclass, field
 from enum import IntEnum
 from pathlib import Path
-from typing import List, Optional, Sequence
+from typing import Iterable, List, Optional, Sequence
 
 import numpy as np
 
@@ -454,3 +454,124 @@ class DeviceStage:
             return False
         self.ctx.check(status)
         return True
+
+
+class DepthPipeline:
+    """refine_multiview_depth over a stream of frames of one rig, each frame's upload and the
+    previous frame's read-back overlapping the current frame's stage on the GPU.
+
+    Two ``DeviceStage`` objects on one context alternate. While frame i runs on one of them,
+    frame i + 1's planes and warps go up into the other's device buffers on a copy stream, and
+    frame i - 1's outputs come down from the other's output buffers into pinned host memory on
+    a second copy stream. The stages themselves run one after the other (they share the
+    context's working buffers), so every frame gets the bits a call of its own gives. For the
+    uploads to overlap, pass pinned CPU tensors; numpy arrays are first copied into the
+    pipeline's own pinned buffers on the host.
+    """
+
+    def __init__(self, inputs: Sequence, reference_index: int, alignments: Sequence, options: DepthOptions,
+                 context=None):
+        import torch
+
+        from .runtime import default_context
+
+        ctx = context if context is not None else default_context()
+        self.stages = [DeviceStage(inputs, reference_index, alignments, options, context=ctx) for _ in range(2)]
+        first = self.stages[0]
+        self.ctx, self.targets, self.nodes = ctx, first.targets, first.nodes
+        self._device = first._device
+        self._in = torch.cuda.Stream(self._device)
+        self._out = torch.cuda.Stream(self._device)
+        self._in_ready = [torch.cuda.Event() for _ in range(2)]
+        self._out_done = [torch.cuda.Event() for _ in range(2)]
+
+        def pinned_like(t):
+            return torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+
+        # read-back buffers per stage: the host copies of its outputs
+        self._host = []
+        for st in self.stages:
+            self._host.append({"depth": pinned_like(st.depth), "confidence": pinned_like(st.confidence),
+                               "provenance": pinned_like(st.provenance),
+                               "points": {t: pinned_like(st.points[t]) for t in self.targets},
+                               "point_confidence": {t: pinned_like(st.point_confidence[t]) for t in self.targets}})
+        # pinned staging for numpy frames, per stage: planes, warp points, warp confidence
+        self._staging = [[[pinned_like(x) for x in xs] for xs in (st.planes, st.warp_points, st.warp_confidence)]
+                         for st in self.stages]
+
+    def _upload(self, k: int, frame) -> int:
+        """Queue frame's host → device copies into stage k on the upload stream; returns bytes."""
+        import torch
+
+        st = self.stages[k]
+        planes, points, confidence = (list(frame) + [None, None])[:3]
+        moved = 0
+        with torch.cuda.stream(self._in):
+            for which, (srcs, dsts) in enumerate(((planes, st.planes), (points, st.warp_points),
+                                                  (confidence, st.warp_confidence))):
+                if srcs is None:
+                    continue
+                for i, (src, dst) in enumerate(zip(srcs, dsts)):
+                    if not isinstance(src, torch.Tensor):
+                        stage = self._staging[k][which][i]
+                        stage.numpy().reshape(-1)[:] = np.asarray(src, dtype=np.float32).reshape(-1)
+                        src = stage
+                    dst.copy_(src.reshape(dst.shape), non_blocking=True)
+                    moved += dst.numel() * dst.element_size()
+            self._in_ready[k].record(self._in)
+        return moved
+
+    def _download(self, k: int) -> int:
+        """Queue stage k's outputs device → pinned host on the read-back stream; returns bytes."""
+        import torch
+
+        st, host = self.stages[k], self._host[k]
+        pairs = [(host["depth"], st.depth), (host["confidence"], st.confidence),
+                 (host["provenance"], st.provenance)]
+        pairs += [(host["points"][t], st.points[t]) for t in self.targets]
+        pairs += [(host["point_confidence"][t], st.point_confidence[t]) for t in self.targets]
+        with torch.cuda.stream(self._out):
+            for dst, src in pairs:
+                dst.copy_(src, non_blocking=True)
+            self._out_done[k].record(self._out)
+        return sum(src.numel() * src.element_size() for _, src in pairs)
+
+    def _outputs(self, k: int) -> dict:
+        self._out_done[k].synchronize()
+        host = self._host[k]
+        return {"depth": host["depth"].numpy(), "confidence": host["confidence"].numpy(),
+                "provenance": host["provenance"].numpy(),
+                "points": {t: v.numpy() for t, v in host["points"].items()},
+                "point_confidence": {t: v.numpy() for t, v in host["point_confidence"].items()}}
+
+    def run(self, frames: Iterable):
+        """Yield (ok, outputs) per frame, in order. A frame is (planes, warp_points,
+        warp_confidence), each a per-view list of host arrays or CPU tensors shaped like the
+        constructor's inputs (warp_points and warp_confidence may be None: the previous warps
+        stay). ok is False where the reference returns None. outputs holds numpy views of the
+        pipeline's pinned read-back buffers ("depth", "confidence", "provenance", and per target
+        "points" and "point_confidence"). They are reused two frames later, so copy what you
+        keep. ``self.bytes_up`` and ``self.bytes_down`` count the bytes each frame moved."""
+        import torch
+
+        it = iter(frames)
+        current = next(it, None)
+        if current is None:
+            return
+        self.bytes_up, self.bytes_down = [self._upload(0, current)], []
+        i, pending = 0, None
+        while current is not None:
+            k = i % 2
+            following = next(it, None)
+            if following is not None:  # the other stage's last stage call has returned
+                self.bytes_up.append(self._upload(1 - k, following))
+            st = self.stages[k]
+            st.stream.wait_event(self._in_ready[k])   # this frame's inputs are up
+            st.stream.wait_event(self._out_done[k])   # frame i - 2's outputs are read back
+            ok = st()
+            self.bytes_down.append(self._download(k))
+            if pending is not None:
+                yield pending[0], self._outputs(pending[1])
+            pending = (ok, k)
+            current, i = following, i + 1
+        yield pending[0], self._outputs(pending[1])
