@@ -48,7 +48,7 @@ struct chiaro_depth_ctx {
     std::map<std::string, Buffer> buffers;
     cudaEvent_t events[8] = {};
     cudaStream_t copy_stream = nullptr;  // host transfers that overlap the stage's kernels
-    cudaEvent_t planes_ready = nullptr, map_ready = nullptr;
+    cudaEvent_t planes_ready = nullptr, map_ready = nullptr, ref_ready = nullptr;
     // batched SGM: the last captured graph and the tuned warps per CTA per size bucket
     uint64_t batch_key = 0;
     cudaGraphExec_t batch_exec = nullptr;
@@ -1622,11 +1622,20 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     launch_geometry(ctx, d_views, reference, targets, g.coarse_columns, g.coarse_rows, g.coarse_step,
                     coarse_geometry);
     launch_geometry(ctx, d_views, reference, targets, g.columns, g.rows, g.step, fine_geometry);
-    if (host && !host->planes.empty()) {
-        for (const auto &u : host->planes)
+    // the reference's plane goes up first: the tap lattice and the fine reference patches
+    // need only it (and the warps), so they run while the targets' planes arrive
+    const bool host_planes = host && !host->planes.empty();
+    if (host_planes) {
+        const auto &r = host->planes[(size_t)reference];
+        CK(cudaMemcpyAsync(r.dst, r.src, r.bytes, cudaMemcpyHostToDevice, ctx->copy_stream));
+        CK(cudaEventRecord(ctx->ref_ready, ctx->copy_stream));
+        for (size_t i = 0; i < host->planes.size(); ++i) {
+            if ((int)i == reference) continue;
+            const auto &u = host->planes[i];
             CK(cudaMemcpyAsync(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice, ctx->copy_stream));
+        }
         CK(cudaEventRecord(ctx->planes_ready, ctx->copy_stream));
-        CK(cudaStreamWaitEvent(s, ctx->planes_ready, 0));
+        CK(cudaStreamWaitEvent(s, ctx->ref_ready, 0));
     }
     if (lattice.planes) {
         LatticeParams p{};
@@ -1641,6 +1650,24 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
         tap_lattice_kernel<<<blocks_for((size_t)lattice.columns * lattice.rows, 256), 256, 0, s>>>(p);
         CK(cudaGetLastError());
     }
+    // each fine node's reference patch at the direct radius, read by the direct pass and,
+    // at the same radius, by the decisions
+    RefPatch *fine_patches = dbuf<RefPatch>(ctx, "fine_patches", M);
+    {
+        PatchParams pp{};
+        pp.views = d_views;
+        pp.reference = reference;
+        pp.columns = (int)g.columns;
+        pp.rows = (int)g.rows;
+        pp.step = (int)g.step;
+        pp.radius = direct_radius;
+        pp.spatial = d_sp_direct;
+        if (fine_lattice) pp.lattice = lattice;
+        pp.out = fine_patches;
+        patch_sums_kernel<<<blocks_for(M, 256), 256, 0, s>>>(pp);
+        CK(cudaGetLastError());
+    }
+    if (host_planes) CK(cudaStreamWaitEvent(s, ctx->planes_ready, 0));
     // quad planes of the target luminance for the fast ZNCC path
     for (int t : targets) {
         const PlaneRef &lp = h_views[t].luma;
@@ -1735,23 +1762,6 @@ void run_stage(chiaro_depth_ctx *ctx, std::vector<DevView> h_views, DevView *d_v
     Field direct = field_bufs(ctx, "direct", M);
     float *fguidance = dbuf<float>(ctx, "fine_guidance", M);
     uint8_t *ftested = dbuf<uint8_t>(ctx, "fine_tested", M);
-    // each fine node's reference patch at the direct radius, read by the direct pass and,
-    // at the same radius, by the decisions
-    RefPatch *fine_patches = dbuf<RefPatch>(ctx, "fine_patches", M);
-    {
-        PatchParams pp{};
-        pp.views = d_views;
-        pp.reference = reference;
-        pp.columns = (int)g.columns;
-        pp.rows = (int)g.rows;
-        pp.step = (int)g.step;
-        pp.radius = direct_radius;
-        pp.spatial = d_sp_direct;
-        if (fine_lattice) pp.lattice = lattice;
-        pp.out = fine_patches;
-        patch_sums_kernel<<<blocks_for(M, 256), 256, 0, s>>>(pp);
-        CK(cudaGetLastError());
-    }
     {
         DirectParams p{};
         p.geometry = fine_geometry;
@@ -2142,6 +2152,7 @@ int chiaro_depth_ctx_create(int device, chiaro_depth_ctx **out) {
         for (auto &e : ctx->events) CK(cudaEventCreate(&e));
         CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&ctx->planes_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->ref_ready, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ctx->map_ready, cudaEventDisableTiming));
     } catch (const CudaError &e) {
         delete ctx;
@@ -2163,6 +2174,7 @@ void chiaro_depth_ctx_destroy(chiaro_depth_ctx *ctx) {
     if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
     if (ctx->stage_exec) cudaGraphExecDestroy(ctx->stage_exec);
     if (ctx->planes_ready) cudaEventDestroy(ctx->planes_ready);
+    if (ctx->ref_ready) cudaEventDestroy(ctx->ref_ready);
     if (ctx->map_ready) cudaEventDestroy(ctx->map_ready);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
