@@ -186,7 +186,8 @@ def issue_roofline(stage_ms, sm_mhz, cost_threads=None):
     peak = 148 * 4 * sm_mhz * 1e6
     cost = f"cost_volume_kernel<{cost_threads}>" if f"cost_volume_kernel<{cost_threads}>" in counts \
         else "cost_volume_kernel"
-    stages = {"cost_volume": [cost], "direct": ["direct_depth_kernel", "direct_wide_kernel", "patch_sums_kernel"],
+    # the fine reference patches run right after the tap lattice, inside the cost volume's events
+    stages = {"cost_volume": [cost, "patch_sums_kernel"], "direct": ["direct_depth_kernel", "direct_wide_kernel"],
               "decisions": ["target_decision_kernel"]}
     out = {"unit": "warp instructions / s", "peak": peak, "peak_source": f"148 SMs x 4 schedulers at {sm_mhz:.0f} MHz",
            "instructions_source": "profiles/correlation_issue_five_view.md (ncu smsp__inst_executed.sum, one launch)"}
