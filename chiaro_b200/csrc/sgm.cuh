@@ -88,8 +88,8 @@ __host__ __device__ inline void sgm_path_of(int b, int columns, int rows, int &p
 }
 
 // Path `warp_path` of the launch's enumeration (sgm_path_of), walked by the
-// calling warp; pass k writes paths + k * pitch.
-template <int K>
+// calling warp; pass k writes paths + k * pitch. P: steps of data prefetched ahead.
+template <int K, int P = SGM_PREFETCH>
 __device__ __forceinline__ void sgm_walk_path(const float *__restrict__ data, const float *__restrict__ guidance,
                                               float *__restrict__ paths, size_t pitch, int columns, int rows,
                                               int labels, int warp_path) {
@@ -105,7 +105,6 @@ __device__ __forceinline__ void sgm_walk_path(const float *__restrict__ data, co
         dr = -dr;
         dc = -dc;
     }
-    constexpr int P = SGM_PREFETCH;
     bool valid[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) valid[k] = lane + 32 * k < labels;
@@ -188,6 +187,20 @@ __global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA) sgm_paths_kernel(const
     const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
     if (warp_path >= (int)sgm_total_paths(columns, rows)) return;  // whole warp
     sgm_walk_path<K>(data, guidance, paths, pitch, columns, rows, labels, warp_path);
+}
+
+// The same with one step of prefetch and registers held down so that more CTAs fit an SM:
+// on a grid with more paths than the form above keeps resident, every path runs at once
+// instead of the last ones starting as the first finish. The same path code, so the same bits.
+constexpr int sgm_resident_blocks(int K) { return K <= 5 ? 12 : (K <= 7 ? 10 : 8); }
+
+template <int K>
+__global__ void __launch_bounds__(32 * SGM_PATHS_PER_CTA, sgm_resident_blocks(K))
+    sgm_paths_resident_kernel(const float *__restrict__ data, const float *__restrict__ guidance,
+                              float *__restrict__ paths, size_t pitch, int columns, int rows, int labels) {
+    const int warp_path = blockIdx.x * SGM_PATHS_PER_CTA + (threadIdx.x >> 5);
+    if (warp_path >= (int)sgm_total_paths(columns, rows)) return;  // whole warp
+    sgm_walk_path<K, 1>(data, guidance, paths, pitch, columns, rows, labels, warp_path);
 }
 
 // out = ((0 + L1) + L2) + ... + L8 per cell, the reference's order.

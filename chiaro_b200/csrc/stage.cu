@@ -299,9 +299,16 @@ void launch_geometry(chiaro_depth_ctx *ctx, const DevView *d_views, int referenc
 template <int K>
 void sgm_paths(chiaro_depth_ctx *ctx, const float *data, const float *guidance, float *paths, size_t pitch,
                int columns, int rows, int labels) {
-    const unsigned blocks = (unsigned)div_ceil(sgm_total_paths(columns, rows), SGM_PATHS_PER_CTA);
-    sgm_paths_kernel<K><<<blocks, 32 * SGM_PATHS_PER_CTA, 0, ctx->stream>>>(data, guidance, paths, pitch, columns,
-                                                                            rows, labels);
+    const size_t total_paths = sgm_total_paths(columns, rows);
+    const unsigned blocks = (unsigned)div_ceil(total_paths, SGM_PATHS_PER_CTA);
+    // more paths than the prefetching form keeps resident (six 4-warp CTAs per SM): the
+    // resident form runs them all at once
+    if (total_paths > (size_t)ctx->sm_count * 24)
+        sgm_paths_resident_kernel<K><<<blocks, 32 * SGM_PATHS_PER_CTA, 0, ctx->stream>>>(
+            data, guidance, paths, pitch, columns, rows, labels);
+    else
+        sgm_paths_kernel<K><<<blocks, 32 * SGM_PATHS_PER_CTA, 0, ctx->stream>>>(data, guidance, paths, pitch,
+                                                                                columns, rows, labels);
     CK(cudaGetLastError());
 }
 
