@@ -8,8 +8,8 @@
 // and the short ones fill the tail. A resident grid of warps pulls tasks from
 // the list with one atomicAdd per task (lane 0, broadcast by shuffle) and walks
 // each path with the same warp-per-path code as the single-instance SGM
-// (sgm_walk_path), writing that direction's path costs into the instance's
-// path buffers. No warp waits on another: the ordered sum of the 8 path
+// (sgm_walk_path, one step of prefetch: fewer registers, so more warps walk at once),
+// writing that direction's path costs into the instance's path buffers. No warp waits on another: the ordered sum of the 8 path
 // buffers, ((0 + L1) + L2) + ... + L8 per cell as the reference adds them,
 // runs as a second kernel over all instances. An instance whose label count
 // the launch was not built for sets the error word instead of being walked.
@@ -44,7 +44,7 @@ __global__ void sgm_batch_paths_kernel(const SgmInstance *__restrict__ instances
 #define SGM_BATCH_CASE(k)                                                                                    \
     case k:                                                                                                  \
         if (k <= KMAX)                                                                                       \
-            sgm_walk_path<(k <= KMAX ? k : 1)>(in.costs, in.guidance, in.paths, in.pitch, in.columns, in.rows, \
+            sgm_walk_path<(k <= KMAX ? k : 1), 1>(in.costs, in.guidance, in.paths, in.pitch, in.columns, in.rows, \
                                               in.labels, task.y);                                           \
         else if (lane == 0)                                                                                  \
             atomicExch(error, 1);                                                                            \
