@@ -551,7 +551,9 @@ class DepthPipeline:
         stay). ok is False where the reference returns None. outputs holds numpy views of the
         pipeline's pinned read-back buffers ("depth", "confidence", "provenance", and per target
         "points" and "point_confidence"). They are reused two frames later, so copy what you
-        keep. ``self.bytes_up`` and ``self.bytes_down`` count the bytes each frame moved."""
+        keep. A frame's upload is queued one frame ahead and read by its own stage: leave a
+        frame's host tensors unchanged until the results of the frame after it are yielded.
+        ``self.bytes_up`` and ``self.bytes_down`` count the bytes each frame moved."""
         import torch
 
         it = iter(frames)
