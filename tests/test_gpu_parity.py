@@ -241,6 +241,27 @@ def test_stage_with_a_wide_patch_bit_exact():
     _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
 
 
+@pytest.mark.parametrize("radius", [1, 2])
+def test_stage_with_a_narrow_patch_bit_exact(radius):
+    """patch_radius 1 and 2: the direct pass works at radius 3 and reads the reference patches
+    computed at that radius, while the decisions, at the smaller radius, sum their own."""
+    sc = scenes.workload("tiny", seed=10 + radius)
+    opt = DepthOptions(**{**sc.options.__dict__, "patch_radius": radius})
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc, options=opt)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+
+
+@pytest.mark.parametrize("sources,radius", [(2, 2), (3, 3)])
+def test_stage_with_two_and_three_targets_bit_exact(sources, radius):
+    """Two targets take the CTA-pooled decisions (12 and 16 items per node), three the
+    per-warp form (18 and 24 items); with the narrow radius the decisions sum their own
+    patches, with radius 3 they read the precomputed ones."""
+    sc = scenes.workload("tiny", seed=20 + sources, n_sources=sources)
+    opt = DepthOptions(**{**sc.options.__dict__, "patch_radius": radius})
+    dmap, omap, al_g, dbg_g, dbg_o = _run_both(sc, options=opt)
+    _compare_stage_outputs(dmap, omap, al_g, dbg_g, dbg_o, len(sc.cameras))
+
+
 def test_stage_at_the_finest_coarse_grid_bit_exact():
     """grid_step 4: the coarse grid at the direct grid's step (the finest the reference
     reaches, depth.rs:326-328), as in the five-view workload's step-4 configuration."""
